@@ -1,0 +1,151 @@
+/* pywave_b200 -- C ABI of the B200-native acoustic FD / TRI / FWI-gradient path.
+ *
+ * Plain C: pointers, sizes and status codes; no torch or CUDA types in the
+ * signatures (streams are passed as `void *`, a cudaStream_t; NULL = the
+ * legacy default stream).  Every entry point returns PW_OK (0) or a negative
+ * PW_ERR_* status; pw_last_error() gives the message of the calling thread's
+ * last failure.
+ *
+ * Array conventions follow the reference: column-major, z fastest
+ * (pywave/afd2d.py:48 `vel.flatten(order='F')`); traces with time fastest
+ * ([ny][nx][nt], pywave/src/afd.c:202-206,473-486); pfwi data [ns][nr][nt]
+ * (pywave/pfwi.py:74).  Pointers are device pointers unless the args carry
+ * PW_HOST_PTRS, in which case the library stages host<->device copies on the
+ * given stream itself (the drop-in path of the reference's Python glue).
+ */
+#ifndef PYWAVE_B200_H
+#define PYWAVE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PW_OK 0
+#define PW_ERR_SHAPE (-1)     /* inconsistent or unsupported sizes / indices */
+#define PW_ERR_CFL (-2)       /* time step violates the scheme's stability limit */
+#define PW_ERR_OOM (-3)       /* device allocation failed */
+#define PW_ERR_TIMEOUT (-4)   /* a bounded device-side wait gave up */
+#define PW_ERR_CUDA (-5)      /* a CUDA runtime call failed */
+#define PW_ERR_VALUE (-6)     /* NaN/Inf or non-positive velocity, bad flag */
+
+#define PW_HOST_PTRS 1        /* all array pointers are host memory */
+#define PW_NO_CFL_CHECK 2     /* skip the host-side stability check */
+
+/* ---------------------------------------------------------------- afd --- */
+
+/* Arguments of the afd propagator: afd2dc / afd3dc of the reference
+ * (pywave/src/afd.c:23-314 and 316-578; parse formats afd.c:73,366), with
+ * abc forced on and every face using nbt/ct as afd.c:98-116,389-402 do. */
+typedef struct pw_afd_args {
+  int dim;        /* 2 or 3 */
+  int nz, nx, ny; /* interior model size (ny = 1 for 2-D) */
+  int nt;         /* time samples */
+  int nbt;        /* absorbing taper width on every face (afd.c:101-116) */
+  float ct;       /* taper coefficient, w = exp(-(ct*(nbt-1-i))^2) (wave_abc.c:142) */
+  float dt, dz, dx, dy;
+  int ns;         /* forward: number of point sources */
+  int tri;        /* 0: forward modelling, 1: time-reversal (reverse time, inject traces) */
+  int jsnap;      /* snapshot interval (0 = no snapshots), wave_fdm.c:652-661 */
+  int gz;         /* receiver depth in interior rows below the top (0 = the reference's z=0) */
+  int flags;      /* PW_HOST_PTRS | PW_NO_CFL_CHECK */
+} pw_afd_args;
+
+/* Forward modelling or time reversal with the afd scheme.
+ * Replaces afd2dc / afd3dc (pywave/src/afd.c:316, :23) and the time loops of
+ * fdm2d / fdm (pywave/src/wave_fdm.c:397-686, 28-381).
+ *   vel     [ny][nx][nz]                 interior velocity
+ *   src     forward: [k][ns] with k rows sx,sz,f,t,A (2-D) or sx,sy,sz,f,t,A
+ *           (3-D), exactly afd2d.py:68 / afd3d.py:70's packing;
+ *           tri: traces [ny][nx][nt] injected at the receiver row
+ *   wavelet optional [ns][nt] source time functions; NULL = the reference's
+ *           Ricker table built from f,t,A (wave_fdm.c:502-516)
+ *   dat     forward: recorded traces [ny][nx][nt] (may be NULL); unused in tri
+ *   wfd     snapshots [ntsnap][ny][nx][nz], ntsnap = #{it < nt : it % jsnap == 0}
+ *           (may be NULL); the reference's afd2dc returns dat then wfd. */
+int pw_afd(const pw_afd_args *a, const float *vel, const float *src, const float *wavelet,
+           float *dat, float *wfd, void *stream);
+
+/* Time-reversal source imaging with G receiver groups propagated in lockstep
+ * and the image fused into the time loop:
+ *   img = sum_{it % jsnap == 0} prod_g u_g(it)^2        (then / max if normalize)
+ * This is what the TRI demos assemble in Python from G afd2d/afd3d(tri=True)
+ * runs (demos/test_third_tri.py:61-77, demos/test_mod2d_tri_psVSfd.py:166-190);
+ * the reference's own C image (wave_fdm.c:666-672) is never returned
+ * (afd.c:562-574).
+ *   group   [ny][nx] group id (0..ngroups-1) of each receiver, -1 = unused;
+ *           NULL = the demos' x-bands of width nx/ngroups
+ *   dat     traces [ny][nx][nt] (every group reads its own receivers)
+ *   img     [ny][nx][nz] */
+int pw_tri_image(const pw_afd_args *a, int ngroups, const int *group, const float *vel,
+                 const float *dat, float *img, int normalize, void *stream);
+
+/* --------------------------------------------------------------- pfwi --- */
+
+/* pfwi's 20-float parameter array (pywave/pfwi.py:40-61) decoded, plus the
+ * settings pfwi.c hard-codes (sz=5, rz=1, nr=nx, dr=dx, r0=ox: pfwi.c:796-801). */
+typedef struct pw_fwi_args {
+  int nz, nx;
+  float dz, dx, oz, ox;
+  int nt;
+  float dt, ot;
+  int ns;
+  float ds, os;
+  int nb;          /* sponge width (wave_fwiutil.c:31-36) */
+  float coef;      /* sponge coefficient, bc[i] = expf(-(coef*(nb-i))^2) */
+  float f0;        /* reference frequency (unused by the acoustic path) */
+  int acqui_type;  /* 1 fixed spread, otherwise moving spread (wave_fwiutil.c:55-71) */
+  int interval;    /* snapshot interval of the reference-mode gradient */
+  int niter;       /* L-BFGS iterations (pw_fwi) */
+  int sz, rz;      /* source / receiver depth below the top (pfwi.c: 5 and 1) */
+  int flags;       /* PW_HOST_PTRS | PW_NO_CFL_CHECK */
+} pw_fwi_args;
+
+/* Fills a pw_fwi_args from pfwi's float parameter array (pfwi.c:691-713
+ * reads it; only the first 20 entries are meaningful). */
+int pw_fwi_args_from_pararray(const float *pararray, int n, pw_fwi_args *out);
+
+/* Acoustic forward modelling of all shots: forward_modeling_ac
+ * (pywave/src/pfwi.c:27) -> forward_modeling_a (wave_fwimodeling.c:21-114).
+ *   vel [nx][nz], wav [nt], data [ns][nr][nt]. */
+int pw_pfwi_forward(const pw_fwi_args *a, const float *vel, const float *wav, float *data,
+                    void *stream);
+
+#define PW_GRAD_REFERENCE 0  /* gradient_av's imaging: snapshot-difference u_tt, interior only */
+#define PW_GRAD_EXACT 1      /* exact discrete adjoint of the forward scheme, incl. the sponge
+                                and the edge-replicated padding; checkpointed */
+
+/* One FWI gradient over all shots: gradient_av (wave_fwigradient.c:93-242)
+ * without its post-processing (see pw_gradient_postprocess).
+ *   weight  [nr][nt] residual weights; NULL = residual_weighting as fwic sets
+ *           it up (wave_fwiutil.c:225-296, pfwi.c:849-855)
+ *   grad    [nx][nz] dJ/dv (EXACT) or the reference's raw gradient (REFERENCE)
+ *   misfit  0.5*sum(r^2) in FP64 (REFERENCE: unweighted residual as the
+ *           reference; EXACT: 0.5*sum(w r^2), consistent with grad)
+ *   ckpt_k  checkpoint interval of the EXACT mode (0 = autotuned) */
+int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const float *wav,
+                     const float *dobs, const float *weight, float *grad, double *misfit,
+                     int ckpt_k, void *stream);
+
+/* gradient_av's tail (wave_fwigradient.c:244-255): triangle smoothing
+ * rect x rect (wave_fwiutil.c:298-335) and the scale factor; *scaling <= 0 on
+ * entry means "first call": it is set to 0.1/max|grad| as the reference's
+ * static does. */
+int pw_gradient_postprocess(int nz, int nx, int rect, int waterz, float *grad, float *scaling,
+                            int flags, void *stream);
+
+/* ------------------------------------------------------------ utility --- */
+
+const char *pw_last_error(void);
+const char *pw_version(void);
+/* Releases the calling device's cached device memory. */
+int pw_release_cache(void);
+/* Device time of the calling thread's last completed call: the time loop
+ * alone (CUDA events recorded on the call's stream around its step kernels),
+ * the number of step-kernel launches in it, and the whole call's kernel
+ * launches.  Used by the benchmark to time the dominant kernel live. */
+int pw_last_timing(double *loop_ms, long long *step_launches, long long *total_launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,308 @@
+"""ctypes front-end of the CPU oracle (oracle/pw_oracle.c).
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may import this
+module, and only as the checker or the timed CPU baseline.  The product
+(``pywave_b200``) never imports it and fails loudly when its CUDA library is
+missing.
+
+Array conventions follow the reference: column-major with z fastest
+(``vel.flatten(order='F')`` in pywave/afd2d.py:48), traces ``[nx][nt]`` with
+time fastest (pywave/src/afd.c:473-486).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle restatement (gcc, no FMA contraction)."""
+    srcs = [os.path.join(HERE, f) for f in ("pw_oracle.c", "pw_oracle_body.h")]
+    stale = (not os.path.exists(LIB_PATH)) or any(
+        os.path.getmtime(s) > os.path.getmtime(LIB_PATH) for s in srcs)
+    if force or stale:
+        subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    return LIB_PATH
+
+
+def build_ref() -> bool:
+    """Compile the reference itself into oracle/_ref (needs its sources)."""
+    if not os.path.isdir("/root/reference/pywave/src"):
+        return False
+    subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    return True
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB_PATH)
+        L.or_next_fast.argtypes = [C.c_int]
+        L.or_next_fast.restype = C.c_int
+        L.or_pad_first.argtypes = [C.c_int]
+        L.or_pad_first.restype = C.c_int
+        L.or_ricker.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, _f64p]
+        L.or_ricker.restype = None
+        L.or_smooth2d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        L.or_smooth2d.restype = None
+        L.or_residual_weights.argtypes = [C.c_int] * 6 + [_f32p]
+        L.or_residual_weights.restype = None
+        for sfx, rp in (("f32", _f32p), ("f64", _f64p)):
+            f = getattr(L, "or_afd_" + sfx)
+            f.argtypes = ([C.c_int] * 5 + [C.c_float] * 5 + [C.c_int, C.c_int, _i32p, _i32p, _i32p,
+                          rp, C.c_int, rp, C.c_int, C.c_int, rp, rp, C.c_void_p])
+            f.restype = C.c_int
+            geo = [C.c_int, _i32p, C.c_int, C.c_int, _i32p, _i32p, _i32p, C.c_int, C.c_int]
+            f = getattr(L, "or_pfwi_forward_" + sfx)
+            f.argtypes = [C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 2 + geo + [rp, rp, rp]
+            f.restype = None
+            real = C.c_float if sfx == "f32" else C.c_double
+            f = getattr(L, "or_pfwi_gradient_ref_" + sfx)
+            f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 2 + [C.c_int]
+                          + geo + [rp, rp, rp, rp, rp])
+            f.restype = real
+            f = getattr(L, "or_pfwi_gradient_exact_" + sfx)
+            f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 2 + geo
+                          + [rp, rp, rp, C.c_void_p, rp])
+            f.restype = real
+            f = getattr(L, "or_pfwi_misfit_" + sfx)
+            f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 2 + geo
+                          + [rp, rp, rp, C.c_void_p])
+            f.restype = real
+        _lib = L
+    return _lib
+
+
+# --------------------------------------------------------------------------
+# afd (pywave/afd2d.py, afd3d.py -> afd.c -> wave_fdm.c)
+# --------------------------------------------------------------------------
+
+def next_fast(n: int) -> int:
+    return lib().or_next_fast(int(n))
+
+
+def ricker(nt: int, dt: float, f0: float, t0: float, A: float) -> np.ndarray:
+    """Ricker table of fdm2d/fdm (wave_fdm.c:502-516), float64."""
+    out = np.zeros(nt, np.float64)
+    lib().or_ricker(int(nt), float(dt), float(f0), float(t0), float(A), out)
+    return out
+
+
+def _ntsnap(nt, jsnap):
+    return sum(1 for it in range(nt) if jsnap and it % jsnap == 0)
+
+
+def afd(vel, nt, dt, d, nbt=30, ct=0.01, src=None, tri=False, dat=None, jsnap=0, gz=0,
+        precision="f32", rick=None):
+    """Run the afd propagator (fdm2d when vel is 2-D, fdm when 3-D).
+
+    vel: (nz,nx) or (nz,nx,ny).  d: (dz,dx) or (dz,dx,dy).
+    src: dict with sx, sz, [sy], f, t, A (forward mode).
+    dat: TRI traces, (nt,nx) or (nt,nx,ny) as afd2d/afd3d receive them.
+    rick: optional [ns][nt] wavelet table replacing the Ricker table.
+    Returns (traces (nt,nx[,ny]) or None, snapshots (nz,nx[,ny],ntsnap) or None).
+    """
+    vel = np.asarray(vel)
+    dim = vel.ndim
+    R = np.float32 if precision == "f32" else np.float64
+    fn = getattr(lib(), "or_afd_" + precision)
+    if dim == 2:
+        nz1, nx1 = vel.shape
+        ny1 = 1
+        dz, dx = d
+        dy = 1.0
+    else:
+        nz1, nx1, ny1 = vel.shape
+        dz, dx, dy = d
+    velf = np.ascontiguousarray(vel.astype(np.float32).flatten(order="F").astype(R))
+    if tri:
+        ns = 0
+        spz = spx = spy = np.zeros(1, np.int32)
+        rick = np.zeros(1, R)
+        datin = np.ascontiguousarray(np.asarray(dat, np.float32).flatten(order="F").astype(R))
+    else:
+        sx = np.asarray(src["sx"]).astype(np.float32).astype(np.int32)
+        sz = np.asarray(src["sz"]).astype(np.float32).astype(np.int32)
+        sy = np.asarray(src.get("sy", np.zeros_like(sx))).astype(np.float32).astype(np.int32)
+        ns = len(sx)
+        spz, spx, spy = (np.ascontiguousarray(a, dtype=np.int32) for a in (sz, sx, sy))
+        f = np.asarray(src["f"], np.float32)
+        t = np.asarray(src["t"], np.float32)
+        A = np.asarray(src["A"], np.float32)
+        if rick is None:
+            rick = np.stack([ricker(nt, dt, f[i], t[i], A[i]) for i in range(ns)])
+        rick = np.ascontiguousarray(np.asarray(rick).astype(np.float32).astype(R))
+        datin = np.zeros(1, R)
+    dout = np.zeros(nt * nx1 * ny1, R)
+    ntsnap = _ntsnap(nt, jsnap)
+    wfd = np.zeros(max(1, ntsnap * nz1 * nx1 * ny1), R)
+    rc = fn(dim, nz1, nx1, ny1, nbt, ct, dt, dz, dx, dy, nt, ns, spz, spx, spy, rick,
+            1 if tri else 0, datin, int(jsnap), int(gz), velf, dout,
+            wfd.ctypes.data if ntsnap > 0 else None)
+    if rc != 0:
+        raise MemoryError("oracle allocation failed")
+    traces = None
+    if not tri:
+        traces = dout.reshape((nt, nx1) if dim == 2 else (nt, nx1, ny1), order="F")
+    snaps = None
+    if ntsnap > 0:
+        shp = (nz1, nx1, ntsnap) if dim == 2 else (nz1, nx1, ny1, ntsnap)
+        snaps = wfd.reshape(shp, order="F")
+    return traces, snaps
+
+
+def tri_groups_image(snaps_per_group):
+    """The demos' TRI image (demos/test_third_tri.py:71-77,
+    demos/test_mod2d_tri_psVSfd.py:184-190): sum over snapshots of the
+    product over groups of the squared snapshot, divided by its maximum."""
+    img = 1
+    for s in snaps_per_group:
+        img = img * s * s
+    img = np.sum(img, axis=-1)
+    return img / img.max()
+
+
+def group_bands(nx: int, ng: int):
+    """Receiver groups of the TRI demos: x-bands of width nx//ng; columns
+    beyond ng*(nx//ng) belong to no group (demos/test_third_tri.py:63-66)."""
+    dg = nx // ng
+    return [np.arange(g * dg, g * dg + dg) for g in range(ng)]
+
+
+# --------------------------------------------------------------------------
+# pfwi (pywave/pfwi.py -> pfwi.c -> wave_fwi*.c)
+# --------------------------------------------------------------------------
+
+def pfwi_geometry(nz, nx, dz, dx, oz, ox, ns, ds, os_, nb, acqui_type=1, sz=5, rz=1):
+    """Resolved acquisition geometry of preparation (wave_fwiutil.c:44-71)
+    with the fixed settings of pfwi.c:796-801 (sz=5, rz=1, nr=nx, dr=dx,
+    r0=ox).  Float arithmetic in the reference's order."""
+    f32 = np.float32
+    dx32 = f32(dx)
+    ds_v = int(float(f32(ds) / dx32) + 0.5)
+    s0_v = int(float(f32(os_) / dx32) + 0.5 + nb)
+    nr = nx
+    dr = dx32
+    r0 = f32(ox)
+    x0 = f32(ox)
+    dr_v = int(float(dr / dx32) + 0.5)
+    sx = np.array([s0_v + i * ds_v for i in range(ns)], np.int32)
+    xend = f32(x0 + f32((nx - 1) * dx32))
+    r0v = np.zeros(ns, np.int32)
+    r02 = np.zeros(ns, np.int32)
+    nr2 = np.zeros(ns, np.int32)
+    for i in range(ns):
+        if acqui_type == 1:
+            r0v[i] = int(float((r0 - x0) / dx32) + 0.5 + nb)
+            r02[i] = 0
+            nr2[i] = nr
+        else:
+            sxf = f32(f32(os_) + f32(f32(ds) * i))
+            rbegin = x0 if f32(sxf + r0) < x0 else f32(sxf + r0)
+            rend = f32(f32(sxf + r0) + f32((nr - 1) * dr))
+            rend = rend if rend < xend else xend
+            r0v[i] = int(float(rbegin / dx32) + 0.5 + nb)
+            r02[i] = int(float(f32(f32(rbegin - sxf) - r0) / dx32) + 0.5)
+            nr2[i] = int(float(f32(rend - rbegin) / dx32) + 1.5)
+    return dict(sx=sx, sz=sz + nb, nr=nr, r0v=r0v, r02=r02, nr2=nr2, drv=dr_v, rz=rz + nb)
+
+
+def _geo_args(g, ns):
+    return (ns, g["sx"], g["sz"], g["nr"], g["r0v"], g["r02"], g["nr2"], g["drv"], g["rz"])
+
+
+def pfwi_forward(vel, wav, nb, coef, dz, dx, dt, geo, ns, precision="f32"):
+    """forward_modeling_a; vel (nz,nx); returns data (nt,nr,ns) like pfwi.py:74."""
+    R = np.float32 if precision == "f32" else np.float64
+    nz, nx = vel.shape
+    nt = len(wav)
+    v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F").astype(R))
+    w = np.ascontiguousarray(np.asarray(wav, np.float32).astype(R))
+    out = np.zeros(ns * geo["nr"] * nt, R)
+    getattr(lib(), "or_pfwi_forward_" + precision)(nz, nx, nb, dz, dx, nt, dt, coef,
+                                                   *_geo_args(geo, ns), v, w, out)
+    return out.reshape(nt, geo["nr"], ns, order="F")
+
+
+def residual_weights(nt, nr, wtn1=None, wtn2=None, woffn1=None, woffn2=None):
+    """residual_weighting (oreo=false) as fwic configures it; (nr,nt) C-order."""
+    w = np.zeros(nr * nt, np.float32)
+    lib().or_residual_weights(nt, nr, 0 if wtn1 is None else wtn1, nt - 1 if wtn2 is None else wtn2,
+                              0 if woffn1 is None else woffn1, nr - 1 if woffn2 is None else woffn2, w)
+    return w.reshape(nr, nt)
+
+
+def _dobs_flat(dobs, R):
+    # dobs (nt,nr,ns) F-order -> flat [ns][nr][nt]
+    return np.ascontiguousarray(np.asarray(dobs, np.float32).flatten(order="F").astype(R))
+
+
+def pfwi_gradient_ref(vel, wav, dobs, nb, coef, dz, dx, dt, geo, ns, interval=1, weight=None,
+                      precision="f32"):
+    """gradient_av before scaling/smoothing.  Returns (grad (nz,nx), fcost)."""
+    R = np.float32 if precision == "f32" else np.float64
+    nz, nx = vel.shape
+    nt = len(wav)
+    if weight is None:
+        weight = residual_weights(nt, geo["nr"])
+    v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F").astype(R))
+    w = np.ascontiguousarray(np.asarray(wav, np.float32).astype(R))
+    g = np.zeros(nz * nx, R)
+    f = getattr(lib(), "or_pfwi_gradient_ref_" + precision)(
+        nz, nx, nb, dz, dx, nt, dt, coef, interval, *_geo_args(geo, ns), v, w,
+        _dobs_flat(dobs, R), np.ascontiguousarray(np.asarray(weight, np.float32).astype(R)), g)
+    return g.reshape(nz, nx, order="F"), float(f)
+
+
+def pfwi_postprocess(grad, rect=3, scaling=None):
+    """gradient_av's tail (wave_fwigradient.c:244-255): first-call scaling
+    0.1/max|g| (float), triangle smoothing rect x rect, times the scale."""
+    g = np.ascontiguousarray(np.asarray(grad, np.float32).flatten(order="F"))
+    if scaling is None:
+        scaling = np.float32(0.1 / float(np.max(np.abs(g))))
+    nz, nx = grad.shape
+    lib().or_smooth2d(rect, rect, nz, nx, g)
+    g = g * np.float32(scaling)
+    return g.reshape(nz, nx, order="F"), scaling
+
+
+def pfwi_gradient_exact(vel, wav, dobs, nb, coef, dz, dx, dt, geo, ns, weight=None,
+                        precision="f64"):
+    """Exact discrete adjoint gradient dJ/dv and J (FP64 by default)."""
+    R = np.float32 if precision == "f32" else np.float64
+    nz, nx = vel.shape
+    nt = len(wav)
+    v = np.ascontiguousarray(np.asarray(vel, np.float64).flatten(order="F").astype(R))
+    w = np.ascontiguousarray(np.asarray(wav, np.float64).astype(R))
+    wt = None if weight is None else np.ascontiguousarray(np.asarray(weight).astype(R))
+    g = np.zeros(nz * nx, R)
+    J = getattr(lib(), "or_pfwi_gradient_exact_" + precision)(
+        nz, nx, nb, dz, dx, nt, dt, coef, *_geo_args(geo, ns), v, w,
+        _dobs_flat(dobs, R), None if wt is None else wt.ctypes.data, g)
+    return g.reshape(nz, nx, order="F"), float(J)
+
+
+def pfwi_misfit(vel, wav, dobs, nb, coef, dz, dx, dt, geo, ns, weight=None, precision="f64"):
+    R = np.float32 if precision == "f32" else np.float64
+    nz, nx = vel.shape
+    nt = len(wav)
+    v = np.ascontiguousarray(np.asarray(vel, np.float64).flatten(order="F").astype(R))
+    w = np.ascontiguousarray(np.asarray(wav, np.float64).astype(R))
+    wt = None if weight is None else np.ascontiguousarray(np.asarray(weight).astype(R))
+    return float(getattr(lib(), "or_pfwi_misfit_" + precision)(
+        nz, nx, nb, dz, dx, nt, dt, coef, *_geo_args(geo, ns), v, w, _dobs_flat(dobs, R),
+        None if wt is None else wt.ctypes.data))

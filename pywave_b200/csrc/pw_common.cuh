@@ -1,0 +1,136 @@
+// Shared internals of libpywave_b200: status handling, the per-device
+// workspace, exact-rounding float helpers and small host utilities.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <mutex>
+
+#include "../../include/pywave_b200.h"
+
+namespace pw {
+
+// ---------------------------------------------------------------- errors --
+void set_error(const char *fmt, ...);
+
+struct Status {
+  int code = PW_OK;
+  bool ok() const { return code == PW_OK; }
+};
+
+#define PW_CUDA(call)                                                         \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess) {                                                  \
+      ::pw::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #call,             \
+                      cudaGetErrorString(e_));                                \
+      return e_ == cudaErrorMemoryAllocation ? PW_ERR_OOM : PW_ERR_CUDA;      \
+    }                                                                         \
+  } while (0)
+
+#define PW_CHECK(cond, code, ...)                                             \
+  do {                                                                        \
+    if (!(cond)) {                                                            \
+      ::pw::set_error(__VA_ARGS__);                                           \
+      return (code);                                                          \
+    }                                                                         \
+  } while (0)
+
+#define PW_TRY(expr)                                                          \
+  do {                                                                        \
+    int rc_ = (expr);                                                         \
+    if (rc_ != PW_OK) return rc_;                                             \
+  } while (0)
+
+// ------------------------------------------------------------ workspace --
+// One grow-only device allocation per device, carved into 256-byte aligned
+// slices per call.  A call holds the device's lock from carve to its final
+// stream synchronisation, so concurrent calls serialise instead of aliasing.
+class Workspace {
+ public:
+  static Workspace &for_current_device();
+  // Reserve `bytes` (rounded); returns PW_OK or PW_ERR_OOM.
+  int reserve(size_t bytes);
+  char *base() const { return base_; }
+  void release();
+  std::mutex &mutex() { return mu_; }
+
+ private:
+  char *base_ = nullptr;
+  size_t cap_ = 0;
+  std::mutex mu_;
+};
+
+// Builds a slice layout first (sizes), then binds to the workspace base.
+class Carve {
+ public:
+  size_t add(size_t bytes) {
+    size_t off = total_;
+    total_ += (bytes + 255) & ~size_t(255);
+    return off;
+  }
+  size_t total() const { return total_; }
+
+ private:
+  size_t total_ = 0;
+};
+
+template <class T>
+inline T *at(char *base, size_t off) { return reinterpret_cast<T *>(base + off); }
+
+// ------------------------------------------------------------- helpers ----
+inline int ceil_div(long long a, long long b) { return int((a + b - 1) / b); }
+inline long long round_up(long long a, long long b) { return (a + b - 1) / b * b; }
+
+// kiss_fft_next_fast_size (pywave/src/wave_kissfft.c:412-424): the smallest
+// n' >= n with no prime factor other than 2, 3, 5.
+int next_fast(int n);
+// First-axis padding of fft2_init/fft3_init with cmplx=0, pad1=1
+// (pywave/src/wave_fft2.c:45-46): 2*next_fast((n+1)/2).
+inline int pad_first(int n) { return 2 * next_fast((n + 1) / 2); }
+
+// The Ricker table of fdm2d/fdm (pywave/src/wave_fdm.c:502-516; shape
+// wave_ricker.c:22-58; zero-phase filter wave_freqfilt.c:76-99), evaluated as
+// the closed-form cosine sum of the spike's filtered spectrum in double, with
+// the spectral shape samples rounded to float as the reference stores them.
+void ricker_table(int nt, float dt, float f0, float t0, float A, float *out);
+
+// Per-thread record of the last call's device timing (pw_last_timing).
+struct Timing {
+  double loop_ms = 0;
+  long long step_launches = 0;
+  long long total_launches = 0;
+};
+Timing &timing();
+// RAII pair of CUDA events bracketing a time loop on a stream.
+class LoopTimer {
+ public:
+  explicit LoopTimer(cudaStream_t s);
+  ~LoopTimer();
+  void start();
+  void stop();
+  // Synchronises on the stop event and stores the elapsed time in timing().
+  void finish(long long step_launches, long long total_launches);
+
+ private:
+  cudaStream_t s_;
+  cudaEvent_t a_ = nullptr, b_ = nullptr;
+};
+
+// Copy helper honouring PW_HOST_PTRS.
+int to_device(void *dst, const void *src, size_t bytes, bool host, cudaStream_t s);
+int to_host(void *dst, const void *src, size_t bytes, bool host, cudaStream_t s);
+
+}  // namespace pw
+
+// ------------------------------------------------- device-side helpers ----
+// Explicitly rounded float ops: the parity-critical expressions are written
+// with these so that nvcc never contracts a*b+c into an FMA, which keeps the
+// evaluation order (and rounding) of the reference's C code.
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }

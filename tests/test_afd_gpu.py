@@ -1,0 +1,166 @@
+"""Parity of the CUDA afd path (K1/K2/K3) against the reference's golden vectors
+and the oracle restatement.  GPU only; every call goes through the C ABI."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _kw(g, keys=("nt", "dt", "ns", "sx", "sz", "f", "t", "A", "nbt", "ct", "jsnap")):
+    out = {}
+    for k in keys:
+        v = g[k]
+        out[k] = v.tolist() if v.ndim else v.item()
+    return out
+
+
+def test_afd2d_bit_exact_vs_reference(golden, cuda_lib):
+    import pywave_b200 as pw
+    g = golden("afd2d_fwd")
+    kw = _kw(g)
+    d, w = pw.afd2d(g["vel"], ax=[0, 20, 51], az=[0, 20, 41], wavelet=g["rick"], **kw)
+    assert np.array_equal(d, g["traces"])
+    assert np.array_equal(w, g["snaps"])
+
+
+def test_afd2d_own_wavelet(golden, oracle, cuda_lib):
+    import pywave_b200 as pw
+    g = golden("afd2d_fwd")
+    kw = _kw(g)
+    d, w = pw.afd2d(g["vel"], ax=[0, 20, 51], az=[0, 20, 41], **kw)
+    assert rel_l2(d, g["traces"]) < 1e-5
+    src = dict(sx=g["sx"], sz=g["sz"], f=g["f"], t=g["t"], A=g["A"])
+    to, so = oracle.afd(g["vel"], kw["nt"], kw["dt"], (20., 20.), nbt=30, ct=0.01, src=src, jsnap=3)
+    assert np.array_equal(d, to) and np.array_equal(w, so)
+
+
+def test_afd2d_tri_bit_exact(golden, cuda_lib):
+    import pywave_b200 as pw
+    g = golden("afd2d_tri")
+    echo, w = pw.afd2d(g["vel"], nt=g["dat"].shape[0], dt=0.001, ax=[0, 20, 51], az=[0, 20, 41],
+                       jsnap=4, dat=g["dat"], tri=True, nbt=30, ct=0.01)
+    assert np.array_equal(echo, g["dat"])
+    assert np.array_equal(w, g["snaps"])
+
+
+def test_afd3d_bit_exact_vs_reference(golden, cuda_lib):
+    import pywave_b200 as pw
+    g = golden("afd3d_fwd")
+    kw = _kw(g, ("nt", "dt", "ns", "sx", "sy", "sz", "f", "t", "A", "nbt", "ct", "jsnap"))
+    d, w = pw.afd3d(g["vel"], ax=[0, 20, 20], ay=[0, 20, 22], az=[0, 20, 24], wavelet=g["rick"], **kw)
+    assert np.array_equal(d, g["traces"])
+    assert np.array_equal(w, g["snaps"])
+
+
+def test_afd3d_tri_bit_exact(golden, cuda_lib):
+    import pywave_b200 as pw
+    g = golden("afd3d_tri")
+    _, w = pw.afd3d(g["vel"], nt=g["dat"].shape[0], dt=0.001, ax=[0, 20, 20], ay=[0, 20, 22],
+                    az=[0, 20, 24], jsnap=4, dat=g["dat"], tri=True, nbt=8, ct=0.02)
+    assert np.array_equal(w, g["snaps"])
+
+
+def test_config1_gather_depth5(golden, oracle, cuda_lib):
+    """201x201 three-layer model, 20 Hz source at
+    (z=5, x=100), receivers at z=5 on every x, nt=1501.  Bit-exact against
+    the reference given its wavelet; <= 1e-5 with the closed-form Ricker; the
+    error of both against the FP64 oracle is stated."""
+    import pywave_b200 as pw
+    g = golden("c1_gather_z5")
+    vel = np.full((201, 201), 1500, np.float32)
+    vel[60:] = 2200
+    vel[130:] = 3000
+    kw = dict(nt=1501, dt=0.001, ax=[0, 10, 201], az=[0, 10, 201], ns=1, sx=[100], sz=[5], f=[20],
+              t=[0.05], A=[1], nbt=30, ct=0.01, jsnap=0, gz=5)
+    d_ref_wav = pw.afd2d(vel, wavelet=g["rick"], **kw)
+    assert np.array_equal(d_ref_wav, g["gather"])
+    d = pw.afd2d(vel, **kw)
+    assert rel_l2(d, g["gather"]) < 1e-5
+    src = dict(sx=[100], sz=[5], f=[20], t=[0.05], A=[1])
+    d64, _ = oracle.afd(vel, 1501, 0.001, (10., 10.), src=src, gz=5, precision="f64")
+    e_gpu, e_ref = rel_l2(d, d64), rel_l2(g["gather"], d64)
+    print(f"config1: rel-L2 vs FP64 oracle: gpu {e_gpu:.3e}, reference {e_ref:.3e}")
+    assert e_gpu < 1e-4 and e_ref < 1e-4
+
+
+@pytest.mark.parametrize("dim,ng", [(2, 1), (2, 3), (2, 4), (3, 2), (3, 4)])
+def test_tri_image_matches_per_group_runs(oracle, cuda_lib, dim, ng):
+    """The fused lockstep image equals the demos' image built from ng separate
+    time-reversal runs (oracle, FP32)."""
+    import pywave_b200 as pw
+    rng = np.random.default_rng(dim * 10 + ng)
+    if dim == 2:
+        vel = np.full((37, 45), 2000, np.float32)
+        vel[18:] = 2600
+        src = dict(sx=[22], sz=[20], f=[12], t=[0.05], A=[1])
+        d, _ = oracle.afd(vel, 260, 0.001, (20., 20.), nbt=12, ct=0.02, src=src)
+        spacing = (20., 20.)
+    else:
+        vel = (2200 + 200 * rng.random((18, 21, 19))).astype(np.float32)
+        src = dict(sx=[10], sy=[9], sz=[11], f=[15], t=[0.04], A=[1])
+        d, _ = oracle.afd(vel, 140, 0.001, (20., 20., 20.), nbt=8, ct=0.02, src=src)
+        spacing = (20., 20., 20.)
+    nt, nx = d.shape[0], d.shape[1]
+    snaps = []
+    groups = pw.group_bands(nx, ng, 1 if dim == 2 else vel.shape[2])
+    for gi in range(ng):
+        mask = (groups == gi).T  # [nx, ny]
+        dg = d * (mask[None, :, 0] if dim == 2 else mask[None, :, :])
+        _, s = oracle.afd(vel, nt, 0.001, spacing, nbt=12 if dim == 2 else 8, ct=0.02, tri=True,
+                          dat=dg, jsnap=4)
+        snaps.append(s)
+    ref = oracle.tri_groups_image(snaps)
+    img = pw.tri_image(vel, d, dt=0.001, d=spacing, ngroups=ng, nbt=12 if dim == 2 else 8,
+                       ct=0.02, jsnap=4)
+    assert rel_l2(img, ref) < 1e-5
+
+
+def test_device_pointer_path(golden, cuda_lib):
+    """Same call with inputs resident in HBM (torch tensors, no PW_HOST_PTRS)."""
+    import torch
+    from pywave_b200 import _lib as L
+    g = golden("afd2d_fwd")
+    vel = torch.tensor(g["vel"].flatten(order="F"), device="cuda")
+    src = np.concatenate([g["sx"], g["sz"], g["f"], g["t"], g["A"]]).astype(np.float32)
+    src_d = torch.tensor(src, device="cuda")
+    wav = torch.tensor(g["rick"], device="cuda")
+    nt, nx = g["traces"].shape
+    dat = torch.empty(nt * nx, device="cuda")
+    a = L.AfdArgs(dim=2, nz=41, nx=51, ny=1, nt=nt, nbt=30, ct=0.01, dt=0.001, dz=20, dx=20, dy=1,
+                  ns=2, tri=0, jsnap=0, gz=0, flags=0)
+    s = torch.cuda.current_stream().cuda_stream
+    L.check(L.lib().pw_afd(a, vel.data_ptr(), src_d.data_ptr(), wav.data_ptr(), dat.data_ptr(),
+                           None, s))
+    out = dat.cpu().numpy().reshape(nt, nx, order="F")
+    assert np.array_equal(out, g["traces"])
+
+
+@pytest.mark.parametrize("nz,nx", [(1, 1), (3, 5), (7, 130), (64, 3), (33, 33)])
+def test_ragged_sizes_match_oracle(oracle, cuda_lib, nz, nx):
+    import pywave_b200 as pw
+    rng = np.random.default_rng(nz * 1000 + nx)
+    vel = (1800 + 600 * rng.random((nz, nx))).astype(np.float32)
+    src = dict(sx=[nx // 2], sz=[nz // 2], f=[15], t=[0.02], A=[1])
+    d, w = pw.afd2d(vel, nt=90, dt=0.001, ax=[0, 15, nx], az=[0, 15, nz], ns=1, sx=[nx // 2],
+                    sz=[nz // 2], f=[15], t=[0.02], A=[1], nbt=5, ct=0.05, jsnap=7)
+    to, so = oracle.afd(vel, 90, 0.001, (15., 15.), nbt=5, ct=0.05, src=src, jsnap=7)
+    assert np.array_equal(d, to) and np.array_equal(w, so)
+
+
+def test_errors_are_raised_before_launch(cuda_lib):
+    import pywave_b200 as pw
+    from pywave_b200 import _lib as L
+    vel = np.full((20, 20), 2000, np.float32)
+    with pytest.raises(L.CFLError):
+        pw.afd2d(vel, nt=10, dt=0.01, ax=[0, 10, 20], az=[0, 10, 20], ns=1, sx=[5], sz=[5],
+                 f=[10], t=[0.0], A=[1], jsnap=0)
+    bad = vel.copy()
+    bad[3, 3] = np.nan
+    with pytest.raises(ValueError):
+        pw.afd2d(bad, nt=10, ax=[0, 10, 20], az=[0, 10, 20], ns=1, sx=[5], sz=[5], f=[10],
+                 t=[0.0], A=[1], jsnap=0)
+    with pytest.raises(ValueError):
+        pw.afd2d(vel, nt=10, ax=[0, 10, 20], az=[0, 10, 20], ns=1, sx=[25], sz=[5], f=[10],
+                 t=[0.0], A=[1], jsnap=0)
