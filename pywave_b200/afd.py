@@ -113,6 +113,7 @@ def tri_image(vel, dat, dt=0.001, d=None, ngroups=4, groups=None, nbt=30, ct=0.0
         groups = group_bands(nx, ngroups, ny)
     groups = np.ascontiguousarray(np.asarray(groups, np.int32).reshape(ny, nx))
     img = np.empty(nz * nx * ny, np.float32)
-    L.check(L.lib().pw_tri_image(a, int(ngroups), L.ptr(groups), L.ptr(vel.flatten(order="F")),
-                                 L.ptr(src), L.ptr(img), 1 if normalize else 0, None))
+    vflat = np.ascontiguousarray(vel.flatten(order="F"))  # keep alive across the call
+    L.check(L.lib().pw_tri_image(a, int(ngroups), L.ptr(groups), L.ptr(vflat), L.ptr(src),
+                                 L.ptr(img), 1 if normalize else 0, None))
     return img.reshape((nz, nx) if dim == 2 else (nz, nx, ny), order="F")
