@@ -51,7 +51,7 @@ def parse():
 NBT, CT, H, DT = 30, 0.01, 10.0, 0.001
 
 
-def c2_model(n, seed):
+def c2_model(n, seed, nt=1501):
     """Velocity 1500 -> 3000 m/s linear in z plus a 5% seeded perturbation
     (N(0,1) field, Gaussian-smoothed sigma=5 points, scaled to +-5%)."""
     from scipy.ndimage import gaussian_filter
@@ -65,6 +65,7 @@ def c2_model(n, seed):
     pos = rng.integers(lo, hi, size=(3, 3))  # (sx, sy, sz) per source
     f = rng.uniform(15, 25, 3)
     t = rng.uniform(0.1, 0.5, 3)
+    t = np.minimum(t, 0.5 * (nt - 1) * DT)  # short profiling runs keep the onsets inside nt
     return vel, pos, f, t
 
 
@@ -228,7 +229,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     stream = torch.cuda.current_stream().cuda_stream
     n, nt, G = args.n, args.nt, args.groups
-    vel, pos, f, t = c2_model(n, 1234 + rank)
+    vel, pos, f, t = c2_model(n, 1234 + rank, nt)
     vel_d, dat_d = gen_traces(vel, pos, f, t, nt, stream)
     groups = np.ascontiguousarray(np.tile(np.where(np.arange(n) // (n // G) < G,
                                                    np.arange(n) // (n // G), -1), (n, 1)).astype(np.int32))

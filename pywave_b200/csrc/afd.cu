@@ -3,19 +3,33 @@
 //   4th-order Laplacian -> leapfrog -> injection -> double taper ->
 //   receiver sampling -> snapshot / image accumulation
 // of the reference's fdm2d / fdm time loop (pywave/src/wave_fdm.c:551-662,
-// 209-354) with its exact float evaluation order.
+// 209-354) with its exact float evaluation order (no FMA contraction).
 //
-// Device layout ("field layout"): every field is a zero-haloed array
-//   off(iz,ix,iy) = (iz + HZ) + lz*(ix + hx) + sy*(iy + hy),
-// z fastest, lz a multiple of 32 floats, so each thread owns one aligned
-// float4 of 4 consecutive z cells.  The halo cells are never written and stay
-// zero, which reproduces the reference's zero border beyond the expanded grid.
+// Kernel axes.  z is contiguous; x is the tile axis; y is the marched axis.
+// 3-D maps (z,x,y) to the model's (z,x,y).  2-D maps the model's x to the
+// marched axis y and uses a dummy x axis of extent 1, so one kernel serves
+// both.  Field layout: a zero-haloed array
+//   off(iz,ix,iy) = (iz + HZ) + sx*(ix + hx) + sy*(iy + hy),
+// leading dimension a multiple of 32 floats; each thread owns one aligned
+// float4 of 4 consecutive z cells.  Halo cells are never written and stay
+// zero: that is the reference's zero border beyond the expanded grid.
+//
+// Data movement.  A CTA owns a z-x tile (ZW float4 x TX columns) and marches
+// it along y.  Each plane's tile (with a 1-float4 z halo and 2-column x halo),
+// the previous wavefield and vv are staged in shared memory by cp.async
+// 16-byte copies, P planes ahead of the plane being updated; the y neighbours
+// of a cell come from a 5-deep register queue.  Receiver groups of a TRI
+// image are processed one after another inside the CTA (one register queue
+// live at a time); at imaging steps the last group reads the other groups'
+// fresh values back (written by the same thread moments earlier, so L2 hits)
+// and accumulates prod_g u_g^2.
 //
 // Two buffers per wavefield: at step k the kernel reads A = u_k and B =
 // u_{k-1} (as stored, tapered once) and overwrites B with u_{k+1}.  The
 // reference's `prev` array is taper(u_{k-1}) (wave_fdm.c:595-597,633-636); it
-// is recomputed on the fly from B with the same multiplications, so the scheme
-// moves 16 bytes per point update (read A, B, vv; write B).
+// is recomputed on the fly from B with the same multiplications, so one
+// group-point update moves 16 bytes (read A, B, vv; write B), vv shared by
+// all groups.
 #include "pw_common.cuh"
 
 #include <algorithm>
@@ -25,48 +39,46 @@ namespace pw {
 namespace afd {
 
 constexpr int HZ = 4;       // z halo (cells) in front of iz = 0
-constexpr int MAXG = 4;     // receiver groups propagated in lockstep per launch
+constexpr int MAXG = 8;     // receiver groups per lockstep launch
 constexpr int MAXSRC = 16;  // point sources resolved inside the kernel
 
 struct Geo {
-  int nz, nx, ny;                    // expanded extents (interior + 2*nbt)
-  int lz, px, py;                    // allocation: leading dim, x extent, y extent
+  int nz, nx, ny;                    // extents in kernel axes
+  int lz;                            // leading dimension (floats)
+  long long sx, sy;                  // x / y strides (floats)
   int hx, hy;                        // x / y halo widths
-  long long sy;                      // y-plane stride = lz*px
+  int py;                            // allocated y extent (ny + 2*hy)
   int lz0, lz1, lx0, lx1, ly0, ly1;  // Laplacian is non-zero on [lo,hi) per axis
 };
 
 __host__ __device__ inline long long foff(const Geo &g, int iz, int ix, int iy) {
-  return (long long)(iz + HZ) + (long long)g.lz * (ix + g.hx) + g.sy * (iy + g.hy);
+  return (long long)(iz + HZ) + g.sx * (ix + g.hx) + g.sy * (iy + g.hy);
 }
 
 struct StepArgs {
   Geo g;
-  int tz4, tx, ych;  // tile: float4 columns along z, columns along x, planes per CTA along y
+  int ych;  // planes per CTA along y
+  int ngroups;
   float c0, c1, c2, idx, idy, idz, k0;
   const float *cur[MAXG];
   float *nxt[MAXG];
   const float *vv;
-  const float *wz1, *wz2, *wx1, *wx2, *wy1, *wy2;  // taper factors (1 outside the faces)
+  // taper factor per cell along each axis: the top/left face weight, the
+  // bottom/right one, or 1 (faces of one axis are disjoint, and x*1 is exact,
+  // so one product per axis equals abc_apply's face-by-face products)
+  const float *wz, *wx, *wy;
   int it, nt;
   int ns;
   int sz[MAXSRC], sx[MAXSRC], sy[MAXSRC];
   const float *rick;  // [ns][nt]
-  int rz, rx0, ry0, nrx, nry;
-  const float *tri_dat;  // [nt][nry][nrx]
-  const int *gid;        // [nry][nrx] or null: every receiver feeds group 0
-  float *rec;            // forward traces [nt][nry][nrx] or null
-  int nb, nz1, nx1, ny1, nby;
-  float *wfd;            // this step's snapshot [ny1][nx1][nz1] (group 0) or null
-  float *img;            // image accumulator (field layout) or null
+  int rz, rx0, ry0, nrx, nry;  // receivers: row rz, x in [rx0,rx0+nrx), y in [ry0,ry0+nry)
+  const float *tri_dat;        // [nt][nry][nrx]
+  const int *gid;              // [nry][nrx] or null: every receiver feeds group 0
+  float *rec;                  // forward traces [nt][nry][nrx] or null
+  int nbz, nbx, nby, nz1, nx1, ny1;  // interior = [nb, nb+n1) per kernel axis
+  float *wfd;                  // this step's snapshot [ny1][nx1][nz1] (group 0) or null
+  float *img;                  // image accumulator (field layout) or null
 };
-
-__device__ __forceinline__ float4 ld4(const float *base, const Geo &g, int z4, int ix, int iy) {
-  if (z4 < -1 || z4 * 4 >= g.nz || ix < -g.hx || ix >= g.nx + g.hx || iy < -g.hy ||
-      iy >= g.ny + g.hy)
-    return make_float4(0.f, 0.f, 0.f, 0.f);
-  return __ldg(reinterpret_cast<const float4 *>(base + foff(g, z4 * 4, ix, iy)));
-}
 
 __device__ __forceinline__ float el(const float4 &v, int e) {
   return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
@@ -75,191 +87,313 @@ __device__ __forceinline__ void set_el(float4 &v, int e, float x) {
   if (e == 0) v.x = x; else if (e == 1) v.y = x; else if (e == 2) v.z = x; else v.w = x;
 }
 
-template <int DIM, int G, bool TRI>
-__global__ void __launch_bounds__(DIM == 3 ? 256 : 512) step_kernel(const StepArgs a) {
-  extern __shared__ float4 smem[];
-  const Geo &g = a.g;
-  const int tz4 = a.tz4, tx = a.tx;
-  const int W = tz4 + 2;
-  const int plane4 = W * (tx + 4);
-  const int tid = threadIdx.x;
-  const int zl = tid % tz4, xl = tid / tz4;
-  const int z4 = blockIdx.x * tz4 + zl;
-  const int iz0 = z4 * 4;
-  const int ix = blockIdx.y * tx + xl;
-  const bool live = (iz0 < g.nz) && (ix < g.nx);
-  const int y_begin = DIM == 3 ? blockIdx.z * a.ych : 0;
-  const int y_end = DIM == 3 ? min(g.ny, y_begin + a.ych) : 1;
-  const int nh = 4 * W + 2 * tx;
+// 16-byte global -> shared async copy; src_bytes = 0 zero-fills the slot.
+__device__ __forceinline__ void cp16(float4 *dst, const float *src, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(n)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-  float wz1[4], wz2[4];
-  bool lzok[4];
+// Per-thread constants of a tile column (z float4 x one x column).
+struct Col {
+  float wz[4];     // z taper factor per cell (1 outside the faces)
+  float wx;        // x taper factor
+  bool lz[4];      // Laplacian non-zero along z
+  bool lx;         // ... along x
+  int iz0, ix;
+};
+
+// Leapfrog update of one float4 of cells, in the reference's float order:
+//   wave = c0*u*k0 + c1*(y-1+y+1)*idy + c2*(y-2+y+2)*idy [+ x terms] + z terms
+//   u_new = (u + (u - taper(u_prev))) + wave*vv  [+ injection]  then taper.
+// MASKED handles the grid edges (Laplacian masks, cells past nz), receiver
+// rows and source cells; the plain path is branch-free.
+template <bool TWO_D, bool TRI, bool MASKED>
+__device__ __forceinline__ float4 update4(const StepArgs &a, const Col &col, int y, int gi,
+                                          bool lyok, bool taper, float wy, bool rec_here,
+                                          int r_idx, bool src_plane, const float4 &c,
+                                          const float4 &L, const float4 &R, const float4 &xm1,
+                                          const float4 &xp1, const float4 &xm2, const float4 &xp2,
+                                          const float4 &q0, const float4 &q1, const float4 &q3,
+                                          const float4 &q4, const float4 &pv, const float4 &vv4) {
+  float4 res;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const float cv = el(c, e);
+    const float zm1 = e == 0 ? L.w : el(c, e - 1);
+    const float zp1 = e == 3 ? R.x : el(c, e + 1);
+    const float zm2 = e == 0 ? L.z : (e == 1 ? L.w : el(c, e - 2));
+    const float zp2 = e == 2 ? R.x : (e == 3 ? R.y : el(c, e + 2));
+    float t = fmul(fmul(a.c0, cv), a.k0);
+    t = fadd(t, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
+    t = fadd(t, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
+    if (!TWO_D) {
+      t = fadd(t, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
+      t = fadd(t, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
+    }
+    t = fadd(t, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
+    t = fadd(t, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
+    float lap = t;
+    if (MASKED) lap = (col.lz[e] && col.lx && lyok) ? t : 0.f;
+    // prev = taper(u_{k-1} as stored)
+    float p = el(pv, e);
+    if (taper) {
+      p = fmul(p, col.wz[e]);
+      if (!TWO_D) p = fmul(p, col.wx);
+      p = fmul(p, wy);
+    }
+    const float vve = el(vv4, e);
+    float v = fadd(cv, fsub(cv, p));
+    v = fadd(v, fmul(lap, vve));
+    if (MASKED) {
+      const int iz = col.iz0 + e;
+      if (TRI) {
+        if (rec_here && iz == a.rz && (a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi))
+          v = fadd(v, fmul(vve, a.tri_dat[(size_t)a.it * a.nrx * a.nry + r_idx]));
+      } else if (src_plane) {
+        for (int s = 0; s < a.ns; s++) {
+          const int dz = iz - a.sz[s], dxs = TWO_D ? 0 : col.ix - a.sx[s], dys = y - a.sy[s];
+          if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
+            const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
+            v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
+          }
+        }
+      }
+    }
+    if (taper) {
+      v = fmul(v, col.wz[e]);
+      if (!TWO_D) v = fmul(v, col.wx);
+      v = fmul(v, wy);
+    }
+    if (MASKED && col.iz0 + e >= a.g.nz) v = 0.f;
+    set_el(res, e, v);
+  }
+  return res;
+}
+
+// TWO_D: dummy x axis (no x stencil terms, no x taper).
+// ZW: float4 columns along z per tile; TX: x columns per tile; P: prefetch depth.
+template <bool TWO_D, int ZW, int TX, int P, bool TRI>
+__global__ void __launch_bounds__(ZW *TX, TWO_D ? 1 : (ZW * TX >= 256 ? 2 : 3))
+    step_kernel(const StepArgs a) {
+  constexpr int NT = ZW * TX;
+  constexpr int W = ZW + 2;                 // smem row (float4) incl. z halo
+  constexpr int ROWS = TWO_D ? 1 : TX + 4;  // smem rows incl. x halo
+  constexpr int XH = TWO_D ? 0 : 2;         // x halo rows on each side
+  constexpr int CPL = W * ROWS;             // curr plane (float4)
+  constexpr int PPL = ZW * TX;              // prev / vv plane (float4)
+  // Slot reuse: the copy for plane i+P+4 is issued in iteration i, while
+  // other threads may still read planes i+1..i+4 (and planes 0..3 in
+  // iteration 0, for the queue); P+6 slots keep the writes clear of them.
+  constexpr int NC = P + 6;                 // curr planes in flight
+  constexpr int NP = P + 2;                 // prev / vv planes in flight
+  constexpr int NH = TWO_D ? 2 : (4 * ZW + 2 * TX);
+  constexpr int HK = (NH + NT - 1) / NT;
+  static_assert(TWO_D || ZW % 8 == 0, "3-D tiles need ZW % 8 == 0");
+  extern __shared__ float4 sm[];
+  float4 *s_cur = sm;
+  float4 *s_prev = sm + NC * CPL;
+  float4 *s_vv = s_prev + NP * PPL;
+
+  const Geo &g = a.g;
+  const int tid = threadIdx.x;
+  const int zl = TWO_D ? tid : (tid & 7) + 8 * (tid / (8 * TX));
+  const int xl = TWO_D ? 0 : (tid >> 3) % TX;
+  const int zt0 = blockIdx.z * ZW, xt0 = blockIdx.y * TX;
+  const int z4 = zt0 + zl;
+  Col col;
+  col.iz0 = 4 * z4;
+  col.ix = xt0 + xl;
+  const int iz0 = col.iz0, ix = col.ix;
+  const int y0 = blockIdx.x * a.ych;
+  const int y1 = min(g.ny, y0 + a.ych);
+  const int nplanes = y1 - y0;
+  const bool live = iz0 < g.nz && ix < g.nx;
+  const bool zx_ok = iz0 < g.nz && ix < g.nx + g.hx;  // the centre float4 is stored
+  const long long o_c = foff(g, iz0, ix, 0);
+  const int ci = (xl + XH) * W + zl + 1;  // centre slot in a curr plane
+  const int pi = xl * ZW + zl;            // slot in a prev / vv plane
+
+  // halo items of this thread: smem slot and global offset at y = 0
+  int h_slot[HK];
+  long long h_off[HK];
+  bool h_ok[HK];
+#pragma unroll
+  for (int k = 0; k < HK; k++) {
+    const int h = tid + k * NT;
+    int r = 0, c = 0;
+    if (h < NH) {
+      if (TWO_D) {
+        c = h == 0 ? 0 : ZW + 1;
+      } else if (h < 4 * ZW) {
+        const int rr = h / ZW;
+        r = rr < 2 ? rr : TX + rr;
+        c = 1 + h % ZW;
+      } else {
+        const int h2 = h - 4 * ZW;
+        r = 2 + (h2 >> 1);
+        c = (h2 & 1) ? ZW + 1 : 0;
+      }
+    }
+    const int z4g = zt0 + c - 1, xg = xt0 + r - XH;
+    h_slot[k] = h < NH ? r * W + c : -1;
+    h_ok[k] = h < NH && z4g >= -1 && z4g * 4 < g.nz && xg >= -g.hx && xg < g.nx + g.hx;
+    h_off[k] = h_ok[k] ? foff(g, z4g * 4, xg, 0) : 0;
+  }
+
+  bool zx_taper = false, lz_all = true;
 #pragma unroll
   for (int e = 0; e < 4; e++) {
     const int iz = iz0 + e;
-    const bool in = live && iz < g.nz;
-    wz1[e] = in ? a.wz1[iz] : 1.f;
-    wz2[e] = in ? a.wz2[iz] : 1.f;
-    lzok[e] = iz >= g.lz0 && iz < g.lz1;
+    col.wz[e] = (live && iz < g.nz) ? a.wz[iz] : 1.f;
+    zx_taper |= col.wz[e] != 1.f;
+    col.lz[e] = iz >= g.lz0 && iz < g.lz1;
+    lz_all &= col.lz[e];
   }
-  const float wx1 = live ? a.wx1[ix] : 1.f, wx2 = live ? a.wx2[ix] : 1.f;
-  const bool lxok = ix >= g.lx0 && ix < g.lx1;
-  const bool rec_x = ix >= a.rx0 && ix < a.rx0 + a.nrx;
-  const bool rec_z = a.rz >= iz0 && a.rz < iz0 + 4;
+  col.wx = (!TWO_D && live) ? a.wx[ix] : 1.f;
+  zx_taper |= col.wx != 1.f;
+  col.lx = TWO_D || (ix >= g.lx0 && ix < g.lx1);
+  const bool plain_zx = lz_all && col.lx && iz0 + 3 < g.nz;
+  const bool rec_zx = (a.rz >= iz0 && a.rz < iz0 + 4) && ix >= a.rx0 && ix < a.rx0 + a.nrx;
+  const bool in_zx = ix >= a.nbx && ix < a.nbx + a.nx1;
+  const bool img_step = a.img != nullptr;
 
-  float4 q[G][5];
+  for (int gi = 0; gi < a.ngroups; gi++) {
+    const float *cur = a.cur[gi];
+    float *nxt = a.nxt[gi];
+    const bool last = gi == a.ngroups - 1;
+    // curr plane k <-> y = y0 - 2 + k; prev/vv plane j <-> y = y0 + j
+    auto issue_cur = [&](int k) {
+      const int y = y0 - 2 + k;
+      const bool yok = y >= -g.hy && y < g.ny + g.hy;
+      float4 *dst = s_cur + (k % NC) * CPL;
+      const long long oy = g.sy * (long long)y;
+      cp16(dst + ci, cur + (zx_ok && yok ? o_c + oy : 0), zx_ok && yok);
 #pragma unroll
-  for (int gi = 0; gi < G; gi++)
+      for (int q = 0; q < HK; q++)
+        if (h_slot[q] >= 0)
+          cp16(dst + h_slot[q], cur + (h_ok[q] && yok ? h_off[q] + oy : 0), h_ok[q] && yok);
+    };
+    auto issue_pv = [&](int j) {
+      const long long o = o_c + g.sy * (long long)(y0 + j);
+      cp16(s_prev + (j % NP) * PPL + pi, live ? nxt + o : nxt, live);
+      cp16(s_vv + (j % NP) * PPL + pi, live ? a.vv + o : a.vv, live);
+    };
+    for (int k = 0; k < 4; k++) issue_cur(k);
 #pragma unroll
-    for (int k = 0; k < 5; k++) q[gi][k] = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (DIM == 3) {
-#pragma unroll
-    for (int gi = 0; gi < G; gi++)
-#pragma unroll
-      for (int k = 0; k < 4; k++) q[gi][k] = ld4(a.cur[gi], g, z4, ix, y_begin - 2 + k);
-  }
-
-  int parity = 0;
-  for (int y = y_begin; y < y_end; y++, parity ^= 1) {
-    float4 *buf = smem + parity * G * plane4;
-#pragma unroll
-    for (int gi = 0; gi < G; gi++) {
-      if (DIM == 3) q[gi][4] = ld4(a.cur[gi], g, z4, ix, y + 2);
-      else q[gi][2] = ld4(a.cur[gi], g, z4, ix, y);
-      buf[gi * plane4 + (xl + 2) * W + zl + 1] = q[gi][2];
-    }
-    for (int h = tid; h < nh; h += blockDim.x) {
-      int r, c;
-      if (h < 4 * W) {
-        const int rr = h / W;
-        r = rr < 2 ? rr : tx + rr;
-        c = h % W;
-      } else {
-        const int h2 = h - 4 * W;
-        r = 2 + (h2 >> 1);
-        c = (h2 & 1) ? tz4 + 1 : 0;
+    for (int b = 0; b < P; b++) {
+      if (b < nplanes) {
+        issue_cur(b + 4);
+        issue_pv(b);
       }
-      const int z4g = blockIdx.x * tz4 + c - 1;
-      const int xg = blockIdx.y * tx + r - 2;
-#pragma unroll
-      for (int gi = 0; gi < G; gi++) buf[gi * plane4 + r * W + c] = ld4(a.cur[gi], g, z4g, xg, y);
+      cp_commit();
     }
-    float4 pv[G];
-    float4 vvv = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (live) {
-#pragma unroll
-      for (int gi = 0; gi < G; gi++)
-        pv[gi] = *reinterpret_cast<const float4 *>(a.nxt[gi] + foff(g, iz0, ix, y));
-      vvv = ld4(a.vv, g, z4, ix, y);
-    }
-    __syncthreads();
-    if (live) {
-      const bool lyok = DIM == 2 || (y >= g.ly0 && y < g.ly1);
-      const float wy1 = DIM == 3 ? a.wy1[y] : 1.f, wy2 = DIM == 3 ? a.wy2[y] : 1.f;
-      const long long o = foff(g, iz0, ix, y);
-      const bool rec_here = rec_z && rec_x && (DIM == 2 || (y >= a.ry0 && y < a.ry0 + a.nry));
-      const int r_idx = rec_here ? (DIM == 3 ? (y - a.ry0) * a.nrx : 0) + (ix - a.rx0) : 0;
-      const bool interior = (ix >= a.nb && ix < a.nb + a.nx1) &&
-                            (DIM == 2 || (y >= a.nby && y < a.nby + a.ny1));
-      float4 outv[G];
-#pragma unroll
-      for (int gi = 0; gi < G; gi++) {
-        const float4 *row = buf + gi * plane4;
-        const float4 c = q[gi][2];
-        const float4 L = row[(xl + 2) * W + zl];
-        const float4 Rr = row[(xl + 2) * W + zl + 2];
-        const float4 xm1 = row[(xl + 1) * W + zl + 1], xp1 = row[(xl + 3) * W + zl + 1];
-        const float4 xm2 = row[xl * W + zl + 1], xp2 = row[(xl + 4) * W + zl + 1];
+    float4 q0, q1, q2, q3, q4;
+    for (int i = 0; i < nplanes; i++) {
+      const int y = y0 + i;
+      if (i + P < nplanes) {
+        issue_cur(i + P + 4);
+        issue_pv(i + P);
+      }
+      cp_commit();
+      cp_wait<P>();
+      __syncthreads();
+      const float4 *pl = s_cur + ((i + 2) % NC) * CPL;
+      if (i == 0) {
+        q0 = s_cur[0 * CPL + ci];
+        q1 = s_cur[1 * CPL + ci];
+        q2 = s_cur[2 * CPL + ci];
+        q3 = s_cur[3 * CPL + ci];
+      }
+      q4 = s_cur[((i + 4) % NC) * CPL + ci];
+      if (live) {
+        const float4 L = pl[ci - 1], R = pl[ci + 1];
+        float4 xm1, xp1, xm2, xp2;
+        if (!TWO_D) {
+          xm1 = pl[ci - W];
+          xp1 = pl[ci + W];
+          xm2 = pl[ci - 2 * W];
+          xp2 = pl[ci + 2 * W];
+        }
+        const float4 pv = s_prev[(i % NP) * PPL + pi];
+        const float4 vv4 = s_vv[(i % NP) * PPL + pi];
+        const float wy = a.wy[y];
+        const bool taper = zx_taper || wy != 1.f;
+        const bool lyok = y >= g.ly0 && y < g.ly1;
+        const bool rec_here = rec_zx && y >= a.ry0 && y < a.ry0 + a.nry;
+        const int r_idx = rec_here ? (y - a.ry0) * a.nrx + (ix - a.rx0) : 0;
+        bool src_plane = false;
+        if (!TRI)
+          for (int s = 0; s < a.ns; s++) src_plane |= (y >= a.sy[s] - 1 && y <= a.sy[s] + 1);
         float4 res;
+        if (plain_zx && lyok && !(TRI && rec_here) && !src_plane)
+          res = update4<TWO_D, TRI, false>(a, col, y, gi, lyok, taper, wy, rec_here, r_idx,
+                                           src_plane, q2, L, R, xm1, xp1, xm2, xp2, q0, q1, q3,
+                                           q4, pv, vv4);
+        else
+          res = update4<TWO_D, TRI, true>(a, col, y, gi, lyok, taper, wy, rec_here, r_idx,
+                                          src_plane, q2, L, R, xm1, xp1, xm2, xp2, q0, q1, q3,
+                                          q4, pv, vv4);
+        const long long o = o_c + g.sy * (long long)y;
+        *reinterpret_cast<float4 *>(nxt + o) = res;
+        if (gi == 0 && !TRI && rec_here && a.rec)
+          a.rec[(size_t)a.it * a.nrx * a.nry + r_idx] = el(res, a.rz - iz0);
+        const bool interior = in_zx && y >= a.nby && y < a.nby + a.ny1;
+        if (gi == 0 && a.wfd && interior) {
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-          const int iz = iz0 + e;
-          const float cv = el(c, e);
-          const float zm1 = e == 0 ? L.w : el(c, e - 1);
-          const float zp1 = e == 3 ? Rr.x : el(c, e + 1);
-          const float zm2 = e == 0 ? L.z : (e == 1 ? L.w : el(c, e - 2));
-          const float zp2 = e == 2 ? Rr.x : (e == 3 ? Rr.y : el(c, e + 2));
-          float t = fmul(fmul(a.c0, cv), a.k0);
-          if (DIM == 3) {
-            t = fadd(t, fmul(fmul(a.c1, fadd(el(q[gi][1], e), el(q[gi][3], e))), a.idy));
-            t = fadd(t, fmul(fmul(a.c2, fadd(el(q[gi][0], e), el(q[gi][4], e))), a.idy));
-          }
-          t = fadd(t, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
-          t = fadd(t, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
-          t = fadd(t, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-          t = fadd(t, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-          const float lap = (lzok[e] && lxok && lyok) ? t : 0.f;
-          // prev = taper(u_{k-1} as stored)
-          float p = el(pv[gi], e);
-          p = fmul(fmul(fmul(fmul(p, wz1[e]), wz2[e]), wx1), wx2);
-          if (DIM == 3) p = fmul(fmul(p, wy1), wy2);
-          const float vve = el(vvv, e);
-          float v = fadd(cv, fsub(cv, p));
-          v = fadd(v, fmul(lap, vve));
-          if (TRI) {
-            if (rec_here && iz == a.rz && (a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi))
-              v = fadd(v, fmul(vve, a.tri_dat[(size_t)a.it * a.nrx * a.nry + r_idx]));
-          } else {
-            for (int s = 0; s < a.ns; s++) {
-              const int dz = iz - a.sz[s], dxs = ix - a.sx[s], dys = DIM == 3 ? y - a.sy[s] : 0;
-              if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
-                const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
-                v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
-              }
-            }
-          }
-          v = fmul(fmul(fmul(fmul(v, wz1[e]), wz2[e]), wx1), wx2);
-          if (DIM == 3) v = fmul(fmul(v, wy1), wy2);
-          if (iz >= g.nz) v = 0.f;
-          set_el(res, e, v);
-          if (!TRI && gi == 0 && rec_here && iz == a.rz && a.rec)
-            a.rec[(size_t)a.it * a.nrx * a.nry + r_idx] = v;
-          if (gi == 0 && a.wfd && interior && iz >= a.nb && iz < a.nb + a.nz1)
-            a.wfd[((size_t)(DIM == 3 ? y - a.nby : 0) * a.nx1 + (ix - a.nb)) * a.nz1 + (iz - a.nb)] = v;
-        }
-        outv[gi] = res;
-        *reinterpret_cast<float4 *>(a.nxt[gi] + o) = res;
-      }
-      if (a.img && interior) {
-        float4 im = *reinterpret_cast<const float4 *>(a.img + o);
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-          const int iz = iz0 + e;
-          if (iz >= a.nb && iz < a.nb + a.nz1) {
-            float prod = 1.f;
-#pragma unroll
-            for (int gi = 0; gi < G; gi++) prod = fmul(fmul(prod, el(outv[gi], e)), el(outv[gi], e));
-            set_el(im, e, fadd(el(im, e), prod));
+          for (int e = 0; e < 4; e++) {
+            const int iz = iz0 + e;
+            if (iz >= a.nbz && iz < a.nbz + a.nz1)
+              a.wfd[((size_t)(y - a.nby) * a.nx1 + (ix - a.nbx)) * a.nz1 + (iz - a.nbz)] = el(res, e);
           }
         }
-        *reinterpret_cast<float4 *>(a.img + o) = im;
-      }
-    }
-    if (DIM == 3) {
+        if (last && img_step && interior) {
+          float4 prod = make_float4(1.f, 1.f, 1.f, 1.f);
+          for (int gg = 0; gg < a.ngroups; gg++) {
+            const float4 u = gg == gi ? res : *reinterpret_cast<const float4 *>(a.nxt[gg] + o);
+            prod.x = fmul(fmul(prod.x, u.x), u.x);
+            prod.y = fmul(fmul(prod.y, u.y), u.y);
+            prod.z = fmul(fmul(prod.z, u.z), u.z);
+            prod.w = fmul(fmul(prod.w, u.w), u.w);
+          }
+          float4 im = *reinterpret_cast<const float4 *>(a.img + o);
 #pragma unroll
-      for (int gi = 0; gi < G; gi++) {
-        q[gi][0] = q[gi][1];
-        q[gi][1] = q[gi][2];
-        q[gi][2] = q[gi][3];
-        q[gi][3] = q[gi][4];
+          for (int e = 0; e < 4; e++) {
+            const int iz = iz0 + e;
+            if (iz >= a.nbz && iz < a.nbz + a.nz1) set_el(im, e, fadd(el(im, e), el(prod, e)));
+          }
+          *reinterpret_cast<float4 *>(a.img + o) = im;
+        }
       }
+      q0 = q1;
+      q1 = q2;
+      q2 = q3;
+      q3 = q4;
     }
+    cp_wait_all();
+    __syncthreads();
   }
 }
 
 // vv = ((v*v)*dt)*dt on the expanded grid with edge replication of the
 // interior velocity (vel_expand, wave_abc.c:14-125; wave_fdm.c:173-175).
-__global__ void expand_vv_kernel(Geo g, const float *vel, int nz1, int nx1, int ny1, int nb,
-                                 int nby, float dt, float *vv) {
+// Kernel axes; (nbz,nbx,nby) and (nz1,nx1,ny1) describe the interior.
+__global__ void expand_vv_kernel(Geo g, const float *vel, int nz1, int nx1, int ny1, int nbz,
+                                 int nbx, int nby, float dt, float *vv) {
   const long long n = (long long)g.nz * g.nx * g.ny;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const int iz = int(i % g.nz);
     const int ix = int((i / g.nz) % g.nx);
     const int iy = int(i / ((long long)g.nz * g.nx));
-    int jz = min(max(iz - nb, 0), nz1 - 1);
-    int jx = min(max(ix - nb, 0), nx1 - 1);
-    int jy = min(max(iy - nby, 0), ny1 - 1);
+    const int jz = min(max(iz - nbz, 0), nz1 - 1);
+    const int jx = min(max(ix - nbx, 0), nx1 - 1);
+    const int jy = min(max(iy - nby, 0), ny1 - 1);
     const float v = vel[((size_t)jy * nx1 + jx) * nz1 + jz];
     vv[foff(g, iz, ix, iy)] = fmul(fmul(fmul(v, v), dt), dt);
   }
@@ -280,16 +414,16 @@ __global__ void transpose_kernel(const float *in, float *out, long long rows, lo
   }
 }
 
-// interior cells of a field-layout array -> [ny1][nx1][nz1]
-__global__ void extract_kernel(Geo g, const float *f, int nb, int nby, int nz1, int nx1, int ny1,
-                               float *out) {
+// interior cells of a field-layout array -> [ny1][nx1][nz1] (kernel axes)
+__global__ void extract_kernel(Geo g, const float *f, int nbz, int nbx, int nby, int nz1, int nx1,
+                               int ny1, float *out) {
   const long long n = (long long)nz1 * nx1 * ny1;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const int iz = int(i % nz1);
     const int ix = int((i / nz1) % nx1);
     const int iy = int(i / ((long long)nz1 * nx1));
-    out[i] = f[foff(g, iz + nb, ix + nb, iy + nby)];
+    out[i] = f[foff(g, iz + nbz, ix + nbx, iy + nby)];
   }
 }
 
@@ -307,130 +441,6 @@ __global__ void scale_by_max_kernel(float *x, long long n, const unsigned int *m
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     x[i] = m > 0.f ? fdiv(x[i], m) : x[i];
-}
-
-// ------------------------------------------------------------------ host --
-
-struct Plan {
-  int dim;
-  int nz1, nx1, ny1, nb, nby;
-  Geo g;
-  int nz2, nx2, ny2;
-  int tz4, tx, ych;
-  dim3 grid;
-  int threads;
-  size_t smem_per_g;
-};
-
-static int make_plan(const pw_afd_args *a, Plan &p) {
-  PW_CHECK(a->dim == 2 || a->dim == 3, PW_ERR_SHAPE, "dim must be 2 or 3 (got %d)", a->dim);
-  PW_CHECK(a->nz >= 1 && a->nx >= 1 && a->ny >= 1 && a->nt >= 1 && a->nbt >= 0, PW_ERR_SHAPE,
-           "sizes must be positive (nz=%d nx=%d ny=%d nt=%d nbt=%d)", a->nz, a->nx, a->ny, a->nt,
-           a->nbt);
-  PW_CHECK(a->dim == 3 || a->ny == 1, PW_ERR_SHAPE, "2-D runs need ny = 1 (got %d)", a->ny);
-  p.dim = a->dim;
-  p.nz1 = a->nz;
-  p.nx1 = a->nx;
-  p.ny1 = a->ny;
-  p.nb = a->nbt;
-  p.nby = a->dim == 3 ? a->nbt : 0;
-  Geo &g = p.g;
-  g.nz = p.nz1 + 2 * p.nb;
-  g.nx = p.nx1 + 2 * p.nb;
-  g.ny = a->dim == 3 ? p.ny1 + 2 * p.nb : 1;
-  p.nz2 = pad_first(g.nz);
-  p.nx2 = next_fast(g.nx);
-  p.ny2 = a->dim == 3 ? next_fast(g.ny) : 1;
-  // faces must not overlap inside the padded grid (abc_apply's top/bottom
-  // and left/right strips are disjoint whenever the interior is non-empty)
-  PW_CHECK(p.nz2 >= 2 * p.nb && p.nx2 >= 2 * p.nb && (a->dim == 2 || p.ny2 >= 2 * p.nb),
-           PW_ERR_SHAPE, "taper faces overlap");
-  g.hx = 2;
-  g.hy = a->dim == 3 ? 2 : 0;
-  g.lz = (int)round_up(HZ + round_up(g.nz, 4) + 4, 32);
-  g.px = g.nx + 2 * g.hx;
-  g.py = g.ny + 2 * g.hy;
-  g.sy = (long long)g.lz * g.px;
-  g.lz0 = 2;
-  g.lz1 = std::min(g.nz, p.nz2 - 2);
-  g.lx0 = 2;
-  g.lx1 = std::min(g.nx, p.nx2 - 2);
-  g.ly0 = a->dim == 3 ? 2 : 0;
-  g.ly1 = a->dim == 3 ? std::min(g.ny, p.ny2 - 2) : 1;
-  // tile shape: z float4 columns x x columns, <= 512 threads
-  const int nz4 = ceil_div(g.nz, 4);
-  int ztiles = ceil_div(nz4, 32);
-  p.tz4 = ceil_div(nz4, ztiles);
-  p.tx = std::max(1, std::min(a->dim == 3 ? 8 : 16, 256 / p.tz4));
-  if (a->dim == 3) {
-    const long long zx = (long long)ztiles * ceil_div(g.nx, p.tx);
-    int ych = 32;
-    while (ych > 8 && zx * ceil_div(g.ny, ych) < 148 * 3) ych /= 2;
-    p.ych = ych;
-  } else {
-    p.ych = 1;
-  }
-  p.threads = p.tz4 * p.tx;
-  p.grid = dim3(ztiles, ceil_div(g.nx, p.tx), a->dim == 3 ? ceil_div(g.ny, p.ych) : 1);
-  p.smem_per_g = 2ull * (p.tz4 + 2) * (p.tx + 4) * sizeof(float4);
-  return PW_OK;
-}
-
-static void taper_tables(const Plan &p, float ct, std::vector<float> &wz1, std::vector<float> &wz2,
-                         std::vector<float> &wx1, std::vector<float> &wx2,
-                         std::vector<float> &wy1, std::vector<float> &wy2) {
-  const int nb = p.nb;
-  std::vector<float> w(std::max(nb, 1));
-  // abc_cal (wave_abc.c:141-143): float product, double exp, stored as float
-  for (int ib = 0; ib < nb; ib++) w[ib] = (float)exp(-ct * ct * (nb - 1 - ib) * (nb - 1 - ib));
-  auto axis = [&](int n, int n2, std::vector<float> &first, std::vector<float> &second) {
-    first.assign(n, 1.f);
-    second.assign(n, 1.f);
-    for (int i = 0; i < nb && i < n; i++) first[i] = w[i];          // top / left face
-    for (int i = 0; i < nb; i++) {                                   // bottom / right face,
-      const int cell = n2 - 1 - i;                                   // indexed from the padded end
-      if (cell >= 0 && cell < n) second[cell] = w[i];
-    }
-  };
-  axis(p.g.nz, p.nz2, wz1, wz2);
-  axis(p.g.nx, p.nx2, wx1, wx2);
-  if (p.dim == 3) axis(p.g.ny, p.ny2, wy1, wy2);
-  else { wy1.assign(1, 1.f); wy2.assign(1, 1.f); }
-}
-
-template <int DIM, int G, bool TRI>
-static int launch_step(const Plan &p, const StepArgs &s, cudaStream_t st) {
-  const size_t smem = p.smem_per_g * G;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(step_kernel<DIM, G, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-    attr_set = true;
-  }
-  step_kernel<DIM, G, TRI><<<p.grid, p.threads, smem, st>>>(s);
-  PW_CUDA(cudaGetLastError());
-  return PW_OK;
-}
-
-static int launch_any(const Plan &p, int G, bool tri, const StepArgs &s, cudaStream_t st) {
-#define PW_L(D, GG, T) \
-  if (p.dim == D && G == GG && tri == T) return launch_step<D, GG, T>(p, s, st);
-  PW_L(2, 1, false) PW_L(3, 1, false)
-  PW_L(2, 1, true) PW_L(2, 2, true) PW_L(2, 3, true) PW_L(2, 4, true)
-  PW_L(3, 1, true) PW_L(3, 2, true) PW_L(3, 3, true) PW_L(3, 4, true)
-#undef PW_L
-  set_error("unsupported kernel variant dim=%d G=%d tri=%d", p.dim, G, (int)tri);
-  return PW_ERR_SHAPE;
-}
-
-static int check_cfl(const pw_afd_args *a, const float *vel_host_max) {
-  if (a->flags & PW_NO_CFL_CHECK) return PW_OK;
-  // 4th-order leapfrog: v dt / h <= 0.612 (2-D) / 0.5 (3-D) (measured limits)
-  const float h = std::min(a->dz, std::min(a->dx, a->dim == 3 ? a->dy : a->dx));
-  const float lim = a->dim == 3 ? 0.5f : 0.612f;
-  const float cfl = (*vel_host_max) * a->dt / h;
-  PW_CHECK(cfl <= lim, PW_ERR_CFL, "unstable: vmax*dt/h = %g exceeds %g", cfl, lim);
-  return PW_OK;
 }
 
 __global__ void vel_stats_kernel(const float *v, long long n, unsigned int *out) {
@@ -454,6 +464,164 @@ __global__ void vel_stats_kernel(const float *v, long long n, unsigned int *out)
   }
 }
 
+// ------------------------------------------------------------------ host --
+
+// Compiled tile variants: 3-D (ZW, TX), 2-D (ZW); P = 2 stages of prefetch.
+constexpr int PF = 2;
+struct Variant {
+  int zw, tx;
+};
+static const Variant k3d[] = {{8, 16}, {16, 8}, {24, 8}, {32, 8}};
+static const Variant k2d[] = {{32, 1}, {64, 1}, {96, 1}, {128, 1}, {256, 1}};
+
+static size_t smem_bytes(bool two_d, int zw, int tx) {
+  const int W = zw + 2, rows = two_d ? 1 : tx + 4;
+  return sizeof(float4) * ((size_t)(PF + 6) * W * rows + 2ull * (PF + 2) * zw * tx);
+}
+
+struct Plan {
+  int dim;
+  int nz1, nx1, ny1, nb;
+  // interior placement in kernel axes
+  int kbz, kbx, kby, knz1, knx1, kny1;
+  Geo g;
+  int nz2, nx2, ny2;  // the reference's padded sizes (model axes)
+  Variant v;
+  int ych;
+  dim3 grid;
+  size_t smem;
+};
+
+template <bool TWO_D, int ZW, int TX, bool TRI>
+static void *kernel_ptr() {
+  return (void *)step_kernel<TWO_D, ZW, TX, PF, TRI>;
+}
+
+static void *pick_kernel(bool two_d, Variant v, bool tri) {
+#define PW_K(D2, Z, T)                                                  \
+  if (two_d == D2 && v.zw == Z && v.tx == T)                           \
+    return tri ? kernel_ptr<D2, Z, T, true>() : kernel_ptr<D2, Z, T, false>();
+  PW_K(false, 8, 16) PW_K(false, 16, 8) PW_K(false, 24, 8) PW_K(false, 32, 8)
+  PW_K(true, 32, 1) PW_K(true, 64, 1) PW_K(true, 96, 1) PW_K(true, 128, 1) PW_K(true, 256, 1)
+#undef PW_K
+  return nullptr;
+}
+
+static int blocks_per_sm(void *fn, int threads, size_t smem) {
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    n = 1;
+  }
+  return std::max(n, 1);
+}
+
+static int make_plan(const pw_afd_args *a, bool tri, Plan &p) {
+  PW_CHECK(a->dim == 2 || a->dim == 3, PW_ERR_SHAPE, "dim must be 2 or 3 (got %d)", a->dim);
+  PW_CHECK(a->nz >= 1 && a->nx >= 1 && a->ny >= 1 && a->nt >= 1 && a->nbt >= 0, PW_ERR_SHAPE,
+           "sizes must be positive (nz=%d nx=%d ny=%d nt=%d nbt=%d)", a->nz, a->nx, a->ny, a->nt,
+           a->nbt);
+  PW_CHECK(a->dim == 3 || a->ny == 1, PW_ERR_SHAPE, "2-D runs need ny = 1 (got %d)", a->ny);
+  const bool two_d = a->dim == 2;
+  p.dim = a->dim;
+  p.nz1 = a->nz;
+  p.nx1 = a->nx;
+  p.ny1 = a->ny;
+  p.nb = a->nbt;
+  const int enz = p.nz1 + 2 * p.nb, enx = p.nx1 + 2 * p.nb, eny = two_d ? 1 : p.ny1 + 2 * p.nb;
+  p.nz2 = pad_first(enz);
+  p.nx2 = next_fast(enx);
+  p.ny2 = two_d ? 1 : next_fast(eny);
+  // abc_apply's opposite faces are disjoint whenever the padded grid holds both
+  PW_CHECK(p.nz2 >= 2 * p.nb && p.nx2 >= 2 * p.nb && (two_d || p.ny2 >= 2 * p.nb), PW_ERR_SHAPE,
+           "taper faces overlap");
+  Geo &g = p.g;
+  g.nz = enz;
+  g.lz = (int)round_up(HZ + round_up(enz, 4) + 4, 32);
+  g.lz0 = 2;
+  g.lz1 = std::min(enz, p.nz2 - 2);
+  if (two_d) {
+    g.nx = 1; g.hx = 0; g.sx = g.lz;
+    g.ny = enx; g.hy = 2; g.sy = g.lz;
+    g.lx0 = 0; g.lx1 = 1;
+    g.ly0 = 2; g.ly1 = std::min(enx, p.nx2 - 2);
+    p.kbz = p.nb; p.kbx = 0; p.kby = p.nb;
+    p.knz1 = p.nz1; p.knx1 = 1; p.kny1 = p.nx1;
+  } else {
+    g.nx = enx; g.hx = 2; g.sx = g.lz;
+    g.ny = eny; g.hy = 2; g.sy = (long long)g.lz * (enx + 4);
+    g.lx0 = 2; g.lx1 = std::min(enx, p.nx2 - 2);
+    g.ly0 = 2; g.ly1 = std::min(eny, p.ny2 - 2);
+    p.kbz = p.nb; p.kbx = p.nb; p.kby = p.nb;
+    p.knz1 = p.nz1; p.knx1 = p.nx1; p.kny1 = p.ny1;
+  }
+  g.py = g.ny + 2 * g.hy;
+
+  // tile choice: fewest idle z lanes, then the largest tile
+  const int nz4 = ceil_div(enz, 4);
+  const Variant *list = two_d ? k2d : k3d;
+  const int nlist = two_d ? 5 : 4;
+  Variant best = list[0];
+  long long best_cover = -1;
+  for (int i = 0; i < nlist; i++) {
+    const long long cover = (long long)ceil_div(nz4, list[i].zw) * list[i].zw;
+    if (best_cover < 0 || cover < best_cover || (cover == best_cover && list[i].zw > best.zw)) {
+      best = list[i];
+      best_cover = cover;
+    }
+  }
+  p.v = best;
+  const int threads = best.zw * best.tx;
+  p.smem = smem_bytes(two_d, best.zw, best.tx);
+  void *fn = pick_kernel(two_d, best, tri);
+  PW_CHECK(fn != nullptr, PW_ERR_SHAPE, "no kernel variant");
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int slots = nsm * blocks_per_sm(fn, threads, p.smem);
+  const long long zx = (long long)ceil_div(nz4, best.zw) * ceil_div(g.nx, best.tx);
+  // planes per CTA: balance wave quantisation against the 4-plane prologue
+  double best_score = -1;
+  int best_ych = 8;
+  for (int ych : {64, 48, 40, 32, 24, 16, 12, 8, 6, 4}) {
+    const long long n = zx * ceil_div(g.ny, ych);
+    const long long waves = (n + slots - 1) / slots;
+    const double eff = (double)n / (double)(waves * slots);
+    const double pro = (double)ych / (ych + 1.0);
+    const double score = eff * pro;
+    if (score > best_score + 1e-9) {
+      best_score = score;
+      best_ych = ych;
+    }
+  }
+  p.ych = std::min(best_ych, g.ny);
+  p.grid = dim3(ceil_div(g.ny, p.ych), ceil_div(g.nx, best.tx), ceil_div(nz4, best.zw));
+  return PW_OK;
+}
+
+// Taper factor per cell along one model axis: the top/left face weight
+// w[i] for i < nb, the bottom/right face weight, which abc_apply indexes from
+// the padded end n2-1-i (wave_abc.c:234,260,286), or 1.
+static void taper_axis(int n, int n2, int nb, const std::vector<float> &w, std::vector<float> &f) {
+  f.assign(n, 1.f);
+  for (int i = 0; i < nb && i < n; i++) f[i] = w[i];
+  for (int i = 0; i < nb; i++) {
+    const int cell = n2 - 1 - i;
+    if (cell >= 0 && cell < n) f[cell] = w[i];
+  }
+}
+
+static int check_cfl(const pw_afd_args *a, float vmax) {
+  if (a->flags & PW_NO_CFL_CHECK) return PW_OK;
+  // 4th-order leapfrog: v dt / h <= 0.612 (2-D) / 0.5 (3-D) (measured limits)
+  const float h = std::min(a->dz, std::min(a->dx, a->dim == 3 ? a->dy : a->dx));
+  const float lim = a->dim == 3 ? 0.5f : 0.612f;
+  const float cfl = vmax * a->dt / h;
+  PW_CHECK(cfl <= lim, PW_ERR_CFL, "unstable: vmax*dt/h = %g exceeds %g", cfl, lim);
+  return PW_OK;
+}
+
 // Finite positive velocities and the stability limit, checked on the device
 // copy before the time loop starts.
 static int check_velocity(const pw_afd_args *a, const float *vel_dev, size_t n, unsigned int *mx,
@@ -468,56 +636,42 @@ static int check_velocity(const pw_afd_args *a, const float *vel_dev, size_t n, 
   PW_CHECK(h[2] == 0, PW_ERR_VALUE, "velocity has non-finite or non-positive values");
   float vmax;
   memcpy(&vmax, &h[0], 4);
-  return check_cfl(a, &vmax);
+  return check_cfl(a, vmax);
 }
 
-struct Run {
-  Plan p;
-  int G;
-  bool tri;
-  int ntsnap;
-  // device slices
-  float *vv, *wz1, *wz2, *wx1, *wx2, *wy1, *wy2;
-  float *A[MAXG], *B[MAXG];
-  float *rick, *trid, *rec, *img, *vel;
-  int *gid;
-  unsigned int *mx;
-};
-
 // Shared driver of pw_afd / pw_tri_image.
-static int run(const pw_afd_args *a, int G, const int *group_host_or_dev, const float *vel,
-               const float *src, const float *wavelet, float *dat, float *wfd, float *img_out,
-               int normalize, cudaStream_t st) {
+static int run(const pw_afd_args *a, int G, const int *group, const float *vel, const float *src,
+               const float *wavelet, float *dat, float *wfd, float *img_out, int normalize,
+               cudaStream_t st) {
   PW_CHECK(a != nullptr, PW_ERR_VALUE, "null args");
   const bool host = (a->flags & PW_HOST_PTRS) != 0;
-  Run r{};
-  PW_TRY(make_plan(a, r.p));
-  const Plan &p = r.p;
+  const bool tri = a->tri != 0 || img_out != nullptr;
+  Plan p;
+  PW_TRY(make_plan(a, tri, p));
   const Geo &g = p.g;
-  r.G = G;
-  r.tri = a->tri != 0 || img_out != nullptr;
+  const bool two_d = p.dim == 2;
   PW_CHECK(G >= 1 && G <= MAXG, PW_ERR_SHAPE, "ngroups must be in [1,%d] (got %d)", MAXG, G);
   PW_CHECK(a->jsnap >= 0, PW_ERR_VALUE, "jsnap must be >= 0");
   PW_CHECK(a->gz >= 0 && a->gz < a->nz, PW_ERR_SHAPE, "receiver depth gz=%d outside [0,%d)", a->gz,
            a->nz);
   PW_CHECK(!img_out || a->jsnap > 0, PW_ERR_VALUE, "TRI imaging needs jsnap > 0");
   const int nt = a->nt;
-  r.ntsnap = 0;
+  int ntsnap = 0;
   if (a->jsnap > 0)
     for (int it = 0; it < nt; it++)
-      if (it % a->jsnap == 0) r.ntsnap++;
+      if (it % a->jsnap == 0) ntsnap++;
   const size_t nvel = (size_t)p.nz1 * p.nx1 * p.ny1;
   const size_t nrec = (size_t)p.nx1 * p.ny1;
   const size_t nfield = (size_t)g.sy * g.py + 64;
 
-  // host-side parameters: sources, wavelets, tables
+  // sources and wavelets (host)
   int ns = 0;
-  std::vector<int> sz, sx, sy;
+  std::vector<int> ksz, ksx, ksy;
   std::vector<float> rick;
-  if (!r.tri) {
+  if (!tri) {
     ns = a->ns;
     PW_CHECK(ns >= 0 && ns <= MAXSRC, PW_ERR_SHAPE, "ns must be in [0,%d] (got %d)", MAXSRC, ns);
-    const int rows = a->dim == 3 ? 6 : 5;
+    const int rows = two_d ? 5 : 6;
     std::vector<float> s((size_t)rows * ns);
     if (ns > 0) {
       PW_CHECK(src != nullptr, PW_ERR_VALUE, "source array is null");
@@ -528,16 +682,22 @@ static int run(const pw_afd_args *a, int G, const int *group_host_or_dev, const 
     for (int i = 0; i < ns; i++) {
       // afd.c:416-425 (2-D) / 136-147 (3-D): positions are truncated to int
       const int spx = (int)s[i];
-      const int spy = a->dim == 3 ? (int)s[ns + i] : 0;
-      const int spz = (int)s[(a->dim == 3 ? 2 : 1) * ns + i];
+      const int spy = two_d ? 0 : (int)s[ns + i];
+      const int spz = (int)s[(two_d ? 1 : 2) * ns + i];
       const float f0 = s[(rows - 3) * ns + i], t0 = s[(rows - 2) * ns + i], A = s[(rows - 1) * ns + i];
       PW_CHECK(spx >= 0 && spx < p.nx1 && spz >= 0 && spz < p.nz1 && spy >= 0 && spy < p.ny1,
                PW_ERR_SHAPE, "source %d at (z=%d,x=%d,y=%d) outside the model", i, spz, spx, spy);
-      PW_CHECK(p.nb >= 1 || (spx > 0 && spx < p.nx1 - 1 && spz > 0 && spz < p.nz1 - 1),
+      PW_CHECK(p.nb >= 1 || (spx > 0 && spx < p.nx1 - 1 && spz > 0 && spz < p.nz1 - 1 &&
+                             (two_d || (spy > 0 && spy < p.ny1 - 1))),
                PW_ERR_SHAPE, "source %d stencil leaves the grid", i);
-      sx.push_back(spx + p.nb);
-      sy.push_back(a->dim == 3 ? spy + p.nb : 0);
-      sz.push_back(spz + p.nb);
+      ksz.push_back(spz + p.nb);
+      if (two_d) {
+        ksx.push_back(0);
+        ksy.push_back(spx + p.nb);
+      } else {
+        ksx.push_back(spx + p.nb);
+        ksy.push_back(spy + p.nb);
+      }
       if (wavelet == nullptr) {
         PW_CHECK(t0 >= 0.f && (int)(t0 / a->dt) < nt, PW_ERR_VALUE,
                  "source %d onset t=%g outside [0, nt*dt)", i, t0);
@@ -549,61 +709,81 @@ static int run(const pw_afd_args *a, int G, const int *group_host_or_dev, const 
       else PW_CUDA(cudaMemcpy(rick.data(), wavelet, (size_t)ns * nt * sizeof(float), cudaMemcpyDeviceToHost));
     }
   }
-  std::vector<float> wz1, wz2, wx1, wx2, wy1, wy2;
-  taper_tables(p, a->ct, wz1, wz2, wx1, wx2, wy1, wy2);
+  // taper tables in kernel axes
+  std::vector<float> w(std::max(p.nb, 1));
+  // abc_cal (wave_abc.c:141-143): float product, double exp, stored as float
+  for (int ib = 0; ib < p.nb; ib++)
+    w[ib] = (float)exp(-a->ct * a->ct * (p.nb - 1 - ib) * (p.nb - 1 - ib));
+  std::vector<float> wz, wx, wy;
+  taper_axis(g.nz, p.nz2, p.nb, w, wz);
+  if (two_d) {
+    wx.assign(1, 1.f);
+    taper_axis(g.ny, p.nx2, p.nb, w, wy);
+  } else {
+    taper_axis(g.nx, p.nx2, p.nb, w, wx);
+    taper_axis(g.ny, p.ny2, p.nb, w, wy);
+  }
 
   // workspace layout
   Carve cv;
   const size_t o_vv = cv.add(nfield * 4);
   size_t o_A[MAXG], o_B[MAXG];
-  for (int i = 0; i < G; i++) { o_A[i] = cv.add(nfield * 4); o_B[i] = cv.add(nfield * 4); }
-  const size_t o_t = cv.add((wz1.size() * 2 + wx1.size() * 2 + wy1.size() * 2) * 4);
+  for (int i = 0; i < G; i++) {
+    o_A[i] = cv.add(nfield * 4);
+    o_B[i] = cv.add(nfield * 4);
+  }
+  const size_t ntab = wz.size() + wx.size() + wy.size();
+  const size_t o_t = cv.add(ntab * 4);
   const size_t o_rick = cv.add(rick.size() * 4 + 4);
   const size_t o_vel = cv.add(host ? nvel * 4 : 0);
-  const size_t o_trid = cv.add(r.tri ? (size_t)nt * nrec * 4 : 0);
-  const size_t o_trin = cv.add((r.tri && host) ? (size_t)nt * nrec * 4 : 0);
-  const size_t o_rec = cv.add(!r.tri && dat ? (size_t)nt * nrec * 4 : 0);
-  const size_t o_dat = cv.add(!r.tri && dat && host ? (size_t)nt * nrec * 4 : 0);
+  const size_t o_trid = cv.add(tri ? (size_t)nt * nrec * 4 : 0);
+  const size_t o_trin = cv.add((tri && host) ? (size_t)nt * nrec * 4 : 0);
+  const size_t o_rec = cv.add(!tri && dat ? (size_t)nt * nrec * 4 : 0);
+  const size_t o_dat = cv.add(!tri && dat && host ? (size_t)nt * nrec * 4 : 0);
   const size_t o_img = cv.add(img_out ? nfield * 4 : 0);
   const size_t o_imgx = cv.add(img_out && host ? nvel * 4 : 0);
-  const size_t o_gid = cv.add(group_host_or_dev || G > 1 ? nrec * 4 : 0);
-  const size_t o_wfd = cv.add(wfd && host ? (size_t)r.ntsnap * nvel * 4 : 0);
+  const bool use_gid = group != nullptr || G > 1;
+  const size_t o_gid = cv.add(use_gid ? nrec * 4 : 0);
+  const size_t o_wfd = cv.add(wfd && host ? (size_t)ntsnap * nvel * 4 : 0);
   const size_t o_mx = cv.add(16);
 
   Workspace &ws = Workspace::for_current_device();
   std::lock_guard<std::mutex> lock(ws.mutex());
   PW_TRY(ws.reserve(cv.total()));
   char *base = ws.base();
-  r.vv = at<float>(base, o_vv);
-  for (int i = 0; i < G; i++) { r.A[i] = at<float>(base, o_A[i]); r.B[i] = at<float>(base, o_B[i]); }
+  float *vv = at<float>(base, o_vv);
+  float *A[MAXG], *B[MAXG];
+  for (int i = 0; i < G; i++) {
+    A[i] = at<float>(base, o_A[i]);
+    B[i] = at<float>(base, o_B[i]);
+  }
   float *tb = at<float>(base, o_t);
-  r.wz1 = tb; r.wz2 = r.wz1 + wz1.size(); r.wx1 = r.wz2 + wz2.size(); r.wx2 = r.wx1 + wx1.size();
-  r.wy1 = r.wx2 + wx2.size(); r.wy2 = r.wy1 + wy1.size();
-  r.rick = at<float>(base, o_rick);
-  r.vel = host ? at<float>(base, o_vel) : const_cast<float *>(vel);
-  r.trid = at<float>(base, o_trid);
-  r.rec = at<float>(base, o_rec);
-  r.img = img_out ? at<float>(base, o_img) : nullptr;
-  r.gid = (group_host_or_dev || G > 1) ? at<int>(base, o_gid) : nullptr;
-  r.mx = at<unsigned int>(base, o_mx);
+  float *d_wz = tb, *d_wx = d_wz + wz.size(), *d_wy = d_wx + wx.size();
+  float *d_rick = at<float>(base, o_rick);
+  const float *d_vel = host ? at<float>(base, o_vel) : vel;
+  float *trid = at<float>(base, o_trid);
+  float *rec = at<float>(base, o_rec);
+  float *img = img_out ? at<float>(base, o_img) : nullptr;
+  int *gid = use_gid ? at<int>(base, o_gid) : nullptr;
+  unsigned int *mx = at<unsigned int>(base, o_mx);
 
   // inputs
   PW_CHECK(vel != nullptr, PW_ERR_VALUE, "velocity is null");
   PW_CUDA(cudaMemsetAsync(base, 0, cv.total(), st));
-  if (host) PW_TRY(to_device(r.vel, vel, nvel * 4, true, st));
-  PW_TRY(check_velocity(a, r.vel, nvel, r.mx, st));
+  if (host) PW_TRY(to_device(at<float>(base, o_vel), vel, nvel * 4, true, st));
+  PW_TRY(check_velocity(a, d_vel, nvel, mx, st));
   {
     std::vector<float> all;
-    all.insert(all.end(), wz1.begin(), wz1.end()); all.insert(all.end(), wz2.begin(), wz2.end());
-    all.insert(all.end(), wx1.begin(), wx1.end()); all.insert(all.end(), wx2.begin(), wx2.end());
-    all.insert(all.end(), wy1.begin(), wy1.end()); all.insert(all.end(), wy2.begin(), wy2.end());
+    for (auto *v : {&wz, &wx, &wy}) all.insert(all.end(), v->begin(), v->end());
     PW_CUDA(cudaMemcpyAsync(tb, all.data(), all.size() * 4, cudaMemcpyHostToDevice, st));
   }
-  if (!r.tri && ns > 0)
-    PW_CUDA(cudaMemcpyAsync(r.rick, rick.data(), (size_t)ns * nt * 4, cudaMemcpyHostToDevice, st));
-  expand_vv_kernel<<<1184, 256, 0, st>>>(g, r.vel, p.nz1, p.nx1, p.ny1, p.nb, p.nby, a->dt, r.vv);
+  if (!tri && ns > 0)
+    PW_CUDA(cudaMemcpyAsync(d_rick, rick.data(), (size_t)ns * nt * 4, cudaMemcpyHostToDevice, st));
+  expand_vv_kernel<<<1184, 256, 0, st>>>(g, d_vel, p.knz1, p.knx1, p.kny1, p.kbz, p.kbx, p.kby,
+                                         a->dt, vv);
   PW_CUDA(cudaGetLastError());
-  if (r.tri) {
+  long long aux_launches = 2;
+  if (tri) {
     PW_CHECK(src != nullptr, PW_ERR_VALUE, "TRI traces are null");
     const float *din = src;
     if (host) {
@@ -612,89 +792,116 @@ static int run(const pw_afd_args *a, int G, const int *group_host_or_dev, const 
       din = tmp;
     }
     dim3 tb2(32, 8), tg(ceil_div(nt, 32), ceil_div((long long)nrec, 32));
-    transpose_kernel<<<tg, tb2, 0, st>>>(din, r.trid, (long long)nrec, nt);
+    transpose_kernel<<<tg, tb2, 0, st>>>(din, trid, (long long)nrec, nt);
     PW_CUDA(cudaGetLastError());
+    aux_launches++;
   }
-  if (r.gid) {
-    if (group_host_or_dev) {
-      PW_TRY(to_device(r.gid, group_host_or_dev, nrec * 4, host, st));
+  if (gid) {
+    if (group) {
+      PW_TRY(to_device(gid, group, nrec * 4, host, st));
     } else {
       // the demos' x-bands: dg = nx/G, columns >= G*dg unused
       std::vector<int> gh(nrec);
       const int dg = p.nx1 / G;
       for (int iy = 0; iy < p.ny1; iy++)
-        for (int ix = 0; ix < p.nx1; ix++) gh[(size_t)iy * p.nx1 + ix] = dg > 0 && ix / dg < G ? ix / dg : -1;
-      PW_CUDA(cudaMemcpyAsync(r.gid, gh.data(), nrec * 4, cudaMemcpyHostToDevice, st));
+        for (int ix = 0; ix < p.nx1; ix++)
+          gh[(size_t)iy * p.nx1 + ix] = dg > 0 && ix / dg < G ? ix / dg : -1;
+      PW_CUDA(cudaMemcpyAsync(gid, gh.data(), nrec * 4, cudaMemcpyHostToDevice, st));
     }
   }
 
   // time loop
   StepArgs s{};
   s.g = g;
-  s.tz4 = p.tz4; s.tx = p.tx; s.ych = p.ych;
+  s.ych = p.ych;
+  s.ngroups = G;
   {
     const float c0 = -30. / 12., c1 = +16. / 12., c2 = -1. / 12.;  // wave_fdm.c:15
-    s.c0 = c0; s.c1 = c1; s.c2 = c2;
-    s.idz = 1 / (a->dz * a->dz);
-    s.idx = 1 / (a->dx * a->dx);
-    s.idy = a->dim == 3 ? 1 / (a->dy * a->dy) : 0.f;
-    s.k0 = a->dim == 3 ? (s.idy + s.idx) + s.idz : s.idx + s.idz;
+    s.c0 = c0;
+    s.c1 = c1;
+    s.c2 = c2;
+    const float idz = 1 / (a->dz * a->dz), idx = 1 / (a->dx * a->dx);
+    s.idz = idz;
+    if (two_d) {
+      s.idy = idx;  // the model's x is the marched axis
+      s.idx = 0.f;
+      s.k0 = idx + idz;
+    } else {
+      const float idy = 1 / (a->dy * a->dy);
+      s.idx = idx;
+      s.idy = idy;
+      s.k0 = (idy + idx) + idz;
+    }
   }
-  s.vv = r.vv;
-  s.wz1 = r.wz1; s.wz2 = r.wz2; s.wx1 = r.wx1; s.wx2 = r.wx2; s.wy1 = r.wy1; s.wy2 = r.wy2;
+  s.vv = vv;
+  s.wz = d_wz;
+  s.wx = d_wx;
+  s.wy = d_wy;
   s.nt = nt;
   s.ns = ns;
-  for (int i = 0; i < ns; i++) { s.sz[i] = sz[i]; s.sx[i] = sx[i]; s.sy[i] = sy[i]; }
-  s.rick = r.rick;
+  for (int i = 0; i < ns; i++) {
+    s.sz[i] = ksz[i];
+    s.sx[i] = ksx[i];
+    s.sy[i] = ksy[i];
+  }
+  s.rick = d_rick;
   s.rz = p.nb + a->gz;
-  s.rx0 = p.nb; s.ry0 = p.nby; s.nrx = p.nx1; s.nry = p.ny1;
-  s.tri_dat = r.tri ? r.trid : nullptr;
-  s.gid = r.gid;
-  s.rec = (!r.tri && dat) ? r.rec : nullptr;
-  s.nb = p.nb; s.nz1 = p.nz1; s.nx1 = p.nx1; s.ny1 = p.ny1; s.nby = p.nby;
+  if (two_d) {
+    s.rx0 = 0; s.nrx = 1; s.ry0 = p.nb; s.nry = p.nx1;
+  } else {
+    s.rx0 = p.nb; s.nrx = p.nx1; s.ry0 = p.nb; s.nry = p.ny1;
+  }
+  s.tri_dat = tri ? trid : nullptr;
+  s.gid = gid;
+  s.rec = (!tri && dat) ? rec : nullptr;
+  s.nbz = p.kbz; s.nbx = p.kbx; s.nby = p.kby;
+  s.nz1 = p.knz1; s.nx1 = p.knx1; s.ny1 = p.kny1;
   float *wfd_dev = wfd ? (host ? at<float>(base, o_wfd) : wfd) : nullptr;
-  float *A[MAXG], *B[MAXG];
-  for (int i = 0; i < G; i++) { A[i] = r.A[i]; B[i] = r.B[i]; }
+  void *fn = pick_kernel(two_d, p.v, tri);
+  const int threads = p.v.zw * p.v.tx;
   LoopTimer timer(st);
   timer.start();
   for (int k = 0; k < nt; k++) {
-    const int it = r.tri ? nt - 1 - k : k;
+    const int it = tri ? nt - 1 - k : k;
     s.it = it;
-    for (int i = 0; i < G; i++) { s.cur[i] = A[i]; s.nxt[i] = B[i]; }
+    for (int i = 0; i < G; i++) {
+      s.cur[i] = A[i];
+      s.nxt[i] = B[i];
+    }
     const bool snap = a->jsnap > 0 && it % a->jsnap == 0;
     s.wfd = (snap && wfd_dev) ? wfd_dev + (size_t)(it / a->jsnap) * nvel : nullptr;
-    s.img = (snap && r.img) ? r.img : nullptr;
-    PW_TRY(launch_any(p, G, r.tri, s, st));
+    s.img = (snap && img) ? img : nullptr;
+    void *args[] = {(void *)&s};
+    PW_CUDA(cudaLaunchKernel(fn, p.grid, dim3(threads), args, p.smem, st));
     for (int i = 0; i < G; i++) std::swap(A[i], B[i]);
   }
   timer.stop();
 
   // outputs
-  if (!r.tri && dat) {
+  if (!tri && dat) {
     float *dst = host ? at<float>(base, o_dat) : dat;
     dim3 tb2(32, 8), tg(ceil_div((long long)nrec, 32), ceil_div(nt, 32));
-    transpose_kernel<<<tg, tb2, 0, st>>>(r.rec, dst, nt, (long long)nrec);
+    transpose_kernel<<<tg, tb2, 0, st>>>(rec, dst, nt, (long long)nrec);
     PW_CUDA(cudaGetLastError());
+    aux_launches++;
     if (host) PW_TRY(to_host(dat, dst, (size_t)nt * nrec * 4, true, st));
   }
-  if (wfd && host) PW_TRY(to_host(wfd, wfd_dev, (size_t)r.ntsnap * nvel * 4, true, st));
+  if (wfd && host) PW_TRY(to_host(wfd, wfd_dev, (size_t)ntsnap * nvel * 4, true, st));
   if (img_out) {
     float *dst = host ? at<float>(base, o_imgx) : img_out;
-    extract_kernel<<<1184, 256, 0, st>>>(g, r.img, p.nb, p.nby, p.nz1, p.nx1, p.ny1, dst);
+    extract_kernel<<<1184, 256, 0, st>>>(g, img, p.kbz, p.kbx, p.kby, p.knz1, p.knx1, p.kny1, dst);
     PW_CUDA(cudaGetLastError());
+    aux_launches++;
     if (normalize) {
-      absmax_kernel<<<592, 256, 0, st>>>(dst, (long long)nvel, r.mx);
-      scale_by_max_kernel<<<1184, 256, 0, st>>>(dst, (long long)nvel, r.mx);
+      absmax_kernel<<<592, 256, 0, st>>>(dst, (long long)nvel, mx);
+      scale_by_max_kernel<<<1184, 256, 0, st>>>(dst, (long long)nvel, mx);
       PW_CUDA(cudaGetLastError());
+      aux_launches += 2;
     }
     if (host) PW_TRY(to_host(img_out, dst, nvel * 4, true, st));
   }
   PW_CUDA(cudaStreamSynchronize(st));
-  // launches: velocity check, vv expansion, [trace transpose], time loop,
-  // [trace transpose | image extract (+2 for normalisation)]
-  const long long aux = 2 + (r.tri ? 1 : 0) + ((!r.tri && dat) ? 1 : 0) +
-                        (img_out ? (normalize ? 3 : 1) : 0);
-  timer.finish(nt, nt + aux);
+  timer.finish(nt, nt + aux_launches);
   return PW_OK;
 }
 
