@@ -30,6 +30,7 @@ extern "C" {
 
 #define PW_HOST_PTRS 1        /* all array pointers are host memory */
 #define PW_NO_CFL_CHECK 2     /* skip the host-side stability check */
+#define PW_PER_SHOT 4         /* pfwi: one shot at a time (the reference's summation order) */
 
 /* ---------------------------------------------------------------- afd --- */
 
@@ -97,7 +98,7 @@ typedef struct pw_fwi_args {
   int interval;    /* snapshot interval of the reference-mode gradient */
   int niter;       /* L-BFGS iterations (pw_fwi) */
   int sz, rz;      /* source / receiver depth below the top (pfwi.c: 5 and 1) */
-  int flags;       /* PW_HOST_PTRS | PW_NO_CFL_CHECK */
+  int flags;       /* PW_HOST_PTRS | PW_NO_CFL_CHECK | PW_PER_SHOT */
 } pw_fwi_args;
 
 /* Fills a pw_fwi_args from pfwi's float parameter array (pfwi.c:691-713
@@ -132,6 +133,17 @@ int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const flo
  * static does. */
 int pw_gradient_postprocess(int nz, int nx, int rect, int waterz, float *grad, float *scaling,
                             int flags, void *stream);
+
+/* Full-waveform inversion as fwic runs it (pywave/src/pfwi.c:497-1029 ->
+ * fwi, wave_fwi.c:24-119): gradient_av + gradient_smooth2 (rect 3, first-call
+ * scale), L-BFGS with 20 pairs and the Wolfe line search of
+ * wave_fwilbfgs.c:108-165 (20 trials, c1 1e-4, c2 0.9, factor 10, clip [0,10]),
+ * stopping when misfit/misfit0 < 0.01.  Inner products run in FP64 on the GPU.
+ *   vel0 [nx][nz] starting model, dobs [ns][nr][nt],
+ *   vinv [niter][nx][nz] model after each iteration (zero after an early stop),
+ *   iters_done number of completed iterations. */
+int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav, const float *dobs,
+           float *vinv, int *iters_done, void *stream);
 
 /* ------------------------------------------------------------ utility --- */
 

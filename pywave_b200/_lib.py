@@ -24,6 +24,7 @@ PW_ERR_CUDA = -5
 PW_ERR_VALUE = -6
 PW_HOST_PTRS = 1
 PW_NO_CFL_CHECK = 2
+PW_PER_SHOT = 4
 PW_GRAD_REFERENCE = 0
 PW_GRAD_EXACT = 1
 
@@ -78,6 +79,7 @@ _SIGS = {
                                    C.c_int, _vp]),
     "pw_gradient_postprocess": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int,
                                           _vp]),
+    "pw_fwi": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp, C.POINTER(C.c_int), _vp]),
     "pw_last_error": (C.c_char_p, []),
     "pw_version": (C.c_char_p, []),
     "pw_release_cache": (C.c_int, []),

@@ -1,5 +1,647 @@
-// pfwi acoustic path (forward modelling, FWI gradient, post-processing).
+// pfwi acoustic path on sm_100a: forward modelling, FWI gradients (the
+// reference's gradient_av imaging and the exact discrete adjoint with
+// checkpointing), residual / FP64 misfit and gradient post-processing.
+//
+// Scheme (pywave/src/wave_fwimodeling.c:72-104, wave_fwigradient.c:132-241):
+//   term = Lap8(a) (zero outside [4,pad-4)) + rr*w[it]
+//   a_new = S((2a - S(b)) + (v*v*dt^2)*term),   S = sponge, b = previous a
+// on the padded grid (nz+2nb) x (nx+2nb).  Same field layout, two-buffer
+// scheme and cp.async plane pipeline as the afd kernel, with an 8th-order
+// stencil: the model's x is the marched axis (9-deep register queue), z is
+// tiled (float4 per thread, one float4 of halo on each side = 4 cells).
+// All shots of a call advance together, one after another inside each CTA,
+// sharing the v^2 dt^2 plane.
 #include "pw_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace pw {
+namespace pf {
+
+constexpr int HZ = 4;        // z halo (cells) in front of iz = 0
+constexpr int HX = 4;        // x halo (planes) in front of ix = 0
+constexpr int MAXS = 64;     // shots per launch
+constexpr int MAXSRCW = 16;  // source-map cells per shot
+
+// Shot geometry resolved on the host (preparation, wave_fwiutil.c:44-71).
+struct ShotGeo {
+  int r0v, r02, nr2;          // receivers rx = r0v + ir*drv, ir < nr2, stored at trace r02 + ir
+  int nsrc;                   // non-zero source-map cells
+  int scell[MAXSRCW];         // (ix << 16) | iz of each cell
+  float sw[MAXSRCW];          // source-map weight rr
+};
+
+enum Mode { FWD = 0, ADJ_REF = 1, ADJ_EXACT = 2 };
+
+struct PfArgs {
+  int pnz, pnx;               // padded grid
+  int lz;                     // leading dimension of the field layout
+  int nb, nz, nx;             // sponge width, interior
+  float c0, c1, c2, c3, c4;   // 8th-order coefficients (wave_fwiutil.c:17)
+  float dx2, dz2;
+  int nshots;
+  const float *cur[MAXS];
+  float *nxt[MAXS];
+  const float *V;             // v*v*dt^2 (field layout)
+  const float *bz, *bx;       // sponge factor per z / x cell (1 off the faces)
+  int it, nt;
+  const ShotGeo *geo;         // [nshots] (device)
+  int rz, drv, nr;
+  const float *wav;           // forward: wavelet [nt]
+  float *rec;                 // forward: traces [shot][nt][nr] or null
+  float *snap;                // forward: interior snapshot for this step [shot][nx][nz] or null
+  long long snap_stride;      // floats between shots' snapshots
+  float *tout;                // forward: term output [shot] (field layout) or null
+  long long tout_stride;
+  const float *res;           // adjoint: residual [shot][nt][nr]
+  // ADJ_REF imaging: grad[ix][iz] += (w1-2w0+wm1)/wdt2 * phi * (-2/v^3) in double
+  const float *wprev, *wcur, *wnext;  // snapshots wit-1, wit, wit+1 [shot][nx][nz]
+  long long wstride;
+  float wdt2;
+  const float *vint;          // interior velocity [nx][nz]
+  float *grad;                // [nx][nz] (ADJ_REF) or field layout (ADJ_EXACT: sum phi*term)
+  const float *tin;           // ADJ_EXACT: term of the forward step [shot] (field layout)
+  long long tin_stride;
+  int imaging;                // this step images
+  long long fstride;          // field size (floats)
+};
+
+__device__ __forceinline__ float el(const float4 &v, int e) {
+  return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void set_el(float4 &v, int e, float x) {
+  if (e == 0) v.x = x; else if (e == 1) v.y = x; else if (e == 2) v.z = x; else v.w = x;
+}
+__device__ __forceinline__ long long pfoff(int lz, int iz, int ix) {
+  return (long long)(iz + HZ) + (long long)lz * (ix + HX);
+}
+
+__device__ __forceinline__ void cp16(float4 *dst, const float *src, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(n)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// z terms of the 8th-order Laplacian for cell e of the float4 c, with L / R
+// the float4s below and above (cells -4..-1, +4..+7).
+__device__ __forceinline__ float znb(const float4 &L, const float4 &c, const float4 &R, int e, int d) {
+  const int j = e + d;  // -4 .. 7
+  if (j < 0) return el(L, j + 4);
+  if (j > 3) return el(R, j - 4);
+  return el(c, j);
+}
+
+// One pfwi step over a z column segment of ZW float4 marching along x.
+template <int ZW, int P, int MODE>
+__global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
+  constexpr int W = ZW + 2;   // curr plane (float4) incl. z halo
+  constexpr int NC = P + 10;  // curr planes (x-4..x+4 live, P ahead, 1 slack)
+  constexpr int NP = P + 2;
+  extern __shared__ float4 sm[];
+  float4 *s_cur = sm;
+  float4 *s_prev = sm + NC * W;
+  float4 *s_V = s_prev + NP * ZW;
+  float4 *s_t = s_V + NP * ZW;  // ADJ_EXACT: forward term tile
+
+  const int tid = threadIdx.x;
+  const int z4 = blockIdx.y * ZW + tid;
+  const int iz0 = 4 * z4;
+  const int x0 = blockIdx.x * xch;
+  const int x1 = min(a.pnx, x0 + xch);
+  const int nplanes = x1 - x0;
+  const int lz = a.lz;
+  const bool live = iz0 < a.pnz;
+  const long long o_c = pfoff(lz, iz0, 0);
+  const int ci = tid + 1;
+  const int hz4 = tid == 0 ? blockIdx.y * ZW - 1 : blockIdx.y * ZW + ZW;  // halo float4 (threads 0, 1)
+  const bool has_h = tid < 2;
+  const int hslot = tid == 0 ? 0 : ZW + 1;
+  const bool h_ok = has_h && hz4 >= -1 && hz4 * 4 < a.pnz;
+  const long long h_off = h_ok ? pfoff(lz, hz4 * 4, 0) : 0;
+
+  float bzf[4];
+  bool lz_ok[4], zin[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int iz = iz0 + e;
+    bzf[e] = (live && iz < a.pnz) ? a.bz[iz] : 1.f;
+    lz_ok[e] = iz >= 4 && iz < a.pnz - 4;
+    zin[e] = iz < a.pnz;
+  }
+  const bool rec_row = a.rz >= iz0 && a.rz < iz0 + 4;
+
+  for (int s = 0; s < a.nshots; s++) {
+    const float *cur = a.cur[s];
+    float *nxt = a.nxt[s];
+    const float *tin = MODE == ADJ_EXACT ? a.tin + s * a.tin_stride : nullptr;
+    const ShotGeo &sg = a.geo[s];
+    auto issue_cur = [&](int k) {  // plane x = x0 - 4 + k
+      const int x = x0 - 4 + k;
+      const bool xok = x >= -HX && x < a.pnx + HX;
+      float4 *dst = s_cur + (k % NC) * W;
+      const long long ox = (long long)lz * x;
+      cp16(dst + ci, cur + (live && xok ? o_c + ox : 0), live && xok);
+      if (has_h) cp16(dst + hslot, cur + (h_ok && xok ? h_off + ox : 0), h_ok && xok);
+    };
+    auto issue_pv = [&](int j) {  // plane x = x0 + j
+      const long long o = o_c + (long long)lz * (x0 + j);
+      cp16(s_prev + (j % NP) * ZW + tid, live ? nxt + o : nxt, live);
+      cp16(s_V + (j % NP) * ZW + tid, live ? a.V + o : a.V, live);
+      if (MODE == ADJ_EXACT) cp16(s_t + (j % NP) * ZW + tid, live ? tin + o : tin, live && a.imaging);
+    };
+    for (int k = 0; k < 8; k++) issue_cur(k);
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      if (b < nplanes) {
+        issue_cur(b + 8);
+        issue_pv(b);
+      }
+      cp_commit();
+    }
+    float4 q[9];
+    for (int i = 0; i < nplanes; i++) {
+      const int x = x0 + i;
+      if (i + P < nplanes) {
+        issue_cur(i + P + 8);
+        issue_pv(i + P);
+      }
+      cp_commit();
+      cp_wait<P>();
+      __syncthreads();
+      if (i == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) q[k] = s_cur[k * W + ci];
+      }
+      q[8] = s_cur[((i + 8) % NC) * W + ci];
+      const float4 *pl = s_cur + ((i + 4) % NC) * W;
+      if (live) {
+        const float4 c = q[4];
+        const float4 L = pl[ci - 1], R = pl[ci + 1];
+        const float4 pv = s_prev[(i % NP) * ZW + tid];
+        const float4 V4 = s_V[(i % NP) * ZW + tid];
+        const float bxf = a.bx[x];
+        const bool lx_ok = x >= 4 && x < a.pnx - 4;
+        const long long o = o_c + (long long)lz * x;
+        // receivers read the field before the update (wave_fwimodeling.c:76-79)
+        int rir = -1;
+        if (rec_row) {
+          const int d = x - sg.r0v;
+          if (d >= 0 && d % a.drv == 0 && d / a.drv < sg.nr2) rir = sg.r02 + d / a.drv;
+        }
+        if (MODE == FWD && rir >= 0 && a.rec)
+          a.rec[((size_t)s * a.nt + a.it) * a.nr + rir] = el(c, a.rz - iz0);
+        const bool interior = x >= a.nb && x < a.nb + a.nx;
+        if (MODE == FWD && a.snap && interior) {
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const int iz = iz0 + e;
+            if (iz >= a.nb && iz < a.nb + a.nz)
+              a.snap[s * a.snap_stride + (size_t)(x - a.nb) * a.nz + (iz - a.nb)] = el(c, e);
+          }
+        }
+        float4 term4, res4;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int iz = iz0 + e;
+          const float cv = el(c, e);
+          float tx = fmul(a.c0, cv);
+          tx = fadd(tx, fmul(a.c1, fadd(el(q[5], e), el(q[3], e))));
+          tx = fadd(tx, fmul(a.c2, fadd(el(q[6], e), el(q[2], e))));
+          tx = fadd(tx, fmul(a.c3, fadd(el(q[7], e), el(q[1], e))));
+          tx = fadd(tx, fmul(a.c4, fadd(el(q[8], e), el(q[0], e))));
+          float tz = fmul(a.c0, cv);
+          tz = fadd(tz, fmul(a.c1, fadd(znb(L, c, R, e, 1), znb(L, c, R, e, -1))));
+          tz = fadd(tz, fmul(a.c2, fadd(znb(L, c, R, e, 2), znb(L, c, R, e, -2))));
+          tz = fadd(tz, fmul(a.c3, fadd(znb(L, c, R, e, 3), znb(L, c, R, e, -3))));
+          tz = fadd(tz, fmul(a.c4, fadd(znb(L, c, R, e, 4), znb(L, c, R, e, -4))));
+          float t = (lz_ok[e] && lx_ok) ? fadd(fdiv(tx, a.dx2), fdiv(tz, a.dz2)) : 0.f;
+          if (MODE == FWD) {
+            for (int k = 0; k < sg.nsrc; k++)
+              if (sg.scell[k] == ((x << 16) | iz)) t = fadd(t, fmul(sg.sw[k], a.wav[a.it]));
+          } else if (rir >= 0 && iz == a.rz) {
+            t = fadd(t, a.res[((size_t)s * a.nt + a.it) * a.nr + rir]);
+          }
+          set_el(term4, e, t);
+          // b = S(a_{k-1} as stored): z faces then x faces (apply_sponge)
+          const float p = fmul(bxf, fmul(bzf[e], el(pv, e)));
+          float v = fadd(fsub(fmul(2.f, cv), p), fmul(el(V4, e), t));
+          v = fmul(bxf, fmul(bzf[e], v));
+          set_el(res4, e, zin[e] ? v : 0.f);
+        }
+        *reinterpret_cast<float4 *>(nxt + o) = res4;
+        if (MODE == FWD && a.tout)
+          *reinterpret_cast<float4 *>(a.tout + s * a.tout_stride + o) = term4;
+        if (MODE == ADJ_EXACT && a.imaging) {
+          // dJ/dV accumulates phi_n * term_n (divided by V at the end)
+          const float4 tf = s_t[(i % NP) * ZW + tid];
+          float4 gacc = *reinterpret_cast<const float4 *>(a.grad + o);
+          gacc.x = fadd(gacc.x, fmul(c.x, tf.x));
+          gacc.y = fadd(gacc.y, fmul(c.y, tf.y));
+          gacc.z = fadd(gacc.z, fmul(c.z, tf.z));
+          gacc.w = fadd(gacc.w, fmul(c.w, tf.w));
+          *reinterpret_cast<float4 *>(a.grad + o) = gacc;
+        }
+        if (MODE == ADJ_REF && a.imaging && interior) {
+          // gradient_av (wave_fwigradient.c:221-230), evaluated in double as
+          // the C expression is, accumulated into the float gradient
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const int iz = iz0 + e;
+            if (iz >= a.nb && iz < a.nb + a.nz) {
+              const size_t k = (size_t)(x - a.nb) * a.nz + (iz - a.nb);
+              float temp = a.vint[k];
+              temp = fmul(fmul(temp, temp), temp);
+              temp = (float)(-2. / (double)temp);
+              const double w1 = a.wnext[s * a.wstride + k], w0 = a.wcur[s * a.wstride + k],
+                           wm = a.wprev[s * a.wstride + k];
+              const double gsum = (w1 - 2. * w0 + wm) / (double)a.wdt2 * (double)el(c, e) * (double)temp;
+              a.grad[k] = (float)((double)a.grad[k] + gsum);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; k++) q[k] = q[k + 1];
+    }
+    cp_wait_all();
+    __syncthreads();
+  }
+}
+
+// FP64 misfit and residual, one thread per (shot, it, ir):
+//   REFERENCE: r = dobs - d, J += 0.5 r^2 (unweighted), adjoint source r*w
+//   EXACT:     r = d - dobs, J += 0.5 w r^2, adjoint source w*r
+// d, dobs, res: [shot][nt][nr]; w: [nr][nt] (residual_weighting layout).
+__global__ void residual_kernel(const float *d, const float *dobs, const float *w, float *res,
+                                int ns, int nt, int nr, int exact, double *misfit) {
+  const long long n = (long long)ns * nt * nr;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int ir = int(i % nr);
+    const int it = int((i / nr) % nt);
+    const float wt = w[(size_t)ir * nt + it];
+    if (exact) {
+      const float r = fsub(d[i], dobs[i]);
+      acc += 0.5 * (double)wt * (double)r * (double)r;
+      res[i] = fmul(wt, r);
+    } else {
+      const float r = fsub(dobs[i], d[i]);
+      acc += 0.5 * (double)r * (double)r;
+      res[i] = fmul(r, wt);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) atomicAdd(misfit, v);
+  }
+}
+
+// V = (v*v)*dt2 on the padded grid (pad2d edge replication, wave_fwiutil.c:123-147)
+__global__ void pad_V_kernel(const float *vel, int nz, int nx, int nb, int pnz, int pnx, int lz,
+                             float dt2, float *V) {
+  const long long n = (long long)pnz * pnx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int iz = int(i % pnz), ix = int(i / pnz);
+    const int jz = min(max(iz - nb, 0), nz - 1), jx = min(max(ix - nb, 0), nx - 1);
+    const float v = vel[(size_t)jx * nz + jz];
+    V[pfoff(lz, iz, ix)] = fmul(fmul(v, v), dt2);
+  }
+}
+
+// [rows][cols] -> [cols][rows]
+__global__ void transpose_kernel(const float *in, float *out, long long rows, long long cols) {
+  __shared__ float t[32][33];
+  const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const long long r = r0 + j, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) t[j][threadIdx.x] = in[r * cols + c];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const long long c = c0 + j, r = r0 + threadIdx.x;
+    if (r < rows && c < cols) out[c * rows + r] = t[threadIdx.x][j];
+  }
+}
+
+// Exact gradient: dJ/dv_pad = 2 * sum(phi*term) / v_pad, folded back through
+// pad2d's edge replication onto the interior (one thread per interior cell,
+// summing the padded cells that copy it, in a fixed order).
+__global__ void fold_grad_kernel(const float *gacc, const float *vel, int nz, int nx, int nb,
+                                 int pnz, int pnx, int lz, float *grad) {
+  const long long n = (long long)nz * nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int jz = int(i % nz), jx = int(i / nz);
+    const int z_lo = jz == 0 ? 0 : jz + nb, z_hi = jz == nz - 1 ? pnz - 1 : jz + nb;
+    const int x_lo = jx == 0 ? 0 : jx + nb, x_hi = jx == nx - 1 ? pnx - 1 : jx + nb;
+    const double v = vel[i];
+    double s = 0.0;
+    for (int ix = x_lo; ix <= x_hi; ix++)
+      for (int iz = z_lo; iz <= z_hi; iz++) s += (double)gacc[pfoff(lz, iz, ix)];
+    grad[i] = (float)(2.0 * s / v);
+  }
+}
+
+// ---------------------------------------------- post-processing kernels --
+// One line of np_smooth2 (wave_triangle.c:177-238) per thread, in the
+// reference's float order; tmp: per-thread scratch of n + 2*rect floats.
+__device__ void smooth2_line(int nb, int n, float *x, long long o, long long d, float *tmp) {
+  const int np = n + 2 * nb;
+  const float wt = (float)(1.0 / (nb * nb));
+  float t;
+  for (int i = 0; i < np; i++) tmp[i] = 0.f;
+  for (int i = 0; i < n; i++) tmp[i] = fadd(tmp[i], fmul(-wt, x[o + i * d]));
+  const float w2 = (float)(2. * wt);
+  for (int i = 0; i < n; i++) tmp[i + nb] = fadd(tmp[i + nb], fmul(w2, x[o + i * d]));
+  for (int i = 0; i < n; i++) tmp[i + 2 * nb] = fadd(tmp[i + 2 * nb], fmul(-wt, x[o + i * d]));
+  t = 0.f;
+  for (int i = 0; i < np; i++) { t = fadd(t, tmp[i]); tmp[i] = t; }
+  t = 0.f;
+  for (int i = np - 1; i >= 0; i--) { t = fadd(t, tmp[i]); tmp[i] = t; }
+  for (int i = 0; i < n; i++) x[o + i * d] = tmp[i + nb];
+  for (int m = 0; m < nb; m++) {  // right extension: mirrored, then direct, ...
+    const int b = m / n, i = m % n;
+    const int dst = (b % 2 == 0) ? (n - 1 - i) : i;
+    x[o + dst * d] = fadd(x[o + dst * d], tmp[nb + n + m]);
+  }
+  for (int m = 0; m < nb; m++) {  // left extension: direct, then mirrored, ...
+    const int b = m / n, i = m % n;
+    const int dst = (b % 2 == 0) ? i : (n - 1 - i);
+    x[o + dst * d] = fadd(x[o + dst * d], tmp[nb - 1 - m]);
+  }
+}
+
+__global__ void smooth_lines_kernel(float *x, int nlines, int n, long long line_step,
+                                    long long elem_step, int rect, float *scratch) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nlines) return;
+  smooth2_line(rect, n, x, (long long)l * line_step, elem_step, scratch + (size_t)l * (n + 2 * rect));
+}
+
+__global__ void absmax_kernel(const float *x, long long n, unsigned int *out) {
+  float m = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    m = fmaxf(m, fabsf(x[i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+__global__ void vel_check_kernel(const float *x, long long n, unsigned int *out) {
+  float m = 0.f;
+  unsigned bad = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float v = x[i];
+    if (!(v > 0.f) || !isfinite(v)) bad = 1;
+    else m = fmaxf(m, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, __float_as_uint(m));
+    if (bad) atomicOr(out + 1, 1u);
+  }
+}
+
+// waterz rows to zero and the scale factor (gradient_smooth2 tail,
+// wave_fwiutil.c:323-334); scaling <= 0 means "derive 0.1/max|g| here"
+__global__ void finish_kernel(float *g, int nz, int nx, int waterz, const unsigned int *mx,
+                              float *scaling) {
+  float sc = *scaling;
+  if (sc <= 0.f) sc = (float)(0.1 / (double)__uint_as_float(*mx));
+  const long long n = (long long)nz * nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int iz = int(i % nz);
+    float v = g[i];
+    if (waterz >= 0 ? iz < waterz : iz >= nz + waterz) v = 0.f;
+    g[i] = fmul(v, sc);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && *scaling <= 0.f) *scaling = sc;
+}
+
+// ------------------------------------------------------------------ host --
+
+// Restated source map: a unit spike at (sx, sz) smoothed with rect 2 along
+// z then x (source_map, wave_fwiutil.c:149-177), on the host in float.
+static void smooth_line_host(int nb, int n, float *x, long long o, long long d, std::vector<float> &tmp) {
+  const int np = n + 2 * nb;
+  tmp.assign(np, 0.f);
+  const float wt = (float)(1.0 / (nb * nb));
+  for (int i = 0; i < n; i++) tmp[i] += (-wt) * x[o + i * d];
+  for (int i = 0; i < n; i++) tmp[i + nb] += ((float)(2. * wt)) * x[o + i * d];
+  for (int i = 0; i < n; i++) tmp[i + 2 * nb] += (-wt) * x[o + i * d];
+  float t = 0.f;
+  for (int i = 0; i < np; i++) { t += tmp[i]; tmp[i] = t; }
+  t = 0.f;
+  for (int i = np - 1; i >= 0; i--) { t += tmp[i]; tmp[i] = t; }
+  for (int i = 0; i < n; i++) x[o + i * d] = tmp[i + nb];
+  for (int m = 0; m < nb; m++) {
+    const int b = m / n, i = m % n;
+    const int dst = (b % 2 == 0) ? (n - 1 - i) : i;
+    x[o + dst * d] += tmp[nb + n + m];
+  }
+  for (int m = 0; m < nb; m++) {
+    const int b = m / n, i = m % n;
+    const int dst = (b % 2 == 0) ? i : (n - 1 - i);
+    x[o + dst * d] += tmp[nb - 1 - m];
+  }
+}
+
+static int source_map(int sx, int sz, int pnz, int pnx, ShotGeo &sg) {
+  // the map is separable and local: smooth a small window around the spike
+  const int r = 6;
+  const int x_lo = std::max(0, sx - r), x_hi = std::min(pnx - 1, sx + r);
+  const int z_lo = std::max(0, sz - r), z_hi = std::min(pnz - 1, sz + r);
+  // the fold reflections need the full line when the spike is near an edge
+  const bool full = x_lo == 0 || z_lo == 0 || x_hi == pnx - 1 || z_hi == pnz - 1;
+  std::vector<float> m, tmp;
+  int zs, xs, nzw, nxw;
+  if (full) { zs = 0; xs = 0; nzw = pnz; nxw = pnx; }
+  else { zs = z_lo; xs = x_lo; nzw = z_hi - z_lo + 1; nxw = x_hi - x_lo + 1; }
+  // smoothing a window equals smoothing the full line when the window
+  // holds the whole support (rect 2 spreads one cell each way)
+  m.assign((size_t)nzw * nxw, 0.f);
+  m[(size_t)(sx - xs) * nzw + (sz - zs)] = 1.f;
+  for (int j = 0; j < nxw; j++) smooth_line_host(2, nzw, m.data(), (long long)j * nzw, 1, tmp);
+  for (int j = 0; j < nzw; j++) smooth_line_host(2, nxw, m.data(), j, nzw, tmp);
+  sg.nsrc = 0;
+  for (int ix = 0; ix < nxw; ix++)
+    for (int iz = 0; iz < nzw; iz++) {
+      const float w = m[(size_t)ix * nzw + iz];
+      if (w != 0.f) {
+        PW_CHECK(sg.nsrc < MAXSRCW, PW_ERR_SHAPE, "source map has too many cells");
+        const int gz = iz + zs, gx = ix + xs;
+        PW_CHECK(gz >= 4 && gz < pnz - 4 && gx >= 4 && gx < pnx - 4, PW_ERR_SHAPE,
+                 "source map reaches the zero border of the padded grid");
+        sg.scell[sg.nsrc] = (gx << 16) | gz;
+        sg.sw[sg.nsrc] = w;
+        sg.nsrc++;
+      }
+    }
+  return PW_OK;
+}
+
+struct Setup {
+  pw_fwi_args a;
+  int pnz, pnx, lz;
+  long long fstride;  // floats per field (incl. halo)
+  int nr, rz, drv, sz;
+  std::vector<ShotGeo> geo;
+  std::vector<float> bz, bx;
+  int zw, xch;
+  dim3 grid;
+  size_t smem;
+};
+
+static int setup(const pw_fwi_args *a, Setup &S) {
+  PW_CHECK(a != nullptr, PW_ERR_VALUE, "null args");
+  S.a = *a;
+  PW_CHECK(a->nz >= 1 && a->nx >= 1 && a->nt >= 1 && a->ns >= 1 && a->nb >= 1, PW_ERR_SHAPE,
+           "sizes must be positive (nz=%d nx=%d nt=%d ns=%d nb=%d)", a->nz, a->nx, a->nt, a->ns,
+           a->nb);
+  PW_CHECK(a->dx > 0 && a->dz > 0 && a->dt > 0, PW_ERR_VALUE, "spacings must be positive");
+  const int nb = a->nb;
+  S.pnz = a->nz + 2 * nb;
+  S.pnx = a->nx + 2 * nb;
+  PW_CHECK(S.pnx < 65536 && S.pnz < 65536, PW_ERR_SHAPE, "grid too large");
+  S.lz = (int)round_up(HZ + round_up(S.pnz, 4) + 4, 32);
+  S.fstride = (long long)S.lz * (S.pnx + 2 * HX) + 64;
+  // preparation (wave_fwiutil.c:31-71) with pfwi.c's fixed acquisition
+  std::vector<float> bc(nb);
+  for (int i = 0; i < nb; i++) {
+    float tmp = a->coef * (nb - i);
+    bc[i] = expf(-tmp * tmp);
+  }
+  auto axis = [&](int n, std::vector<float> &f) {
+    f.assign(n, 1.f);
+    for (int i = 0; i < nb; i++) f[i] = bc[i];
+    for (int i = n - nb; i < n; i++) f[i] = bc[n - i - 1];
+  };
+  axis(S.pnz, S.bz);
+  axis(S.pnx, S.bx);
+  const float dx = a->dx;
+  const int ds_v = (int)(a->ds / dx + 0.5);
+  const int s0_v = (int)(a->os / dx + 0.5 + nb);
+  S.sz = a->sz + nb;
+  S.rz = a->rz + nb;
+  S.nr = a->nx;
+  const float dr = dx, r0 = a->ox, x0 = a->ox;
+  S.drv = (int)(dr / dx + 0.5);
+  PW_CHECK(S.drv >= 1, PW_ERR_SHAPE, "receiver interval below one cell");
+  const float xend = x0 + (a->nx - 1) * dx;
+  S.geo.assign(a->ns, ShotGeo{});
+  for (int is = 0; is < a->ns; is++) {
+    ShotGeo &g = S.geo[is];
+    if (a->acqui_type == 1) {
+      g.r0v = (int)((r0 - x0) / dx + 0.5 + nb);
+      g.r02 = 0;
+      g.nr2 = S.nr;
+    } else {
+      const float sx = a->os + a->ds * is;
+      const float rbegin = (sx + r0 < x0) ? x0 : sx + r0;
+      float rend = sx + r0 + (S.nr - 1) * dr;
+      rend = (rend < xend) ? rend : xend;
+      g.r0v = (int)(rbegin / dx + 0.5 + nb);
+      g.r02 = (int)((rbegin - sx - r0) / dx + 0.5);
+      g.nr2 = (int)((rend - rbegin) / dx + 1.5);
+    }
+    PW_CHECK(g.r02 >= 0 && g.r02 + g.nr2 <= S.nr && g.r0v >= 0 &&
+                 g.r0v + (g.nr2 - 1) * S.drv < S.pnx,
+             PW_ERR_SHAPE, "shot %d: receivers outside the grid", is);
+    const int sx = s0_v + is * ds_v;
+    PW_CHECK(sx >= 0 && sx < S.pnx && S.sz >= 0 && S.sz < S.pnz, PW_ERR_SHAPE,
+             "shot %d: source (x=%d, z=%d) outside the padded grid", is, sx, S.sz);
+    PW_TRY(source_map(sx, S.sz, S.pnz, S.pnx, g));
+  }
+  PW_CHECK(S.rz >= 4 && S.rz < S.pnz - 4, PW_ERR_SHAPE, "receiver depth in the zero border");
+  // tile: one z segment of ZW float4 (whole column when it fits)
+  const int nz4 = ceil_div(S.pnz, 4);
+  S.zw = nz4 <= 64 ? 64 : 128;
+  const int ztiles = ceil_div(nz4, S.zw);
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  // planes per CTA: enough CTAs to fill every SM a few times
+  int xch = 64;
+  while (xch > 8 && (long long)ztiles * ceil_div(S.pnx, xch) < 4LL * nsm) xch /= 2;
+  S.xch = xch;
+  S.grid = dim3(ceil_div(S.pnx, xch), ztiles);
+  return PW_OK;
+}
+
+constexpr int PFP = 3;  // prefetch depth (planes)
+
+static size_t smem_for(int zw, int mode) {
+  return sizeof(float4) * ((size_t)(PFP + 10) * (zw + 2) + (size_t)(mode == ADJ_EXACT ? 3 : 2) *
+                                                               (PFP + 2) * zw);
+}
+
+template <int ZW, int MODE>
+static int launch_one(const Setup &S, const PfArgs &p, cudaStream_t st) {
+  const size_t smem = smem_for(ZW, MODE);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(pf_step_kernel<ZW, PFP, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr = true;
+  }
+  pf_step_kernel<ZW, PFP, MODE><<<S.grid, ZW, smem, st>>>(p, S.xch);
+  PW_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+static int launch(const Setup &S, const PfArgs &p, int mode, cudaStream_t st) {
+  if (S.zw == 64) {
+    if (mode == FWD) return launch_one<64, FWD>(S, p, st);
+    if (mode == ADJ_REF) return launch_one<64, ADJ_REF>(S, p, st);
+    return launch_one<64, ADJ_EXACT>(S, p, st);
+  }
+  if (mode == FWD) return launch_one<128, FWD>(S, p, st);
+  if (mode == ADJ_REF) return launch_one<128, ADJ_REF>(S, p, st);
+  return launch_one<128, ADJ_EXACT>(S, p, st);
+}
+
+static void base_args(const Setup &S, PfArgs &p) {
+  memset(&p, 0, sizeof p);
+  p.pnz = S.pnz;
+  p.pnx = S.pnx;
+  p.lz = S.lz;
+  p.nb = S.a.nb;
+  p.nz = S.a.nz;
+  p.nx = S.a.nx;
+  const float c0 = -205. / 72, c1 = 8. / 5, c2 = -1. / 5, c3 = 8. / 315, c4 = -1. / 560;
+  p.c0 = c0; p.c1 = c1; p.c2 = c2; p.c3 = c3; p.c4 = c4;
+  p.dx2 = S.a.dx * S.a.dx;
+  p.dz2 = S.a.dz * S.a.dz;
+  p.nt = S.a.nt;
+  p.rz = S.rz;
+  p.drv = S.drv;
+  p.nr = S.nr;
+  p.fstride = S.fstride;
+}
+
+}  // namespace pf
+}  // namespace pw
+
+using namespace pw;
+using namespace pw::pf;
 
 extern "C" int pw_fwi_args_from_pararray(const float *p, int n, pw_fwi_args *o) {
   PW_CHECK(p && o && n >= 20, PW_ERR_VALUE, "pararray needs 20 values");
@@ -8,22 +650,450 @@ extern "C" int pw_fwi_args_from_pararray(const float *p, int n, pw_fwi_args *o) 
   o->nt = (int)p[6]; o->dt = p[7]; o->ot = p[8]; o->ns = (int)p[10]; o->ds = p[11];
   o->os = p[12]; o->nb = (int)p[14]; o->coef = p[15]; o->f0 = p[16];
   o->acqui_type = (int)p[17]; o->interval = (int)p[18]; o->niter = (int)p[19];
-  o->sz = 5; o->rz = 1;
+  o->sz = 5; o->rz = 1;  // pfwi.c:796-800
   return PW_OK;
 }
 
-extern "C" int pw_pfwi_forward(const pw_fwi_args *, const float *, const float *, float *, void *) {
-  pw::set_error("pw_pfwi_forward: not built yet");
-  return PW_ERR_SHAPE;
+// --------------------------------------------------------------- drivers --
+namespace pw {
+namespace pf {
+
+// residual_weighting with oreo=false as fwic sets it up (wave_fwiutil.c:225-296,
+// pfwi.c:849-855): 1 inside, 10-sample sine tapers on both axes.  [nr][nt].
+static void residual_weights(const pw_fwi_args &a, int nr, std::vector<float> &w) {
+  const int nt = a.nt;
+  const float t0 = a.ot, dt = a.dt, r0 = a.ox, dr = a.dx;
+  const float wt1 = t0, wt2 = t0 + (nt - 1) * dt;
+  const float woff1 = r0, woff2 = r0 + (nr - 1) * dr;
+  const int wtn1 = (int)((wt1 - t0) / dt + 0.5), wtn2 = (int)((wt2 - t0) / dt + 0.5);
+  const int woffn1 = (int)((woff1 - r0) / dr + 0.5), woffn2 = (int)((woff2 - r0) / dr + 0.5);
+  float s[10];
+  for (int i = 0; i < 10; i++) s[i] = sinf(0.5 * M_PI * (i + 1) / 11.);
+  w.assign((size_t)nr * nt, 0.f);
+  auto W = [&](int ir, int it) -> float & { return w[(size_t)ir * nt + it]; };
+  for (int ir = woffn1; ir <= woffn2; ir++)
+    for (int it = wtn1; it <= wtn2; it++) W(ir, it) = 1.f;
+  for (int ir = 0; ir < 10; ir++)
+    for (int it = wtn1; it <= wtn2; it++) {
+      W(woffn1 + ir, it) *= s[ir];
+      W(woffn2 - ir, it) *= s[ir];
+    }
+  for (int it = 0; it < 10; it++)
+    for (int ir = woffn1; ir <= woffn2; ir++) {
+      W(ir, wtn1 + it) *= s[it];
+      W(ir, wtn2 - it) *= s[it];
+    }
 }
 
-extern "C" int pw_pfwi_gradient(const pw_fwi_args *, int, const float *, const float *,
-                                const float *, const float *, float *, double *, int, void *) {
-  pw::set_error("pw_pfwi_gradient: not built yet");
-  return PW_ERR_SHAPE;
+struct Fields {
+  float *V = nullptr;
+  float *A = nullptr, *B = nullptr;  // [nshots][fstride] each
+  ShotGeo *geo = nullptr;
+  float *bz = nullptr, *bx = nullptr, *wav = nullptr;
+};
+
+// Common device state of a call: V, the two wavefield sets, geometry.
+static int bind_common(const Setup &S, int nsb, Carve &cv, size_t &o_V, size_t &o_A, size_t &o_B,
+                       size_t &o_geo, size_t &o_bz, size_t &o_bx, size_t &o_wav) {
+  o_V = cv.add(S.fstride * 4);
+  o_A = cv.add((size_t)nsb * S.fstride * 4);
+  o_B = cv.add((size_t)nsb * S.fstride * 4);
+  o_geo = cv.add(sizeof(ShotGeo) * S.a.ns);
+  o_bz = cv.add(S.bz.size() * 4);
+  o_bx = cv.add(S.bx.size() * 4);
+  o_wav = cv.add((size_t)S.a.nt * 4);
+  return PW_OK;
 }
 
-extern "C" int pw_gradient_postprocess(int, int, int, int, float *, float *, int, void *) {
-  pw::set_error("pw_gradient_postprocess: not built yet");
-  return PW_ERR_SHAPE;
+static int upload_common(const Setup &S, char *base, size_t o_geo, size_t o_bz, size_t o_bx,
+                         size_t o_wav, const float *wav, bool host, cudaStream_t st) {
+  PW_CUDA(cudaMemcpyAsync(base + o_geo, S.geo.data(), sizeof(ShotGeo) * S.a.ns,
+                          cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_bz, S.bz.data(), S.bz.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_bx, S.bx.data(), S.bx.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_TRY(to_device(base + o_wav, wav, (size_t)S.a.nt * 4, host, st));
+  return PW_OK;
+}
+
+static int check_vel_cfl(const Setup &S, const float *vel_dev, size_t n, cudaStream_t st,
+                         unsigned *scratch) {
+  // largest velocity (CFL) and a flag for non-finite / non-positive values
+  PW_CUDA(cudaMemsetAsync(scratch, 0, 8, st));
+  vel_check_kernel<<<296, 256, 0, st>>>(vel_dev, (long long)n, scratch);
+  PW_CUDA(cudaGetLastError());
+  unsigned hv[2] = {0, 0};
+  PW_CUDA(cudaMemcpyAsync(hv, scratch, 8, cudaMemcpyDeviceToHost, st));
+  PW_CUDA(cudaStreamSynchronize(st));
+  float vmax;
+  memcpy(&vmax, &hv[0], 4);
+  PW_CHECK(hv[1] == 0 && vmax > 0.f, PW_ERR_VALUE, "velocity has non-finite or non-positive values");
+  if (S.a.flags & PW_NO_CFL_CHECK) return PW_OK;
+  // 8th-order leapfrog in 2-D: v dt / h <= 0.555 (measured limit)
+  const float hmin = std::min(S.a.dx, S.a.dz);
+  const float cfl = vmax * S.a.dt / hmin;
+  PW_CHECK(cfl <= 0.555f, PW_ERR_CFL, "unstable: vmax*dt/h = %g exceeds 0.555", cfl);
+  return PW_OK;
+}
+
+}  // namespace pf
+}  // namespace pw
+
+extern "C" int pw_pfwi_forward(const pw_fwi_args *a, const float *vel, const float *wav,
+                               float *data, void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  Setup S;
+  PW_TRY(setup(a, S));
+  const bool host = (a->flags & PW_HOST_PTRS) != 0;
+  const int ns = a->ns, nt = a->nt, nr = S.nr;
+  const int nsb = std::min(ns, MAXS);
+  const size_t nvel = (size_t)a->nz * a->nx;
+  Carve cv;
+  size_t o_V, o_A, o_B, o_geo, o_bz, o_bx, o_wav;
+  bind_common(S, nsb, cv, o_V, o_A, o_B, o_geo, o_bz, o_bx, o_wav);
+  const size_t o_vel = cv.add(host ? nvel * 4 : 0);
+  const size_t o_rec = cv.add((size_t)ns * nt * nr * 4);
+  const size_t o_out = cv.add(host ? (size_t)ns * nt * nr * 4 : 0);
+  const size_t o_mx = cv.add(16);
+  Workspace &ws = Workspace::for_current_device();
+  std::lock_guard<std::mutex> lock(ws.mutex());
+  PW_TRY(ws.reserve(cv.total()));
+  char *base = ws.base();
+  PW_CUDA(cudaMemsetAsync(base, 0, cv.total(), st));
+  const float *d_vel = vel;
+  if (host) {
+    PW_TRY(to_device(base + o_vel, vel, nvel * 4, true, st));
+    d_vel = at<float>(base, o_vel);
+  }
+  PW_TRY(check_vel_cfl(S, d_vel, nvel, st, at<unsigned>(base, o_mx)));
+  PW_TRY(upload_common(S, base, o_geo, o_bz, o_bx, o_wav, wav, host, st));
+  float *V = at<float>(base, o_V);
+  pad_V_kernel<<<1184, 256, 0, st>>>(d_vel, a->nz, a->nx, a->nb, S.pnz, S.pnx, S.lz, a->dt * a->dt, V);
+  PW_CUDA(cudaGetLastError());
+  float *rec = at<float>(base, o_rec);
+  PfArgs p;
+  base_args(S, p);
+  p.V = V;
+  p.bz = at<float>(base, o_bz);
+  p.bx = at<float>(base, o_bx);
+  p.wav = at<float>(base, o_wav);
+  LoopTimer timer(st);
+  timer.start();
+  long long launches = 0;
+  for (int s0 = 0; s0 < ns; s0 += nsb) {
+    const int nb_ = std::min(nsb, ns - s0);
+    float *A[MAXS], *B[MAXS];
+    for (int s = 0; s < nb_; s++) {
+      A[s] = at<float>(base, o_A) + (size_t)s * S.fstride;
+      B[s] = at<float>(base, o_B) + (size_t)s * S.fstride;
+    }
+    PW_CUDA(cudaMemsetAsync(base + o_A, 0, (size_t)nsb * S.fstride * 4, st));
+    PW_CUDA(cudaMemsetAsync(base + o_B, 0, (size_t)nsb * S.fstride * 4, st));
+    p.nshots = nb_;
+    p.geo = at<ShotGeo>(base, o_geo) + s0;
+    p.rec = rec + (size_t)s0 * nt * nr;
+    for (int it = 0; it < nt; it++) {
+      p.it = it;
+      for (int s = 0; s < nb_; s++) {
+        p.cur[s] = A[s];
+        p.nxt[s] = B[s];
+      }
+      PW_TRY(launch(S, p, FWD, st));
+      launches++;
+      for (int s = 0; s < nb_; s++) std::swap(A[s], B[s]);
+    }
+  }
+  timer.stop();
+  // [shot][nt][nr] -> [shot][nr][nt]
+  float *dst = host ? at<float>(base, o_out) : data;
+  for (int s = 0; s < ns; s++) {
+    dim3 tb(32, 8), tg(ceil_div(nr, 32), ceil_div(nt, 32));
+    transpose_kernel<<<tg, tb, 0, st>>>(rec + (size_t)s * nt * nr, dst + (size_t)s * nt * nr, nt, nr);
+  }
+  PW_CUDA(cudaGetLastError());
+  if (host) PW_TRY(to_host(data, dst, (size_t)ns * nt * nr * 4, true, st));
+  PW_CUDA(cudaStreamSynchronize(st));
+  timer.finish(launches, launches + 3 + ns);
+  return PW_OK;
+}
+
+// Checkpoint interval of the exact gradient: the segment buffer holds k term
+// fields per shot and the checkpoints two fields every k steps, so
+// k = sqrt(2 nt) minimises their sum; the shot batch shrinks until the whole
+// working set fits the HBM budget (80% of the free memory).
+static void plan_exact(const Setup &S, int ckpt_k, int &k, int &nsb) {
+  const int nt = S.a.nt;
+  k = ckpt_k > 0 ? ckpt_k : std::max(1, (int)std::lround(std::sqrt(2.0 * nt)));
+  k = std::min(k, nt);
+  size_t freeb = 0, totb = 0;
+  if (cudaMemGetInfo(&freeb, &totb) != cudaSuccess) {
+    cudaGetLastError();
+    freeb = (size_t)32 << 30;
+  }
+  const double budget = 0.8 * (double)freeb;
+  const double fb = (double)S.fstride * 4;
+  nsb = std::min(S.a.ns, MAXS);
+  while (nsb > 1) {
+    const int nck = (nt + k - 1) / k;
+    const double need = fb * nsb * (4.0 + 2.0 * nck + k) + fb * 2;
+    if (need <= budget) break;
+    nsb = (nsb + 1) / 2;
+  }
+}
+
+extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const float *wav,
+                                const float *dobs, const float *weight, float *grad,
+                                double *misfit, int ckpt_k, void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  PW_CHECK(mode == PW_GRAD_REFERENCE || mode == PW_GRAD_EXACT, PW_ERR_VALUE, "bad gradient mode");
+  Setup S;
+  PW_TRY(setup(a, S));
+  const bool host = (a->flags & PW_HOST_PTRS) != 0;
+  const bool per_shot = (a->flags & PW_PER_SHOT) != 0;
+  const int ns = a->ns, nt = a->nt, nr = S.nr, nz = a->nz, nx = a->nx;
+  const size_t nvel = (size_t)nz * nx;
+  const bool exact = mode == PW_GRAD_EXACT;
+  const int interval = std::max(1, a->interval);
+  const int wnt = (nt - 1) / interval + 1;
+  int k = 0, nsb = per_shot ? 1 : std::min(ns, MAXS);
+  if (exact) {
+    plan_exact(S, ckpt_k, k, nsb);
+    if (per_shot) nsb = 1;
+  }
+  const int nck = exact ? (nt + k - 1) / k : 0;
+  std::vector<float> wts;
+  if (weight == nullptr) residual_weights(*a, nr, wts);
+
+  Carve cv;
+  size_t o_V, o_A, o_B, o_geo, o_bz, o_bx, o_wav;
+  bind_common(S, nsb, cv, o_V, o_A, o_B, o_geo, o_bz, o_bx, o_wav);
+  const size_t o_vel = cv.add(host ? nvel * 4 : 0);
+  const size_t o_w = cv.add((size_t)nr * nt * 4);
+  const size_t o_dobs = cv.add((size_t)ns * nt * nr * 4);    // [shot][nt][nr]
+  const size_t o_dobs_in = cv.add(host ? (size_t)ns * nt * nr * 4 : 0);
+  const size_t o_d = cv.add((size_t)nsb * nt * nr * 4);      // recorded [shot][nt][nr]
+  const size_t o_res = cv.add((size_t)nsb * nt * nr * 4);
+  const size_t o_snap = cv.add(exact ? 0 : (size_t)nsb * wnt * nvel * 4);
+  const size_t o_ck = cv.add(exact ? (size_t)nsb * nck * 2 * S.fstride * 4 : 0);
+  const size_t o_tb = cv.add(exact ? (size_t)nsb * k * S.fstride * 4 : 0);
+  const size_t o_ga = cv.add(exact ? (size_t)S.fstride * 4 : 0);
+  const size_t o_grad = cv.add(nvel * 4);
+  const size_t o_mis = cv.add(16);
+  const size_t o_mx = cv.add(16);
+  Workspace &ws = Workspace::for_current_device();
+  std::lock_guard<std::mutex> lock(ws.mutex());
+  PW_TRY(ws.reserve(cv.total()));
+  char *base = ws.base();
+  PW_CUDA(cudaMemsetAsync(base, 0, cv.total(), st));
+  const float *d_vel = vel;
+  if (host) {
+    PW_TRY(to_device(base + o_vel, vel, nvel * 4, true, st));
+    d_vel = at<float>(base, o_vel);
+  }
+  PW_TRY(check_vel_cfl(S, d_vel, nvel, st, at<unsigned>(base, o_mx)));
+  PW_TRY(upload_common(S, base, o_geo, o_bz, o_bx, o_wav, wav, host, st));
+  if (weight) PW_TRY(to_device(base + o_w, weight, (size_t)nr * nt * 4, host, st));
+  else PW_CUDA(cudaMemcpyAsync(base + o_w, wts.data(), wts.size() * 4, cudaMemcpyHostToDevice, st));
+  {
+    // dobs [shot][nr][nt] -> [shot][nt][nr]
+    const float *src = dobs;
+    if (host) {
+      PW_TRY(to_device(base + o_dobs_in, dobs, (size_t)ns * nt * nr * 4, true, st));
+      src = at<float>(base, o_dobs_in);
+    }
+    for (int s = 0; s < ns; s++) {
+      dim3 tb(32, 8), tg(ceil_div(nt, 32), ceil_div(nr, 32));
+      transpose_kernel<<<tg, tb, 0, st>>>(src + (size_t)s * nr * nt,
+                                          at<float>(base, o_dobs) + (size_t)s * nt * nr, nr, nt);
+    }
+    PW_CUDA(cudaGetLastError());
+  }
+  float *V = at<float>(base, o_V);
+  pad_V_kernel<<<1184, 256, 0, st>>>(d_vel, nz, nx, a->nb, S.pnz, S.pnx, S.lz, a->dt * a->dt, V);
+  PW_CUDA(cudaGetLastError());
+  float *gdev = at<float>(base, o_grad);
+  float *gacc = at<float>(base, o_ga);
+  double *dmis = at<double>(base, o_mis);
+  PfArgs p;
+  base_args(S, p);
+  p.V = V;
+  p.bz = at<float>(base, o_bz);
+  p.bx = at<float>(base, o_bx);
+  p.wav = at<float>(base, o_wav);
+  p.vint = d_vel;
+  p.wdt2 = (a->dt * interval) * (a->dt * interval);
+  p.grad = exact ? gacc : gdev;
+  const size_t fs = (size_t)S.fstride;
+  long long launches = 0;
+  LoopTimer timer(st);
+  timer.start();
+  for (int s0 = 0; s0 < ns; s0 += nsb) {
+    const int nb_ = std::min(nsb, ns - s0);
+    float *A[MAXS], *B[MAXS];
+    auto reset = [&]() -> int {
+      for (int s = 0; s < nb_; s++) {
+        A[s] = at<float>(base, o_A) + s * fs;
+        B[s] = at<float>(base, o_B) + s * fs;
+      }
+      PW_CUDA(cudaMemsetAsync(base + o_A, 0, (size_t)nsb * fs * 4, st));
+      PW_CUDA(cudaMemsetAsync(base + o_B, 0, (size_t)nsb * fs * 4, st));
+      return PW_OK;
+    };
+    auto step = [&](int mode_, int it) -> int {
+      p.it = it;
+      for (int s = 0; s < nb_; s++) {
+        p.cur[s] = A[s];
+        p.nxt[s] = B[s];
+      }
+      PW_TRY(launch(S, p, mode_, st));
+      launches++;
+      for (int s = 0; s < nb_; s++) std::swap(A[s], B[s]);
+      return PW_OK;
+    };
+    p.nshots = nb_;
+    p.geo = at<ShotGeo>(base, o_geo) + s0;
+    float *dd = at<float>(base, o_d);
+    float *res = at<float>(base, o_res);
+    float *ck = at<float>(base, o_ck);
+    float *tb = at<float>(base, o_tb);
+    float *snap = at<float>(base, o_snap);
+    // ---- forward: traces, and snapshots (reference) or checkpoints (exact)
+    PW_TRY(reset());
+    p.rec = dd;
+    p.tout = nullptr;
+    p.snap_stride = (long long)wnt * nvel;
+    for (int it = 0; it < nt; it++) {
+      if (exact && it % k == 0) {
+        const int m = it / k;
+        for (int s = 0; s < nb_; s++) {
+          float *c = ck + ((size_t)s * nck + m) * 2 * fs;
+          PW_CUDA(cudaMemcpyAsync(c, A[s], fs * 4, cudaMemcpyDeviceToDevice, st));
+          PW_CUDA(cudaMemcpyAsync(c + fs, B[s], fs * 4, cudaMemcpyDeviceToDevice, st));
+        }
+      }
+      p.snap = (!exact && it % interval == 0) ? snap + (size_t)(it / interval) * nvel : nullptr;
+      PW_TRY(step(FWD, it));
+    }
+    p.rec = nullptr;
+    p.snap = nullptr;
+    // ---- residual and FP64 misfit
+    residual_kernel<<<592, 256, 0, st>>>(dd, at<float>(base, o_dobs) + (size_t)s0 * nt * nr,
+                                         at<float>(base, o_w), res, nb_, nt, nr, exact ? 1 : 0, dmis);
+    PW_CUDA(cudaGetLastError());
+    p.res = res;
+    if (!exact) {
+      // ---- backward with gradient_av's imaging (wave_fwigradient.c:201-241)
+      PW_TRY(reset());
+      p.wstride = (long long)wnt * nvel;
+      for (int it = nt - 1; it >= 0; it--) {
+        const int wit = it / interval;
+        p.imaging = (it % interval == 0) && wit != wnt - 1 && wit != 0;
+        if (p.imaging) {
+          p.wprev = snap + (size_t)(wit - 1) * nvel;
+          p.wcur = snap + (size_t)wit * nvel;
+          p.wnext = snap + (size_t)(wit + 1) * nvel;
+        }
+        PW_TRY(step(ADJ_REF, it));
+      }
+    } else {
+      // ---- backward by segments: restore checkpoint, recompute the forward
+      // terms of the segment, run the exact adjoint over it
+      float *PA[MAXS], *PB[MAXS];
+      for (int s = 0; s < nb_; s++) {
+        PA[s] = at<float>(base, o_A) + s * fs;  // reused: adjoint after the forward
+        PB[s] = at<float>(base, o_B) + s * fs;
+      }
+      // the adjoint needs its own pair; the forward recompute restores from
+      // the checkpoints into the segment buffer's first two slots
+      PW_CUDA(cudaMemsetAsync(base + o_A, 0, (size_t)nsb * fs * 4, st));
+      PW_CUDA(cudaMemsetAsync(base + o_B, 0, (size_t)nsb * fs * 4, st));
+      float *adjA[MAXS], *adjB[MAXS];
+      for (int s = 0; s < nb_; s++) {
+        adjA[s] = PA[s];
+        adjB[s] = PB[s];
+      }
+      p.tout_stride = (long long)k * fs;
+      p.tin_stride = (long long)k * fs;
+      for (int m = nck - 1; m >= 0; m--) {
+        const int n0 = m * k, n1 = std::min(nt, n0 + k);
+        // recompute: fwd pair lives in checkpoint m (overwritten, no longer needed)
+        float *FA[MAXS], *FB[MAXS];
+        for (int s = 0; s < nb_; s++) {
+          FA[s] = ck + ((size_t)s * nck + m) * 2 * fs;
+          FB[s] = FA[s] + fs;
+        }
+        for (int n = n0; n < n1; n++) {
+          p.it = n;
+          for (int s = 0; s < nb_; s++) {
+            p.cur[s] = FA[s];
+            p.nxt[s] = FB[s];
+          }
+          p.tout = tb + (size_t)(n - n0) * fs;
+          PW_TRY(launch(S, p, FWD, st));
+          launches++;
+          for (int s = 0; s < nb_; s++) std::swap(FA[s], FB[s]);
+        }
+        p.tout = nullptr;
+        for (int n = n1 - 1; n >= n0; n--) {
+          p.it = n;
+          for (int s = 0; s < nb_; s++) {
+            p.cur[s] = adjA[s];
+            p.nxt[s] = adjB[s];
+          }
+          p.tin = tb + (size_t)(n - n0) * fs;
+          p.imaging = 1;
+          PW_TRY(launch(S, p, ADJ_EXACT, st));
+          launches++;
+          for (int s = 0; s < nb_; s++) std::swap(adjA[s], adjB[s]);
+        }
+      }
+      p.tin = nullptr;
+      p.imaging = 0;
+    }
+  }
+  timer.stop();
+  if (exact) {
+    fold_grad_kernel<<<592, 256, 0, st>>>(gacc, d_vel, nz, nx, a->nb, S.pnz, S.pnx, S.lz, gdev);
+    PW_CUDA(cudaGetLastError());
+  }
+  PW_TRY(to_host(grad, gdev, nvel * 4, host, st));
+  if (misfit) PW_CUDA(cudaMemcpyAsync(misfit, dmis, 8, cudaMemcpyDeviceToHost, st));
+  PW_CUDA(cudaStreamSynchronize(st));
+  timer.finish(launches, launches + 8);
+  return PW_OK;
+}
+
+extern "C" int pw_gradient_postprocess(int nz, int nx, int rect, int waterz, float *grad,
+                                       float *scaling, int flags, void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  PW_CHECK(nz >= 1 && nx >= 1 && grad && scaling, PW_ERR_VALUE, "bad arguments");
+  const bool host = (flags & PW_HOST_PTRS) != 0;
+  const size_t n = (size_t)nz * nx;
+  Carve cv;
+  const size_t o_g = cv.add(host ? n * 4 : 0);
+  const size_t o_tmp = cv.add(rect > 1 ? (size_t)std::max(nz, nx) * (std::max(nz, nx) + 2 * rect) * 4 : 0);
+  const size_t o_mx = cv.add(16);
+  const size_t o_sc = cv.add(16);
+  Workspace &ws = Workspace::for_current_device();
+  std::lock_guard<std::mutex> lock(ws.mutex());
+  PW_TRY(ws.reserve(cv.total()));
+  char *base = ws.base();
+  float *g = host ? at<float>(base, o_g) : grad;
+  if (host) PW_TRY(to_device(g, grad, n * 4, true, st));
+  unsigned *mx = at<unsigned>(base, o_mx);
+  float *sc = at<float>(base, o_sc);
+  PW_CUDA(cudaMemsetAsync(mx, 0, 4, st));
+  PW_CUDA(cudaMemcpyAsync(sc, scaling, 4, host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+  // the first-call scale comes from the raw gradient (wave_fwigradient.c:245-251)
+  absmax_kernel<<<296, 256, 0, st>>>(g, (long long)n, mx);
+  if (rect > 1) {
+    float *tmp = at<float>(base, o_tmp);
+    smooth_lines_kernel<<<ceil_div(nx, 128), 128, 0, st>>>(g, nx, nz, nz, 1, rect, tmp);
+    smooth_lines_kernel<<<ceil_div(nz, 128), 128, 0, st>>>(g, nz, nx, 1, nz, rect, tmp);
+  }
+  finish_kernel<<<296, 256, 0, st>>>(g, nz, nx, waterz, mx, sc);
+  PW_CUDA(cudaGetLastError());
+  if (host) PW_TRY(to_host(grad, g, n * 4, true, st));
+  PW_CUDA(cudaMemcpyAsync(scaling, sc, 4, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
+  PW_CUDA(cudaStreamSynchronize(st));
+  return PW_OK;
 }

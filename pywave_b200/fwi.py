@@ -1,0 +1,106 @@
+"""FWI gradient on the GPU engine: the reference's gradient_av imaging and the
+exact discrete adjoint, and a ``torch.autograd.Function`` mapping velocity to
+the data misfit.
+
+The exact adjoint back-propagates the weighted residual with the forward
+scheme's own transpose (sponge and edge-replicated padding included) and
+images with the zero-lag condition fused into the adjoint step kernel:
+    dJ/dv = pad2d^T( 2/v * sum_n phi_n * (Lap8 a_n + r w_n) ).
+Memory is capped by checkpoints of the forward state every k steps and a
+per-segment recompute (k from the planner when ``ckpt_k=0``).
+
+Arrays follow pfwi: velocity (nz, nx), wavelet (nt,), data (nt, nr, ns).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+try:
+    import torch
+except ImportError:  # pragma: no cover
+    torch = None
+
+
+def fwi_args(par, flags=0):
+    """pw_fwi_args from a pfwi ``par`` dictionary (after fillpar)."""
+    from .pfwi import pararray, fillpar
+    arr = pararray(fillpar(dict(par)))
+    a = L.FwiArgs()
+    L.check(L.lib().pw_fwi_args_from_pararray(L.ptr(arr), int(arr.size), a))
+    a.flags = flags
+    return a
+
+
+def _data_flat(dobs):
+    # (nt, nr, ns) -> [ns][nr][nt]
+    return np.ascontiguousarray(np.asarray(dobs, np.float32).flatten(order="F"))
+
+
+def gradient(vel, wav, dobs, par, mode="exact", ckpt_k=0, per_shot=False, weight=None):
+    """FWI gradient dJ/dv (nz, nx) and the FP64 misfit, host arrays in/out.
+
+    mode "reference": gradient_av's imaging (wave_fwigradient.c:93-242) before
+    its smoothing / scaling; misfit 0.5*sum((dobs-d)^2).
+    mode "exact": exact adjoint of the scheme; misfit 0.5*sum(w*(d-dobs)^2).
+    weight: (nr, nt) residual weights, default the reference's tapers."""
+    flags = L.PW_HOST_PTRS | (L.PW_PER_SHOT if per_shot else 0)
+    a = fwi_args(par, flags)
+    v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F"))
+    w = np.ascontiguousarray(np.asarray(wav, np.float32).reshape(-1))
+    d = _data_flat(dobs)
+    wt = None if weight is None else np.ascontiguousarray(np.asarray(weight, np.float32))
+    g = np.empty(a.nz * a.nx, np.float32)
+    J = ctypes.c_double(0.0)
+    m = L.PW_GRAD_EXACT if mode == "exact" else L.PW_GRAD_REFERENCE
+    L.check(L.lib().pw_pfwi_gradient(a, m, L.ptr(v), L.ptr(w), L.ptr(d), L.ptr(wt), L.ptr(g),
+                                     ctypes.byref(J), int(ckpt_k), None))
+    return g.reshape(a.nz, a.nx, order="F"), J.value
+
+
+def postprocess(grad, rect=3, waterz=0, scaling=None):
+    """gradient_av's tail: triangle smoothing and the (first-call) scale."""
+    g = np.ascontiguousarray(np.asarray(grad, np.float32).flatten(order="F"))
+    nz, nx = np.asarray(grad).shape
+    sc = ctypes.c_float(0.0 if scaling is None else float(scaling))
+    L.check(L.lib().pw_gradient_postprocess(nz, nx, rect, waterz, L.ptr(g), ctypes.byref(sc),
+                                            L.PW_HOST_PTRS, None))
+    return g.reshape(nz, nx, order="F"), sc.value
+
+
+if torch is not None:
+
+    class FwiMisfit(torch.autograd.Function):
+        """J(v) = 0.5 * sum(w * (d(v) - dobs)^2) over all shots, J in FP64.
+
+        forward(vel (nz, nx) CUDA float32, wav (nt,), dobs (ns, nr, nt) CUDA
+        float32, par dict, ckpt_k) runs the forward and the exact adjoint in
+        one pass and keeps dJ/dv for backward."""
+
+        @staticmethod
+        def forward(ctx, vel, wav, dobs, par, ckpt_k=0, weight=None):
+            a = fwi_args(par, 0)
+            v = vel.detach().t().contiguous().float()          # [nx][nz]
+            w = wav.detach().contiguous().float()
+            d = dobs.detach().contiguous().float()              # [ns][nr][nt]
+            wt = None if weight is None else weight.detach().contiguous().float()
+            g = torch.empty_like(v)
+            J = ctypes.c_double(0.0)
+            s = torch.cuda.current_stream(v.device).cuda_stream
+            L.check(L.lib().pw_pfwi_gradient(a, L.PW_GRAD_EXACT, v.data_ptr(), w.data_ptr(),
+                                             d.data_ptr(), None if wt is None else wt.data_ptr(),
+                                             g.data_ptr(), ctypes.byref(J), int(ckpt_k), s))
+            ctx.save_for_backward(g.t())
+            return torch.tensor(J.value, dtype=torch.float64, device=vel.device)
+
+        @staticmethod
+        def backward(ctx, gJ):
+            (g,) = ctx.saved_tensors
+            return (g * gJ.to(g.dtype)), None, None, None, None, None
+
+    def fwi_misfit(vel, wav, dobs, par, ckpt_k=0, weight=None):
+        """Differentiable misfit (see FwiMisfit)."""
+        return FwiMisfit.apply(vel, wav, dobs, par, ckpt_k, weight)
