@@ -340,7 +340,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded velocity, sources and traces)",
             "config": {"workload": f"3-D TRI image {n}^3 h=10m nt={nt} nbt={NBT} groups={G} "
-                                   "jsnap=4 (BASELINE configuration 2)",
+                                   "jsnap=4",
                        "points_per_step": pts, "l2": "inputs larger than L2 (fields+traces "
                        f"{(cells * 4 * (2 * G + 2) + n * n * nt * 4) / 1e9:.2f} GB)",
                        "parallelism": f"replicas x{world} (one event per GPU)"},

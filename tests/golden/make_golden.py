@@ -108,7 +108,7 @@ def main():
                        az=[0, 20, 24], jsnap=4, dat=dg3, tri=True, verb=0, nbt=8, ct=0.02)
     np.savez_compressed(os.path.join(HERE, "afd3d_tri.npz"), vel=vel3, dat=dg3, snaps=wt3)
 
-    # ---- BASELINE config-1 receivers at z=5 (wfd[5].T with jsnap=1) ------
+    # ---- 201x201 three-layer gather, receivers at z=5 (wfd[5].T with jsnap=1) ------
     vc1 = layered(201, 201, [1500, 2200, 3000], [60, 130])
     _, wc1 = quiet(a2.afd2d, vc1, nt=1501, dt=0.001, ax=[0, 10, 201], az=[0, 10, 201], ns=1,
                    sx=[100], sz=[5], f=[20], t=[0.05], A=[1], nbt=30, ct=0.01, jsnap=1, verb=0)

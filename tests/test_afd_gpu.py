@@ -63,7 +63,7 @@ def test_afd3d_tri_bit_exact(golden, cuda_lib):
 
 
 def test_config1_gather_depth5(golden, oracle, cuda_lib):
-    """201x201 three-layer model, 20 Hz source at
+    """2-D three-layer gather: 201x201 model (1500/2200/3000 m/s), 20 Hz source at
     (z=5, x=100), receivers at z=5 on every x, nt=1501.  Bit-exact against
     the reference given its wavelet; <= 1e-5 with the closed-form Ricker; the
     error of both against the FP64 oracle is stated."""
