@@ -66,6 +66,33 @@ typedef struct pw_afd_args {
 int pw_afd(const pw_afd_args *a, const float *vel, const float *src, const float *wavelet,
            float *dat, float *wfd, void *stream);
 
+/* Size of the fixed device scratch array behind pw_afd_noalloc (32 MiB). */
+#define PW_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/* pw_afd's forward modelling (tri = 0) that allocates no device memory.
+ * No counterpart in the reference.  For callers that run inside a host
+ * framework owning every device allocation (a caching pool that must not be
+ * bypassed, a memory budget that a hidden allocation would break): pw_afd grows
+ * a cached workspace with cudaMalloc on first use, this entry point never does.
+ * Its wavefields, padded velocity, taper tables and trace buffer are carved
+ * from one file-scope __device__ array of PW_NOALLOC_SCRATCH_BYTES per device,
+ * whose address comes from cudaGetSymbolAddress; a model that needs more is
+ * rejected with PW_ERR_SHAPE before any device work (a 1000 x 1000 2-D model
+ * with nbt 30 and nt 2000 needs 21 MiB; a 50^3 3-D model with nbt 30 and
+ * nt 1000 needs 29 MiB).
+ *   Same arguments and results as pw_afd, with these differences: every
+ *   pointer is device memory (PW_HOST_PTRS is rejected); with ns > 0 both
+ *   src and wavelet [ns][nt] are required (no Ricker table is built);
+ *   pw_last_timing is not updated.
+ *   The wavefields and the halo of the padded velocity must start at zero:
+ *   each call clears the part of the array it uses on `stream` first.  Calls
+ *   whose GPU work overlapped would race on the one array; a per-device lock
+ *   held until the call's stream has drained keeps calls of one process from
+ *   overlapping.  The first call on a device loads the module holding the
+ *   array, so make it before any stream capture begins. */
+int pw_afd_noalloc(const pw_afd_args *a, const float *vel, const float *src,
+                   const float *wavelet, float *dat, float *wfd, void *stream);
+
 /* Time-reversal source imaging with G receiver groups propagated in lockstep
  * and the image fused into the time loop:
  *   img = sum_{it % jsnap == 0} prod_g u_g(it)^2        (then / max if normalize)

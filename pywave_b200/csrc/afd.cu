@@ -924,3 +924,212 @@ extern "C" int pw_tri_image(const pw_afd_args *a, int ngroups, const int *group,
   return pw::afd::run(&b, ngroups, group, vel, dat, nullptr, nullptr, nullptr, img, normalize,
                       (cudaStream_t)stream);
 }
+
+// ------------------------------------------------------ no-alloc variant --
+// pw_afd_noalloc: run()'s forward modelling with every scratch buffer carved
+// from the fixed device array of noalloc_scratch.cu instead of the cached
+// workspace, for callers that may not allocate device memory.  Same plan,
+// step kernel and launch sequence as run(); device pointers only.
+
+namespace pw {
+int noalloc_scratch(char **ptr);  // noalloc_scratch.cu
+
+namespace afd {
+
+// Per-cell taper factors of one axis from the nb face weights w: taper_axis
+// evaluated on the device.  Only copies of w are stored, so the table equals
+// the host-built one bit for bit.
+__global__ void taper_table_kernel(const float *w, int nb, int n, int n2, float *f) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float v = 1.f;
+    if (i < nb) v = w[i];
+    const int j = n2 - 1 - i;  // bottom/right face, indexed from the padded end
+    if (j >= 0 && j < nb) v = w[j];
+    f[i] = v;
+  }
+}
+
+constexpr int NOALLOC_MAXDEV = 64;
+
+static int run_noalloc(const pw_afd_args *a, const float *vel, const float *src,
+                       const float *wavelet, float *dat, float *wfd, cudaStream_t st) {
+  PW_CHECK(a != nullptr, PW_ERR_VALUE, "null args");
+  PW_CHECK((a->flags & PW_HOST_PTRS) == 0, PW_ERR_VALUE,
+           "pw_afd_noalloc takes device pointers only (PW_HOST_PTRS is set)");
+  PW_CHECK(a->tri == 0, PW_ERR_VALUE, "pw_afd_noalloc runs forward modelling only (tri = 0)");
+  PW_CHECK(vel != nullptr, PW_ERR_VALUE, "velocity is null");
+  Plan p;
+  PW_TRY(make_plan(a, false, p));
+  const Geo &g = p.g;
+  const bool two_d = p.dim == 2;
+  PW_CHECK(a->jsnap >= 0, PW_ERR_VALUE, "jsnap must be >= 0");
+  PW_CHECK(a->gz >= 0 && a->gz < a->nz, PW_ERR_SHAPE, "receiver depth gz=%d outside [0,%d)", a->gz,
+           a->nz);
+  const int nt = a->nt;
+  const int ns = a->ns;
+  PW_CHECK(ns >= 0 && ns <= MAXSRC, PW_ERR_SHAPE, "ns must be in [0,%d] (got %d)", MAXSRC, ns);
+  PW_CHECK(ns == 0 || (src != nullptr && wavelet != nullptr), PW_ERR_VALUE,
+           "pw_afd_noalloc needs the source array and the wavelet table [ns][nt] on the device");
+  const size_t nvel = (size_t)p.nz1 * p.nx1 * p.ny1;
+  const size_t nrec = (size_t)p.nx1 * p.ny1;
+  const size_t nfield = (size_t)g.sy * g.py + 64;
+
+  // scratch layout: run()'s buffers without the host staging ones
+  Carve cv;
+  const size_t o_vv = cv.add(nfield * 4);
+  const size_t o_A = cv.add(nfield * 4);
+  const size_t o_B = cv.add(nfield * 4);
+  const size_t o_w = cv.add((size_t)p.nb * 4);
+  const size_t o_t = cv.add((size_t)(g.nz + g.nx + g.ny) * 4);
+  const size_t o_rec = cv.add(dat ? (size_t)nt * nrec * 4 : 0);
+  const size_t o_mx = cv.add(16);
+  const size_t need = cv.total();
+  PW_CHECK(need <= (size_t)PW_NOALLOC_SCRATCH_BYTES, PW_ERR_SHAPE,
+           "pw_afd_noalloc needs %zu bytes of scratch; its fixed device array holds %zu "
+           "(pw_afd has no such limit)", need, (size_t)PW_NOALLOC_SCRATCH_BYTES);
+
+  int dev = 0;
+  PW_CUDA(cudaGetDevice(&dev));
+  PW_CHECK(dev >= 0 && dev < NOALLOC_MAXDEV, PW_ERR_VALUE, "device %d out of range", dev);
+  // one scratch array per device: a call holds the device's lock until its
+  // stream has drained, so calls never overlap on the array
+  static std::mutex locks[NOALLOC_MAXDEV];
+  std::lock_guard<std::mutex> lock(locks[dev]);
+  char *base = nullptr;
+  PW_TRY(noalloc_scratch(&base));
+  float *vv = at<float>(base, o_vv);
+  float *A = at<float>(base, o_A), *B = at<float>(base, o_B);
+  float *d_w = at<float>(base, o_w);
+  float *d_wz = at<float>(base, o_t), *d_wx = d_wz + g.nz, *d_wy = d_wx + g.nx;
+  float *rec = at<float>(base, o_rec);
+  unsigned int *mx = at<unsigned int>(base, o_mx);
+
+  // wavefields, the padded velocity's halo and the trace buffer start at zero
+  PW_CUDA(cudaMemsetAsync(base, 0, need, st));
+  PW_TRY(check_velocity(a, vel, nvel, mx, st));
+
+  // source positions, read back into a fixed host array
+  int ksz[MAXSRC], ksx[MAXSRC], ksy[MAXSRC];
+  if (ns > 0) {
+    const int rows = two_d ? 5 : 6;
+    float s[6 * MAXSRC];
+    PW_CUDA(cudaMemcpyAsync(s, src, (size_t)rows * ns * sizeof(float), cudaMemcpyDeviceToHost, st));
+    PW_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < ns; i++) {
+      // afd.c:416-425 (2-D) / 136-147 (3-D): positions are truncated to int
+      const int spx = (int)s[i];
+      const int spy = two_d ? 0 : (int)s[ns + i];
+      const int spz = (int)s[(two_d ? 1 : 2) * ns + i];
+      PW_CHECK(spx >= 0 && spx < p.nx1 && spz >= 0 && spz < p.nz1 && spy >= 0 && spy < p.ny1,
+               PW_ERR_SHAPE, "source %d at (z=%d,x=%d,y=%d) outside the model", i, spz, spx, spy);
+      PW_CHECK(p.nb >= 1 || (spx > 0 && spx < p.nx1 - 1 && spz > 0 && spz < p.nz1 - 1 &&
+                             (two_d || (spy > 0 && spy < p.ny1 - 1))),
+               PW_ERR_SHAPE, "source %d stencil leaves the grid", i);
+      ksz[i] = spz + p.nb;
+      ksx[i] = two_d ? 0 : spx + p.nb;
+      ksy[i] = two_d ? spx + p.nb : spy + p.nb;
+    }
+  }
+
+  // face weights abc_cal (wave_abc.c:141-143), staged through a fixed host
+  // buffer chunk by chunk, then expanded to per-cell tables on the device
+  {
+    float wb[256];
+    for (int i0 = 0; i0 < p.nb; i0 += 256) {
+      const int m = std::min(256, p.nb - i0);
+      for (int k = 0; k < m; k++) {
+        const int ib = i0 + k;
+        wb[k] = (float)exp(-a->ct * a->ct * (p.nb - 1 - ib) * (p.nb - 1 - ib));
+      }
+      PW_CUDA(cudaMemcpyAsync(d_w + i0, wb, (size_t)m * 4, cudaMemcpyHostToDevice, st));
+      PW_CUDA(cudaStreamSynchronize(st));
+    }
+  }
+  taper_table_kernel<<<ceil_div(g.nz, 256), 256, 0, st>>>(d_w, p.nb, g.nz, p.nz2, d_wz);
+  if (two_d) {
+    taper_table_kernel<<<1, 32, 0, st>>>(d_w, 0, 1, 1, d_wx);  // dummy axis: factor 1
+    taper_table_kernel<<<ceil_div(g.ny, 256), 256, 0, st>>>(d_w, p.nb, g.ny, p.nx2, d_wy);
+  } else {
+    taper_table_kernel<<<ceil_div(g.nx, 256), 256, 0, st>>>(d_w, p.nb, g.nx, p.nx2, d_wx);
+    taper_table_kernel<<<ceil_div(g.ny, 256), 256, 0, st>>>(d_w, p.nb, g.ny, p.ny2, d_wy);
+  }
+  PW_CUDA(cudaGetLastError());
+  expand_vv_kernel<<<1184, 256, 0, st>>>(g, vel, p.knz1, p.knx1, p.kny1, p.kbz, p.kbx, p.kby,
+                                         a->dt, vv);
+  PW_CUDA(cudaGetLastError());
+
+  // time loop: run()'s step arguments with one group
+  StepArgs s{};
+  s.g = g;
+  s.ych = p.ych;
+  s.ngroups = 1;
+  {
+    const float c0 = -30. / 12., c1 = +16. / 12., c2 = -1. / 12.;  // wave_fdm.c:15
+    s.c0 = c0;
+    s.c1 = c1;
+    s.c2 = c2;
+    const float idz = 1 / (a->dz * a->dz), idx = 1 / (a->dx * a->dx);
+    s.idz = idz;
+    if (two_d) {
+      s.idy = idx;
+      s.idx = 0.f;
+      s.k0 = idx + idz;
+    } else {
+      const float idy = 1 / (a->dy * a->dy);
+      s.idx = idx;
+      s.idy = idy;
+      s.k0 = (idy + idx) + idz;
+    }
+  }
+  s.vv = vv;
+  s.wz = d_wz;
+  s.wx = d_wx;
+  s.wy = d_wy;
+  s.nt = nt;
+  s.ns = ns;
+  for (int i = 0; i < ns; i++) {
+    s.sz[i] = ksz[i];
+    s.sx[i] = ksx[i];
+    s.sy[i] = ksy[i];
+  }
+  s.rick = wavelet;
+  s.rz = p.nb + a->gz;
+  if (two_d) {
+    s.rx0 = 0; s.nrx = 1; s.ry0 = p.nb; s.nry = p.nx1;
+  } else {
+    s.rx0 = p.nb; s.nrx = p.nx1; s.ry0 = p.nb; s.nry = p.ny1;
+  }
+  s.tri_dat = nullptr;
+  s.gid = nullptr;
+  s.rec = dat ? rec : nullptr;
+  s.nbz = p.kbz; s.nbx = p.kbx; s.nby = p.kby;
+  s.nz1 = p.knz1; s.nx1 = p.knx1; s.ny1 = p.kny1;
+  s.img = nullptr;
+  void *fn = pick_kernel(two_d, p.v, false);
+  const int threads = p.v.zw * p.v.tx;
+  for (int it = 0; it < nt; it++) {
+    s.it = it;
+    s.cur[0] = A;
+    s.nxt[0] = B;
+    const bool snap = a->jsnap > 0 && it % a->jsnap == 0;
+    s.wfd = (snap && wfd) ? wfd + (size_t)(it / a->jsnap) * nvel : nullptr;
+    void *args[] = {(void *)&s};
+    PW_CUDA(cudaLaunchKernel(fn, p.grid, dim3(threads), args, p.smem, st));
+    std::swap(A, B);
+  }
+  if (dat) {
+    dim3 tb2(32, 8), tg(ceil_div((long long)nrec, 32), ceil_div(nt, 32));
+    transpose_kernel<<<tg, tb2, 0, st>>>(rec, dat, nt, (long long)nrec);
+    PW_CUDA(cudaGetLastError());
+  }
+  PW_CUDA(cudaStreamSynchronize(st));
+  return PW_OK;
+}
+
+}  // namespace afd
+}  // namespace pw
+
+extern "C" int pw_afd_noalloc(const pw_afd_args *a, const float *vel, const float *src,
+                              const float *wavelet, float *dat, float *wfd, void *stream) {
+  return pw::afd::run_noalloc(a, vel, src, wavelet, dat, wfd, (cudaStream_t)stream);
+}
