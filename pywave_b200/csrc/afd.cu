@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 namespace pw {
 namespace afd {
@@ -59,6 +60,9 @@ struct StepArgs {
   Geo g;
   int ych;  // planes per CTA along y
   int ngroups;
+  int S, ZS, KX, nzc, WPC;  // march tile: slots per column, slots / columns per CTA, z chunks,
+                            // warps per column chunk
+  int WZ, WX;               // warp-tile kernel: warps per CTA along z and x (per group)
   float c0, c1, c2, idx, idy, idz, k0;
   const float *cur[MAXG];
   float *nxt[MAXG];
@@ -380,6 +384,512 @@ __global__ void __launch_bounds__(ZW *TX, TWO_D ? 1 : (ZW * TX >= 256 ? 2 : 3))
   }
 }
 
+// March kernel: register-marched, one float4 of z cells per thread.
+//
+// Lanes map onto (z float4 slot, group) with the G receiver groups of a TRI
+// launch interleaved (lane = slot_in_warp * G + group), warps onto z chunks
+// and x columns.  Slots of one column are contiguous in memory and the x
+// stride is the column length, so a warp touches G runs of consecutive 16-B
+// cells.  Each thread marches its float4 along y:
+//   * y neighbours: a 5-deep register queue;
+//   * z neighbours: shuffles from the adjacent slot's lane (loads at warp and
+//     chunk edges);
+//   * x neighbours (3-D): loads through L1 / L2;
+//   * the leading plane of A, the previous field B and vv: cp.async copies
+//     into a per-thread ring in shared memory, MARCH_NS - 1 planes ahead.
+// A thread only reads ring slots it filled itself, so no barrier is needed;
+// the TRI image product meets the groups of a cell in adjacent lanes and is
+// formed by shuffles.  Same float evaluation order as the reference.
+constexpr int MARCH_MAXT = 512;  // threads per CTA (launch bound)
+constexpr int MARCH_NS = 4;      // ring slots per stream: MARCH_NS - 1 planes in flight
+
+// 16-byte async copy allocating in L1 as well (cp.async.ca).
+__device__ __forceinline__ void cp16ca(float4 *dst, const float *src, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src), "r"(n)
+               : "memory");
+}
+
+template <bool TWO_D, bool TRI, bool SNAP>
+__global__ void __launch_bounds__(MARCH_MAXT) march_kernel(const StepArgs a) {
+  extern __shared__ float4 ring[];
+  constexpr int NS = MARCH_NS, D = NS - 1;
+  const Geo &g = a.g;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int nth = blockDim.x;
+  const int G = a.ngroups;
+  const int spw = 32 / G;
+  const int gi = lane % G;
+  const int sl = lane / G;
+  const int xl = w / a.WPC;
+  const int zs = (w - xl * a.WPC) * spw + sl;
+  const int slot = (blockIdx.x % a.nzc) * a.ZS + zs;
+  const int ix = TWO_D ? 0 : (int)(blockIdx.x / a.nzc) * a.KX + xl;
+  const bool valid = sl < spw && zs < a.ZS && slot < a.S && xl < a.KX && ix < g.nx;
+  const int iz0 = 4 * slot - HZ;
+  const bool live = valid && slot >= 1 && iz0 < g.nz;
+  const float *A = a.cur[0];
+  float *B = a.nxt[0];
+#pragma unroll
+  for (int k = 1; k < MAXG; k++)
+    if (gi == k) {
+      A = a.cur[k];
+      B = a.nxt[k];
+    }
+  const long long sx = g.sx, sy = g.sy;
+  const long long base = valid ? 4LL * slot + sx * (ix + g.hx) + sy * g.hy : 0;
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+
+  float wz[4];
+  bool lzm[4], keep[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int iz = iz0 + e;
+    wz[e] = (live && iz < g.nz) ? a.wz[iz] : 1.f;
+    lzm[e] = iz >= g.lz0 && iz < g.lz1;
+    keep[e] = iz < g.nz;
+  }
+  const float wx = (!TWO_D && live) ? a.wx[ix] : 1.f;
+  const bool lxm = TWO_D || (ix >= g.lx0 && ix < g.lx1);
+  const bool needL = valid && slot >= 1 && (sl == 0 || zs == 0);
+  const bool needR = valid && slot + 1 < a.S && (sl == spw - 1 || zs == a.ZS - 1);
+  const int erz = a.rz - iz0;
+  const bool rec_zx = live && erz >= 0 && erz < 4 && ix >= a.rx0 && ix < a.rx0 + a.nrx;
+  const bool in_zx = ix >= a.nbx && ix < a.nbx + a.nx1;
+  const int nrec = a.nrx * a.nry;
+
+  const int y0 = blockIdx.y * a.ych;
+  const int y1 = min(g.ny, y0 + a.ych);
+  float4 *rA = ring, *rB = ring + NS * nth, *rV = ring + 2 * NS * nth;
+  // plane y's copies: A at y+2 (the queue's leading plane), B and vv at y
+  auto issue = [&](int y) {
+    if (y < y1) {
+      const int k = (y & (NS - 1)) * nth + t;
+      const long long o = base + sy * y;
+      cp16ca(rA + k, A + o + 2 * sy, valid);
+      cp16(rB + k, B + o, valid);
+      cp16(rV + k, a.vv + o, valid);
+    }
+    cp_commit();
+  };
+  float4 q0 = zero4, q1 = zero4, q2 = zero4, q3 = zero4;
+  if (valid) {
+    q0 = __ldg(reinterpret_cast<const float4 *>(A + base + sy * (y0 - 2)));
+    q1 = __ldg(reinterpret_cast<const float4 *>(A + base + sy * (y0 - 1)));
+    q2 = __ldg(reinterpret_cast<const float4 *>(A + base + sy * y0));
+    q3 = __ldg(reinterpret_cast<const float4 *>(A + base + sy * (y0 + 1)));
+  }
+#pragma unroll
+  for (int j = 0; j < D; j++) issue(y0 + j);
+  const unsigned full = 0xffffffffu;
+  for (int y = y0; y < y1; y++) {
+    issue(y + D);
+    cp_wait<D>();
+    const long long o = base + sy * y;
+    const int k = (y & (NS - 1)) * nth + t;
+    const float4 q4 = rA[k];
+    const float4 pv = rB[k];
+    const float4 vv4 = rV[k];
+    float4 xm1, xp1, xm2, xp2;
+    if (!TWO_D) {
+      xm1 = xp1 = xm2 = xp2 = zero4;
+      if (valid) {
+        xm1 = __ldg(reinterpret_cast<const float4 *>(A + o - sx));
+        xp1 = __ldg(reinterpret_cast<const float4 *>(A + o + sx));
+        xm2 = __ldg(reinterpret_cast<const float4 *>(A + o - 2 * sx));
+        xp2 = __ldg(reinterpret_cast<const float4 *>(A + o + 2 * sx));
+      }
+    }
+    float Lz = __shfl_up_sync(full, q2.z, G), Lw = __shfl_up_sync(full, q2.w, G);
+    float Rx = __shfl_down_sync(full, q2.x, G), Ry = __shfl_down_sync(full, q2.y, G);
+    if (needL) {
+      const float4 h = __ldg(reinterpret_cast<const float4 *>(A + o - 4));
+      Lz = h.z;
+      Lw = h.w;
+    }
+    if (needR) {
+      const float4 h = __ldg(reinterpret_cast<const float4 *>(A + o + 4));
+      Rx = h.x;
+      Ry = h.y;
+    }
+    const float wy = __ldg(a.wy + y);
+    const bool lyok = y >= g.ly0 && y < g.ly1;
+    const bool rec_here = rec_zx && y >= a.ry0 && y < a.ry0 + a.nry;
+    const int r_idx = rec_here ? (y - a.ry0) * a.nrx + (ix - a.rx0) : 0;
+    bool inj = false;
+    float dval = 0.f;
+    if (TRI && rec_here) {
+      inj = a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi;
+      if (inj) dval = a.tri_dat[(size_t)a.it * nrec + r_idx];
+    }
+    bool src_plane = false;
+    if (!TRI)
+      for (int s = 0; s < a.ns; s++) src_plane |= (y >= a.sy[s] - 1 && y <= a.sy[s] + 1);
+    float4 res;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const float cv = el(q2, e);
+      const float zm1 = e == 0 ? Lw : el(q2, e - 1);
+      const float zp1 = e == 3 ? Rx : el(q2, e + 1);
+      const float zm2 = e == 0 ? Lz : (e == 1 ? Lw : el(q2, e - 2));
+      const float zp2 = e == 2 ? Rx : (e == 3 ? Ry : el(q2, e + 2));
+      float tt = fmul(fmul(a.c0, cv), a.k0);
+      tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
+      tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
+      if (!TWO_D) {
+        tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
+        tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
+      }
+      tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
+      tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
+      const float lap = (lzm[e] && lxm && lyok) ? tt : 0.f;
+      // prev = taper(u_{k-1} as stored); x1.0 outside the faces is exact
+      float p = fmul(el(pv, e), wz[e]);
+      if (!TWO_D) p = fmul(p, wx);
+      p = fmul(p, wy);
+      const float vve = el(vv4, e);
+      float v = fadd(cv, fsub(cv, p));
+      v = fadd(v, fmul(lap, vve));
+      if (TRI) {
+        if (inj && e == erz) v = fadd(v, fmul(vve, dval));
+      } else if (src_plane) {
+        const int iz = iz0 + e;
+        for (int s = 0; s < a.ns; s++) {
+          const int dz = iz - a.sz[s], dxs = TWO_D ? 0 : ix - a.sx[s], dys = y - a.sy[s];
+          if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
+            const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
+            v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
+          }
+        }
+      }
+      v = fmul(v, wz[e]);
+      if (!TWO_D) v = fmul(v, wx);
+      v = fmul(v, wy);
+      set_el(res, e, keep[e] ? v : 0.f);
+    }
+    if (live) *reinterpret_cast<float4 *>(B + o) = res;
+    if (!TRI && rec_here && a.rec && gi == 0) a.rec[(size_t)a.it * nrec + r_idx] = el(res, erz);
+    if (SNAP) {
+      const bool interior = live && in_zx && y >= a.nby && y < a.nby + a.ny1;
+      if (a.wfd && gi == 0 && interior) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int iz = iz0 + e;
+          if (iz >= a.nbz && iz < a.nbz + a.nz1)
+            a.wfd[((size_t)(y - a.nby) * a.nx1 + (ix - a.nbx)) * a.nz1 + (iz - a.nbz)] =
+                el(res, e);
+        }
+      }
+      if (TRI && a.img != nullptr) {
+        // prod_g u_g^2 in group order; the groups of a slot sit in lanes sl*G + gg
+        float4 prod = make_float4(1.f, 1.f, 1.f, 1.f);
+        for (int gg = 0; gg < G; gg++) {
+          const int src = sl * G + gg;
+          float4 u;
+          u.x = __shfl_sync(full, res.x, src);
+          u.y = __shfl_sync(full, res.y, src);
+          u.z = __shfl_sync(full, res.z, src);
+          u.w = __shfl_sync(full, res.w, src);
+          prod.x = fmul(fmul(prod.x, u.x), u.x);
+          prod.y = fmul(fmul(prod.y, u.y), u.y);
+          prod.z = fmul(fmul(prod.z, u.z), u.z);
+          prod.w = fmul(fmul(prod.w, u.w), u.w);
+        }
+        if (gi == 0 && interior) {
+          float4 im = *reinterpret_cast<const float4 *>(a.img + o);
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const int iz = iz0 + e;
+            if (iz >= a.nbz && iz < a.nbz + a.nz1) set_el(im, e, fadd(el(im, e), el(prod, e)));
+          }
+          *reinterpret_cast<float4 *>(a.img + o) = im;
+        }
+      }
+    }
+    q0 = q1;
+    q1 = q2;
+    q2 = q3;
+    q3 = q4;
+  }
+  cp_wait_all();
+}
+
+// Warp-tile kernel (3-D): each warp owns an 8-slot x 4-column patch of one
+// group's field and marches it along y.  Per plane the warp copies its patch
+// with a 1-slot z halo and 2-column x halo (10 x 8 float4) into a private
+// ring in shared memory with cp.async, so every A value is fetched from L2
+// 80/32 = 2.5 times instead of once per neighbour use; the lanes read their
+// z and x neighbours there after the warp's own cp.async wait and a
+// __syncwarp (no CTA barrier).  The ring holds planes y .. y+2 plus
+// TILE_NS - 3 in flight; the lead plane's centre (y+2) feeds the register
+// queue.  Each lane's B and vv cells ride in the same ring, TILE_NS - 1
+// planes ahead of their use.  Groups of a
+// TRI launch are separate warps of the CTA; on imaging steps they exchange
+// their new values through shared memory between two CTA barriers.
+constexpr int TILE_ZW = 8, TILE_XW = 4;                      // warp patch: z slots x x columns
+constexpr int TILE_TZ = TILE_ZW + 2, TILE_TX = TILE_XW + 4;  // with halos
+constexpr int TILE_TP = TILE_TZ * TILE_TX;                   // float4 per plane
+constexpr int TILE_NS = 5;                                   // ring planes per warp
+constexpr int TILE_MAXT = 512;
+constexpr int TILE_CPL = (TILE_TP + 31) / 32;                // copies per lane per plane
+constexpr int TILE_WP = TILE_TP + 64;                        // ring float4 per warp and plane
+
+template <bool TRI, bool SNAP>
+__global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
+  extern __shared__ float4 tsm[];
+  constexpr int NS = TILE_NS, D = NS - 3;
+  static_assert(NS == 5, "the y loop is unrolled by the queue length 5");
+  const Geo &g = a.g;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int nw = blockDim.x >> 5;
+  const unsigned full = 0xffffffffu;
+  const int G = a.ngroups;
+  const int gi = w % G;
+  const int wt = w / G;
+  const int wzi = wt % a.WZ, wxi = wt / a.WZ;
+  const int zl = lane % TILE_ZW, xl = lane / TILE_ZW;
+  const int s0 = (blockIdx.x % a.nzc) * (a.WZ * TILE_ZW) + wzi * TILE_ZW;  // warp's first slot
+  const int c0 = (int)(blockIdx.x / a.nzc) * (a.WX * TILE_XW) + wxi * TILE_XW;
+  const int slot = s0 + zl, ix = c0 + xl;
+  const bool valid = slot < a.S && ix < g.nx;
+  const int iz0 = 4 * slot - HZ;
+  const bool live = valid && slot >= 1 && iz0 < g.nz;
+  const float *A = a.cur[0];
+  float *B = a.nxt[0];
+#pragma unroll
+  for (int k = 1; k < MAXG; k++)
+    if (gi == k) {
+      A = a.cur[k];
+      B = a.nxt[k];
+    }
+  const long long sx = g.sx, sy = g.sy;
+  const long long safe = sx * g.hx + sy * g.hy;  // slot 0, column 0: in range for every plane
+  const long long base = valid ? 4LL * slot + sx * (ix + g.hx) + sy * g.hy : safe;
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 *ring = tsm + (size_t)w * NS * TILE_WP;  // A patches, then B and vv per lane
+  float4 *rbv = ring + NS * TILE_TP;
+  const int y0 = blockIdx.y * a.ych;
+  const int y1 = min(g.ny, y0 + a.ych);
+
+  // this lane's share of the patch copy: element j = lane + 32k of the
+  // (TILE_TZ x TILE_TX) patch, tz fastest; pointers at the next plane to copy
+  const float *cpp[TILE_CPL];
+  bool c_ok[TILE_CPL];
+#pragma unroll
+  for (int k = 0; k < TILE_CPL; k++) {
+    const int j = lane + 32 * k;
+    const int tz = j % TILE_TZ, tx = j / TILE_TZ;
+    const int sl = s0 - 1 + tz, col = c0 - 2 + tx;
+    c_ok[k] = j < TILE_TP && sl >= 0 && sl < a.S && col >= -g.hx && col < g.nx + g.hx;
+    cpp[k] = A + (c_ok[k] ? 4LL * sl + sx * (col + g.hx) + sy * g.hy : safe) + sy * y0;
+  }
+  int next_plane = y0;
+  const float *cB = B + base + sy * y0, *cV = a.vv + base + sy * y0;
+  // copies of plane next_plane into ring slot rs: the A patch, and this lane's
+  // B and vv cells (used when next_plane is updated); planes past y1 + 1 are
+  // not needed
+  auto issue = [&](int rs) {
+    if (next_plane <= y1 + 1) {
+      float4 *dst = ring + rs * TILE_TP;
+#pragma unroll
+      for (int k = 0; k < TILE_CPL; k++) {
+        const int j = lane + 32 * k;
+        if (j < TILE_TP) cp16(dst + j, cpp[k], c_ok[k]);
+        cpp[k] += sy;
+      }
+      if (next_plane < y1) {
+        cp16(rbv + rs * 64 + lane, cB, valid);
+        cp16(rbv + rs * 64 + 32 + lane, cV, valid);
+      }
+      cB += sy;
+      cV += sy;
+    }
+    next_plane++;
+    cp_commit();
+  };
+
+  float wz4[4];
+  bool lzm[4], keep[4];
+  bool lane_taper = false, lane_plain = true;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int iz = iz0 + e;
+    wz4[e] = (live && iz < g.nz) ? a.wz[iz] : 1.f;
+    lzm[e] = iz >= g.lz0 && iz < g.lz1;
+    keep[e] = iz < g.nz;
+    lane_taper |= wz4[e] != 1.f;
+    lane_plain &= lzm[e] && keep[e];
+  }
+  const float wx = live ? a.wx[ix] : 1.f;
+  const bool lxm = ix >= g.lx0 && ix < g.lx1;
+  lane_taper |= wx != 1.f;
+  lane_plain &= lxm;
+  // warp-uniform: every live lane free of masks, no lane tapered in z or x
+  const bool warp_plain = __all_sync(full, !live || lane_plain);
+  const bool warp_taper_zx = __any_sync(full, live && lane_taper);
+  const int erz = a.rz - iz0;
+  const bool rec_zx = live && erz >= 0 && erz < 4 && ix >= a.rx0 && ix < a.rx0 + a.nrx;
+  const bool warp_rec = __any_sync(full, rec_zx);
+  const bool in_zx = ix >= a.nbx && ix < a.nbx + a.nx1;
+  const int nrec = a.nrx * a.nry;
+  const int ci = (xl + 2) * TILE_TZ + zl + 1;  // centre in the patch
+
+  // queue: plane y-2+k sits in q[(y - y0 + k) % 5]
+  float4 q[5];
+  q[4] = zero4;
+  const float *pA = A + base;
+  float *pB = B + base + sy * y0;
+  q[0] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 2)));
+  q[1] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 1)));
+  q[2] = __ldg(reinterpret_cast<const float4 *>(pA + sy * y0));
+  q[3] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 + 1)));
+  float wyn = y0 < y1 ? __ldg(a.wy + y0) : 1.f;
+#pragma unroll
+  for (int j = 0; j < 2 + D; j++) issue(j);
+
+  for (int yb = y0; yb < y1; yb += NS) {
+#pragma unroll
+    for (int u = 0; u < NS; u++) {
+      const int y = yb + u;
+      if (y < y1) {
+        issue((u + 2 + D) % NS);  // plane y + 2 + D into the slot plane y - 1 left
+        cp_wait<D>();
+        __syncwarp();
+        const float4 *pc = ring + u * TILE_TP;
+        q[(u + 4) % NS] = ring[((u + 2) % NS) * TILE_TP + ci];
+        const float4 q0 = q[u], q1 = q[(u + 1) % NS], q2 = q[(u + 2) % NS],
+                     q3 = q[(u + 3) % NS], q4 = q[(u + 4) % NS];
+        const float4 pv = rbv[u * 64 + lane], vv4 = rbv[u * 64 + 32 + lane];
+        const float4 xm1 = pc[ci - TILE_TZ], xp1 = pc[ci + TILE_TZ];
+        const float4 xm2 = pc[ci - 2 * TILE_TZ], xp2 = pc[ci + 2 * TILE_TZ];
+        const float2 Lf = reinterpret_cast<const float2 *>(pc + ci - 1)[1];  // (z, w)
+        const float2 Rf = reinterpret_cast<const float2 *>(pc + ci + 1)[0];  // (x, y)
+        const float wy = wyn;
+        if (y + 1 < y1) wyn = __ldg(a.wy + y + 1);
+        const bool lyok = y >= g.ly0 && y < g.ly1;
+        bool rec_here = false, inj = false;
+        int r_idx = 0;
+        float dval = 0.f;
+        if (warp_rec) {
+          rec_here = rec_zx && y >= a.ry0 && y < a.ry0 + a.nry;
+          r_idx = rec_here ? (y - a.ry0) * a.nrx + (ix - a.rx0) : 0;
+          if (TRI && rec_here) {
+            inj = a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi;
+            if (inj) dval = a.tri_dat[(size_t)a.it * nrec + r_idx];
+          }
+        }
+        bool src_plane = false;
+        if (!TRI)
+          for (int s = 0; s < a.ns; s++) src_plane |= (y >= a.sy[s] - 1 && y <= a.sy[s] + 1);
+        const bool fast = warp_plain && lyok && !warp_taper_zx && wy == 1.f && !inj && !src_plane;
+        float4 res;
+        if (fast) {
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const float cv = el(q2, e);
+            const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
+            const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
+            const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
+            const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
+            float tt = fmul(fmul(a.c0, cv), a.k0);
+            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
+            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
+            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
+            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
+            tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
+            tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
+            float v = fadd(cv, fsub(cv, el(pv, e)));
+            v = fadd(v, fmul(tt, el(vv4, e)));
+            set_el(res, e, v);
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const float cv = el(q2, e);
+            const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
+            const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
+            const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
+            const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
+            float tt = fmul(fmul(a.c0, cv), a.k0);
+            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
+            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
+            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
+            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
+            tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
+            tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
+            const float lap = (lzm[e] && lxm && lyok) ? tt : 0.f;
+            // prev = taper(u_{k-1} as stored); x1.0 outside the faces is exact
+            float p = fmul(el(pv, e), wz4[e]);
+            p = fmul(p, wx);
+            p = fmul(p, wy);
+            const float vve = el(vv4, e);
+            float v = fadd(cv, fsub(cv, p));
+            v = fadd(v, fmul(lap, vve));
+            if (TRI) {
+              if (inj && e == erz) v = fadd(v, fmul(vve, dval));
+            } else if (src_plane) {
+              const int iz = iz0 + e;
+              for (int s = 0; s < a.ns; s++) {
+                const int dz = iz - a.sz[s], dxs = ix - a.sx[s], dys = y - a.sy[s];
+                if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
+                  const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
+                  v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
+                }
+              }
+            }
+            v = fmul(v, wz4[e]);
+            v = fmul(v, wx);
+            v = fmul(v, wy);
+            set_el(res, e, keep[e] ? v : 0.f);
+          }
+        }
+        if (live) *reinterpret_cast<float4 *>(pB) = res;
+        if (!TRI && rec_here && a.rec && gi == 0) a.rec[(size_t)a.it * nrec + r_idx] = el(res, erz);
+        if (SNAP) {
+          const bool interior = live && in_zx && y >= a.nby && y < a.nby + a.ny1;
+          if (a.wfd && gi == 0 && interior) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              const int iz = iz0 + e;
+              if (iz >= a.nbz && iz < a.nbz + a.nz1)
+                a.wfd[((size_t)(y - a.nby) * a.nx1 + (ix - a.nbx)) * a.nz1 + (iz - a.nbz)] =
+                    el(res, e);
+            }
+          }
+          if (TRI && a.img != nullptr) {
+            float4 *xch = tsm + (size_t)nw * NS * TILE_WP;  // [warp][lane]
+            xch[t] = res;
+            __syncthreads();
+            if (gi == 0 && interior) {
+              float4 prod = make_float4(1.f, 1.f, 1.f, 1.f);
+              for (int gg = 0; gg < G; gg++) {
+                const float4 uu = xch[(wt * G + gg) * 32 + lane];
+                prod.x = fmul(fmul(prod.x, uu.x), uu.x);
+                prod.y = fmul(fmul(prod.y, uu.y), uu.y);
+                prod.z = fmul(fmul(prod.z, uu.z), uu.z);
+                prod.w = fmul(fmul(prod.w, uu.w), uu.w);
+              }
+              float *pI = a.img + (pB - B);
+              float4 im = *reinterpret_cast<const float4 *>(pI);
+#pragma unroll
+              for (int e = 0; e < 4; e++) {
+                const int iz = iz0 + e;
+                if (iz >= a.nbz && iz < a.nbz + a.nz1) set_el(im, e, fadd(el(im, e), el(prod, e)));
+              }
+              *reinterpret_cast<float4 *>(pI) = im;
+            }
+            __syncthreads();
+          }
+        }
+        pB += sy;
+        __syncwarp();  // the ring slot refilled next iteration was read above
+      }
+    }
+  }
+  cp_wait_all();
+}
+
 // vv = ((v*v)*dt)*dt on the expanded grid with edge replication of the
 // interior velocity (vel_expand, wave_abc.c:14-125; wave_fdm.c:173-175).
 // Kernel axes; (nbz,nbx,nby) and (nz1,nx1,ny1) describe the interior.
@@ -490,6 +1000,9 @@ struct Plan {
   int ych;
   dim3 grid;
   size_t smem;
+  void *fn, *fn_snap;  // plain steps / snapshot and imaging steps
+  int threads;
+  int S, ZS, KX, nzc, WPC, WZ, WX;
 };
 
 template <bool TWO_D, int ZW, int TX, bool TRI>
@@ -517,7 +1030,195 @@ static int blocks_per_sm(void *fn, int threads, size_t smem) {
   return std::max(n, 1);
 }
 
-static int make_plan(const pw_afd_args *a, bool tri, Plan &p) {
+template <bool TWO_D, bool TRI, bool SNAP>
+static void *march_ptr() {
+  void *f = (void *)march_kernel<TWO_D, TRI, SNAP>;
+  static bool once = [f] {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         3 * MARCH_NS * MARCH_MAXT * (int)sizeof(float4));
+    return true;
+  }();
+  (void)once;
+  return f;
+}
+
+static void *march_fn(bool two_d, bool tri, bool snap) {
+  if (two_d) {
+    if (tri) return snap ? march_ptr<true, true, true>() : march_ptr<true, true, false>();
+    return snap ? march_ptr<true, false, true>() : march_ptr<true, false, false>();
+  }
+  if (tri) return snap ? march_ptr<false, true, true>() : march_ptr<false, true, false>();
+  return snap ? march_ptr<false, false, true>() : march_ptr<false, false, false>();
+}
+
+// Tile override for measurements: PW_AFD_TILE_G<G>="a,b" fixes the first two
+// tile parameters of the planner for G groups.
+static void tile_override(int G, int &fa, int &fb) {
+  fa = fb = 0;
+  char name[32];
+  snprintf(name, sizeof name, "PW_AFD_TILE_G%d", G);
+  if (const char *e = getenv(name)) sscanf(e, "%d,%d", &fa, &fb);
+}
+
+// Tile of the march kernel: WPC warps per z chunk of ZS = WPC * (32/G) slots,
+// KX columns per CTA, ych planes per CTA.  Score = useful thread-planes /
+// thread-plane capacity spent (idle lanes, dead slots, partial waves, the
+// 2-plane prologue of each y chunk), times a latency factor below 24 resident
+// warps per SM and a penalty for x-neighbour loads served by other CTAs.
+static int plan_march(bool tri, int G, int nsm, Plan &p) {
+  const Geo &g = p.g;
+  const bool two_d = p.dim == 2;
+  void *fn = march_fn(two_d, tri, false);
+  const int S = g.lz / 4;
+  const int spw = 32 / G;
+  const int live_slots = ceil_div(g.nz, 4);
+  const double useful = (double)G * live_slots * g.nx * g.ny;
+  int fw, fk;
+  tile_override(G, fw, fk);
+  double best = -1;
+  int bw = 0, bk = 0, by = 0;
+  for (int WPC = 1; WPC <= ceil_div(S, spw); WPC++) {
+    if (fw && WPC != fw) continue;
+    const int ZS = WPC * spw;
+    const int nzc = ceil_div(S, ZS);
+    if (WPC > 1 && ceil_div(S, (WPC - 1) * spw) == nzc) continue;  // same chunks, fewer lanes
+    for (int KX = 1; KX <= (two_d ? 1 : 64); KX++) {
+      const int threads = 32 * WPC * KX;
+      if (threads > MARCH_MAXT) break;
+      if (fk && KX != fk) continue;
+      const size_t smem = (size_t)3 * MARCH_NS * threads * sizeof(float4);
+      int occ = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        occ = 0;
+      }
+      if (occ <= 0) continue;
+      const long long slots = (long long)nsm * occ;
+      const long long tiles = (long long)nzc * ceil_div(g.nx, KX);
+      const double warps = (double)occ * threads / 32;
+      const double lat = std::min(1.0, warps / 24.0);
+      const double outside = two_d ? 0.0 : (KX == 1 ? 1.0 : 6.0 / (4.0 * KX));
+      const double xh = 1.0 / (1.0 + 0.3 * outside);
+      for (int ych = std::max(4, ceil_div(g.ny, 65535)); ych <= g.ny + 3; ych++) {
+        const int yc = std::min(ych, g.ny);
+        const long long ctas = tiles * ceil_div(g.ny, yc);
+        const long long waves = (ctas + slots - 1) / slots;
+        const double cap = (double)waves * slots * threads * (yc + 2);
+        const double score = useful / cap * lat * xh;
+        if (score > best + 1e-9) {
+          best = score;
+          bw = WPC;
+          bk = KX;
+          by = yc;
+        }
+        if (yc == g.ny) break;
+      }
+    }
+  }
+  PW_CHECK(best > 0, PW_ERR_SHAPE, "no launchable tile for the step kernel");
+  p.fn = fn;
+  p.fn_snap = march_fn(two_d, tri, true);
+  p.S = S;
+  p.WPC = bw;
+  p.ZS = bw * spw;
+  p.nzc = ceil_div(S, p.ZS);
+  p.KX = bk;
+  p.ych = by;
+  p.threads = 32 * bw * bk;
+  p.smem = (size_t)3 * MARCH_NS * p.threads * sizeof(float4);
+  p.grid = dim3((unsigned)(p.nzc * ceil_div(g.nx, bk)), (unsigned)ceil_div(g.ny, by), 1);
+  if (getenv("PW_AFD_VERBOSE"))
+    fprintf(stderr,
+            "afd march plan: G=%d S=%d nzc=%d ZS=%d WPC=%d KX=%d ych=%d threads=%d grid=%ux%u "
+            "score=%.3f\n",
+            G, S, p.nzc, p.ZS, bw, bk, by, p.threads, p.grid.x, p.grid.y, best);
+  return PW_OK;
+}
+
+template <bool TRI, bool SNAP>
+static void *tile_ptr() {
+  void *f = (void *)tile_kernel<TRI, SNAP>;
+  static bool once = [f] {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (TILE_MAXT / 32) * TILE_NS * TILE_WP * (int)sizeof(float4) +
+                             TILE_MAXT * (int)sizeof(float4));
+    return true;
+  }();
+  (void)once;
+  return f;
+}
+
+static size_t tile_smem(int threads, bool tri) {
+  return (size_t)(threads / 32) * TILE_NS * TILE_WP * sizeof(float4) +
+         (tri ? (size_t)threads * sizeof(float4) : 0);
+}
+
+// Tile of the 3-D warp-tile kernel: CTA = G groups x WZ x WX warps of 8 slots
+// x 4 columns, ych planes.  Same score as plan_march without the x-halo term
+// (every warp fetches its own halo).
+static int plan_tile(bool tri, int G, int nsm, Plan &p) {
+  const Geo &g = p.g;
+  void *fn = tri ? tile_ptr<true, false>() : tile_ptr<false, false>();
+  const int S = g.lz / 4;
+  const int live_slots = ceil_div(g.nz, 4);
+  const double useful = (double)G * live_slots * g.nx * g.ny;
+  int fw, fk;
+  tile_override(G, fw, fk);
+  double best = -1;
+  int bz = 0, bx = 0, by = 0;
+  for (int WZ = 1; WZ <= ceil_div(S, TILE_ZW); WZ++) {
+    if (fw && WZ != fw) continue;
+    const int nzc = ceil_div(S, WZ * TILE_ZW);
+    if (WZ > 1 && ceil_div(S, (WZ - 1) * TILE_ZW) == nzc) continue;
+    for (int WX = 1; G * WZ * WX * 32 <= TILE_MAXT; WX++) {
+      if (fk && WX != fk) continue;
+      const int threads = G * WZ * WX * 32;
+      const size_t smem = tile_smem(threads, tri);
+      int occ = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        occ = 0;
+      }
+      if (occ <= 0) continue;
+      const long long slots = (long long)nsm * occ;
+      const long long tiles = (long long)nzc * ceil_div(g.nx, WX * TILE_XW);
+      const double warps = (double)occ * threads / 32;
+      const double lat = std::min(1.0, warps / 24.0);
+      for (int ych = std::max(4, ceil_div(g.ny, 65535)); ych <= g.ny + 3; ych++) {
+        const int yc = std::min(ych, g.ny);
+        const long long ctas = tiles * ceil_div(g.ny, yc);
+        const long long waves = (ctas + slots - 1) / slots;
+        const double cap = (double)waves * slots * threads * (yc + 2);
+        const double score = useful / cap * lat;
+        if (score > best + 1e-9) {
+          best = score;
+          bz = WZ;
+          bx = WX;
+          by = yc;
+        }
+        if (yc == g.ny) break;
+      }
+    }
+  }
+  PW_CHECK(best > 0, PW_ERR_SHAPE, "no launchable tile for the step kernel");
+  p.fn = fn;
+  p.fn_snap = tri ? tile_ptr<true, true>() : tile_ptr<false, true>();
+  p.S = S;
+  p.WZ = bz;
+  p.WX = bx;
+  p.nzc = ceil_div(S, bz * TILE_ZW);
+  p.ych = by;
+  p.threads = G * bz * bx * 32;
+  p.smem = tile_smem(p.threads, tri);
+  p.grid = dim3((unsigned)(p.nzc * ceil_div(g.nx, bx * TILE_XW)), (unsigned)ceil_div(g.ny, by), 1);
+  if (getenv("PW_AFD_VERBOSE"))
+    fprintf(stderr,
+            "afd tile plan: G=%d S=%d nzc=%d WZ=%d WX=%d ych=%d threads=%d grid=%ux%u score=%.3f\n",
+            G, S, p.nzc, bz, bx, by, p.threads, p.grid.x, p.grid.y, best);
+  return PW_OK;
+}
+
+static int make_plan(const pw_afd_args *a, bool tri, int G, Plan &p) {
   PW_CHECK(a->dim == 2 || a->dim == 3, PW_ERR_SHAPE, "dim must be 2 or 3 (got %d)", a->dim);
   PW_CHECK(a->nz >= 1 && a->nx >= 1 && a->ny >= 1 && a->nt >= 1 && a->nbt >= 0, PW_ERR_SHAPE,
            "sizes must be positive (nz=%d nx=%d ny=%d nt=%d nbt=%d)", a->nz, a->nx, a->ny, a->nt,
@@ -597,6 +1298,13 @@ static int make_plan(const pw_afd_args *a, bool tri, Plan &p) {
   }
   p.ych = std::min(best_ych, g.ny);
   p.grid = dim3(ceil_div(g.ny, p.ych), ceil_div(g.nx, best.tx), ceil_div(nz4, best.zw));
+  p.fn = p.fn_snap = fn;
+  p.threads = threads;
+  p.S = p.ZS = p.KX = p.nzc = p.WPC = p.WZ = p.WX = 0;
+  if (getenv("PW_AFD_OLD") == nullptr) {
+    if (two_d || getenv("PW_AFD_MARCH")) PW_TRY(plan_march(tri, G, nsm, p));
+    else PW_TRY(plan_tile(tri, G, nsm, p));
+  }
   return PW_OK;
 }
 
@@ -646,11 +1354,11 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   PW_CHECK(a != nullptr, PW_ERR_VALUE, "null args");
   const bool host = (a->flags & PW_HOST_PTRS) != 0;
   const bool tri = a->tri != 0 || img_out != nullptr;
+  PW_CHECK(G >= 1 && G <= MAXG, PW_ERR_SHAPE, "ngroups must be in [1,%d] (got %d)", MAXG, G);
   Plan p;
-  PW_TRY(make_plan(a, tri, p));
+  PW_TRY(make_plan(a, tri, G, p));
   const Geo &g = p.g;
   const bool two_d = p.dim == 2;
-  PW_CHECK(G >= 1 && G <= MAXG, PW_ERR_SHAPE, "ngroups must be in [1,%d] (got %d)", MAXG, G);
   PW_CHECK(a->jsnap >= 0, PW_ERR_VALUE, "jsnap must be >= 0");
   PW_CHECK(a->gz >= 0 && a->gz < a->nz, PW_ERR_SHAPE, "receiver depth gz=%d outside [0,%d)", a->gz,
            a->nz);
@@ -815,6 +1523,13 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   s.g = g;
   s.ych = p.ych;
   s.ngroups = G;
+  s.S = p.S;
+  s.ZS = p.ZS;
+  s.KX = p.KX;
+  s.nzc = p.nzc;
+  s.WPC = p.WPC;
+  s.WZ = p.WZ;
+  s.WX = p.WX;
   {
     const float c0 = -30. / 12., c1 = +16. / 12., c2 = -1. / 12.;  // wave_fdm.c:15
     s.c0 = c0;
@@ -857,8 +1572,8 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   s.nbz = p.kbz; s.nbx = p.kbx; s.nby = p.kby;
   s.nz1 = p.knz1; s.nx1 = p.knx1; s.ny1 = p.kny1;
   float *wfd_dev = wfd ? (host ? at<float>(base, o_wfd) : wfd) : nullptr;
-  void *fn = pick_kernel(two_d, p.v, tri);
-  const int threads = p.v.zw * p.v.tx;
+  void *fn = p.fn;
+  const int threads = p.threads;
   LoopTimer timer(st);
   timer.start();
   for (int k = 0; k < nt; k++) {
@@ -872,7 +1587,8 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
     s.wfd = (snap && wfd_dev) ? wfd_dev + (size_t)(it / a->jsnap) * nvel : nullptr;
     s.img = (snap && img) ? img : nullptr;
     void *args[] = {(void *)&s};
-    PW_CUDA(cudaLaunchKernel(fn, p.grid, dim3(threads), args, p.smem, st));
+    void *f = (s.wfd || s.img) ? p.fn_snap : fn;
+    PW_CUDA(cudaLaunchKernel(f, p.grid, dim3(threads), args, p.smem, st));
     for (int i = 0; i < G; i++) std::swap(A[i], B[i]);
   }
   timer.stop();
@@ -959,7 +1675,7 @@ static int run_noalloc(const pw_afd_args *a, const float *vel, const float *src,
   PW_CHECK(a->tri == 0, PW_ERR_VALUE, "pw_afd_noalloc runs forward modelling only (tri = 0)");
   PW_CHECK(vel != nullptr, PW_ERR_VALUE, "velocity is null");
   Plan p;
-  PW_TRY(make_plan(a, false, p));
+  PW_TRY(make_plan(a, false, 1, p));
   const Geo &g = p.g;
   const bool two_d = p.dim == 2;
   PW_CHECK(a->jsnap >= 0, PW_ERR_VALUE, "jsnap must be >= 0");
@@ -1063,6 +1779,13 @@ static int run_noalloc(const pw_afd_args *a, const float *vel, const float *src,
   s.g = g;
   s.ych = p.ych;
   s.ngroups = 1;
+  s.S = p.S;
+  s.ZS = p.ZS;
+  s.KX = p.KX;
+  s.nzc = p.nzc;
+  s.WPC = p.WPC;
+  s.WZ = p.WZ;
+  s.WX = p.WX;
   {
     const float c0 = -30. / 12., c1 = +16. / 12., c2 = -1. / 12.;  // wave_fdm.c:15
     s.c0 = c0;
@@ -1105,8 +1828,8 @@ static int run_noalloc(const pw_afd_args *a, const float *vel, const float *src,
   s.nbz = p.kbz; s.nbx = p.kbx; s.nby = p.kby;
   s.nz1 = p.knz1; s.nx1 = p.knx1; s.ny1 = p.kny1;
   s.img = nullptr;
-  void *fn = pick_kernel(two_d, p.v, false);
-  const int threads = p.v.zw * p.v.tx;
+  void *fn = p.fn;
+  const int threads = p.threads;
   for (int it = 0; it < nt; it++) {
     s.it = it;
     s.cur[0] = A;
@@ -1114,7 +1837,8 @@ static int run_noalloc(const pw_afd_args *a, const float *vel, const float *src,
     const bool snap = a->jsnap > 0 && it % a->jsnap == 0;
     s.wfd = (snap && wfd) ? wfd + (size_t)(it / a->jsnap) * nvel : nullptr;
     void *args[] = {(void *)&s};
-    PW_CUDA(cudaLaunchKernel(fn, p.grid, dim3(threads), args, p.smem, st));
+    void *f = s.wfd ? p.fn_snap : fn;
+    PW_CUDA(cudaLaunchKernel(f, p.grid, dim3(threads), args, p.smem, st));
     std::swap(A, B);
   }
   if (dat) {
