@@ -623,17 +623,17 @@ __global__ void __launch_bounds__(MARCH_MAXT) march_kernel(const StepArgs a) {
 // z and x neighbours there after the warp's own cp.async wait and a
 // __syncwarp (no CTA barrier).  The ring holds planes y .. y+2 plus
 // TILE_NS - 3 in flight; the lead plane's centre (y+2) feeds the register
-// queue.  Each lane's B and vv cells ride in the same ring, TILE_NS - 1
-// planes ahead of their use.  Groups of a
-// TRI launch are separate warps of the CTA; on imaging steps they exchange
-// their new values through shared memory between two CTA barriers.
+// queue.  Each lane's B and vv cells ride in the same ring, copied with the
+// A patch of their plane (TILE_NS - 1 planes ahead of their use).  Groups of a TRI launch are separate warps of
+// the CTA; the TRI image of an imaging step is formed afterwards by
+// image_kernel.
 constexpr int TILE_ZW = 8, TILE_XW = 4;                      // warp patch: z slots x x columns
 constexpr int TILE_TZ = TILE_ZW + 2, TILE_TX = TILE_XW + 4;  // with halos
 constexpr int TILE_TP = TILE_TZ * TILE_TX;                   // float4 per plane
 constexpr int TILE_NS = 5;                                   // ring planes per warp
 constexpr int TILE_MAXT = 512;
 constexpr int TILE_CPL = (TILE_TP + 31) / 32;                // copies per lane per plane
-constexpr int TILE_WP = TILE_TP + 64;                        // ring float4 per warp and plane
+constexpr int TILE_WS = TILE_NS * (TILE_TP + 64);            // ring float4 per warp
 
 template <bool TRI, bool SNAP>
 __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
@@ -642,7 +642,6 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
   static_assert(NS == 5, "the y loop is unrolled by the queue length 5");
   const Geo &g = a.g;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  const int nw = blockDim.x >> 5;
   const unsigned full = 0xffffffffu;
   const int G = a.ngroups;
   const int gi = w % G;
@@ -667,7 +666,7 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
   const long long safe = sx * g.hx + sy * g.hy;  // slot 0, column 0: in range for every plane
   const long long base = valid ? 4LL * slot + sx * (ix + g.hx) + sy * g.hy : safe;
   const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  float4 *ring = tsm + (size_t)w * NS * TILE_WP;  // A patches, then B and vv per lane
+  float4 *ring = tsm + (size_t)w * TILE_WS;  // NS A patches, then NS planes of B and vv per lane
   float4 *rbv = ring + NS * TILE_TP;
   const int y0 = blockIdx.y * a.ych;
   const int y1 = min(g.ny, y0 + a.ych);
@@ -699,8 +698,9 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
         cpp[k] += sy;
       }
       if (next_plane < y1) {
-        cp16(rbv + rs * 64 + lane, cB, valid);
-        cp16(rbv + rs * 64 + 32 + lane, cV, valid);
+        const int bs = rs * 64;
+        cp16(rbv + bs + lane, cB, valid);
+        cp16(rbv + bs + 32 + lane, cV, valid);
       }
       cB += sy;
       cV += sy;
@@ -857,30 +857,6 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
                     el(res, e);
             }
           }
-          if (TRI && a.img != nullptr) {
-            float4 *xch = tsm + (size_t)nw * NS * TILE_WP;  // [warp][lane]
-            xch[t] = res;
-            __syncthreads();
-            if (gi == 0 && interior) {
-              float4 prod = make_float4(1.f, 1.f, 1.f, 1.f);
-              for (int gg = 0; gg < G; gg++) {
-                const float4 uu = xch[(wt * G + gg) * 32 + lane];
-                prod.x = fmul(fmul(prod.x, uu.x), uu.x);
-                prod.y = fmul(fmul(prod.y, uu.y), uu.y);
-                prod.z = fmul(fmul(prod.z, uu.z), uu.z);
-                prod.w = fmul(fmul(prod.w, uu.w), uu.w);
-              }
-              float *pI = a.img + (pB - B);
-              float4 im = *reinterpret_cast<const float4 *>(pI);
-#pragma unroll
-              for (int e = 0; e < 4; e++) {
-                const int iz = iz0 + e;
-                if (iz >= a.nbz && iz < a.nbz + a.nz1) set_el(im, e, fadd(el(im, e), el(prod, e)));
-              }
-              *reinterpret_cast<float4 *>(pI) = im;
-            }
-            __syncthreads();
-          }
         }
         pB += sy;
         __syncwarp();  // the ring slot refilled next iteration was read above
@@ -888,6 +864,47 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
     }
   }
   cp_wait_all();
+}
+
+// TRI image of one imaging step: img += prod_g u_g^2 over the interior cells
+// (the demos' image, test_third_tri.py:71-77, in group order), on the field
+// layout, one float4 of z cells per thread.  Used after warp-tile steps.
+struct ImgArgs {
+  Geo g;
+  const float *u[MAXG];
+  int G;
+  float *img;
+  int nbz, nbx, nby, nz1, nx1, ny1;
+  int s0, ns4;  // float4 slots covering the interior z range
+};
+
+__global__ void image_kernel(const ImgArgs a) {
+  const long long n = (long long)a.ns4 * a.nx1 * a.ny1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int sl = a.s0 + (int)(i % a.ns4);
+    const long long r = i / a.ns4;
+    const int ix = (int)(r % a.nx1) + a.nbx, iy = (int)(r / a.nx1) + a.nby;
+    const long long o = 4LL * sl + a.g.sx * (ix + a.g.hx) + a.g.sy * (iy + a.g.hy);
+    float4 prod = make_float4(1.f, 1.f, 1.f, 1.f);
+#pragma unroll
+    for (int k = 0; k < MAXG; k++) {
+      if (k < a.G) {
+        const float4 u = __ldg(reinterpret_cast<const float4 *>(a.u[k] + o));
+        prod.x = fmul(fmul(prod.x, u.x), u.x);
+        prod.y = fmul(fmul(prod.y, u.y), u.y);
+        prod.z = fmul(fmul(prod.z, u.z), u.z);
+        prod.w = fmul(fmul(prod.w, u.w), u.w);
+      }
+    }
+    float4 im = *reinterpret_cast<const float4 *>(a.img + o);
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int iz = 4 * sl - HZ + e;
+      if (iz >= a.nbz && iz < a.nbz + a.nz1) set_el(im, e, fadd(el(im, e), el(prod, e)));
+    }
+    *reinterpret_cast<float4 *>(a.img + o) = im;
+  }
 }
 
 // vv = ((v*v)*dt)*dt on the expanded grid with edge replication of the
@@ -1001,6 +1018,7 @@ struct Plan {
   dim3 grid;
   size_t smem;
   void *fn, *fn_snap;  // plain steps / snapshot and imaging steps
+  bool tile;           // warp-tile kernel: TRI images by image_kernel
   int threads;
   int S, ZS, KX, nzc, WPC, WZ, WX;
 };
@@ -1140,17 +1158,15 @@ static void *tile_ptr() {
   void *f = (void *)tile_kernel<TRI, SNAP>;
   static bool once = [f] {
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (TILE_MAXT / 32) * TILE_NS * TILE_WP * (int)sizeof(float4) +
-                             TILE_MAXT * (int)sizeof(float4));
+                         (TILE_MAXT / 32) * TILE_WS * (int)sizeof(float4));
     return true;
   }();
   (void)once;
   return f;
 }
 
-static size_t tile_smem(int threads, bool tri) {
-  return (size_t)(threads / 32) * TILE_NS * TILE_WP * sizeof(float4) +
-         (tri ? (size_t)threads * sizeof(float4) : 0);
+static size_t tile_smem(int threads) {
+  return (size_t)(threads / 32) * TILE_WS * sizeof(float4);
 }
 
 // Tile of the 3-D warp-tile kernel: CTA = G groups x WZ x WX warps of 8 slots
@@ -1173,7 +1189,7 @@ static int plan_tile(bool tri, int G, int nsm, Plan &p) {
     for (int WX = 1; G * WZ * WX * 32 <= TILE_MAXT; WX++) {
       if (fk && WX != fk) continue;
       const int threads = G * WZ * WX * 32;
-      const size_t smem = tile_smem(threads, tri);
+      const size_t smem = tile_smem(threads);
       int occ = 0;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) {
         cudaGetLastError();
@@ -1203,13 +1219,14 @@ static int plan_tile(bool tri, int G, int nsm, Plan &p) {
   PW_CHECK(best > 0, PW_ERR_SHAPE, "no launchable tile for the step kernel");
   p.fn = fn;
   p.fn_snap = tri ? tile_ptr<true, true>() : tile_ptr<false, true>();
+  p.tile = true;
   p.S = S;
   p.WZ = bz;
   p.WX = bx;
   p.nzc = ceil_div(S, bz * TILE_ZW);
   p.ych = by;
   p.threads = G * bz * bx * 32;
-  p.smem = tile_smem(p.threads, tri);
+  p.smem = tile_smem(p.threads);
   p.grid = dim3((unsigned)(p.nzc * ceil_div(g.nx, bx * TILE_XW)), (unsigned)ceil_div(g.ny, by), 1);
   if (getenv("PW_AFD_VERBOSE"))
     fprintf(stderr,
@@ -1299,6 +1316,7 @@ static int make_plan(const pw_afd_args *a, bool tri, int G, Plan &p) {
   p.ych = std::min(best_ych, g.ny);
   p.grid = dim3(ceil_div(g.ny, p.ych), ceil_div(g.nx, best.tx), ceil_div(nz4, best.zw));
   p.fn = p.fn_snap = fn;
+  p.tile = false;
   p.threads = threads;
   p.S = p.ZS = p.KX = p.nzc = p.WPC = p.WZ = p.WX = 0;
   if (getenv("PW_AFD_OLD") == nullptr) {
@@ -1574,6 +1592,15 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   float *wfd_dev = wfd ? (host ? at<float>(base, o_wfd) : wfd) : nullptr;
   void *fn = p.fn;
   const int threads = p.threads;
+  ImgArgs ia{};
+  ia.g = g;
+  ia.G = G;
+  ia.img = img;
+  ia.nbz = p.kbz; ia.nbx = p.kbx; ia.nby = p.kby;
+  ia.nz1 = p.knz1; ia.nx1 = p.knx1; ia.ny1 = p.kny1;
+  ia.s0 = (p.kbz + HZ) / 4;
+  ia.ns4 = (p.kbz + p.knz1 - 1 + HZ) / 4 - ia.s0 + 1;
+  long long img_launches = 0;
   LoopTimer timer(st);
   timer.start();
   for (int k = 0; k < nt; k++) {
@@ -1585,10 +1612,16 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
     }
     const bool snap = a->jsnap > 0 && it % a->jsnap == 0;
     s.wfd = (snap && wfd_dev) ? wfd_dev + (size_t)(it / a->jsnap) * nvel : nullptr;
-    s.img = (snap && img) ? img : nullptr;
+    const bool img_step = snap && img;
+    s.img = (img_step && !p.tile) ? img : nullptr;
     void *args[] = {(void *)&s};
     void *f = (s.wfd || s.img) ? p.fn_snap : fn;
     PW_CUDA(cudaLaunchKernel(f, p.grid, dim3(threads), args, p.smem, st));
+    if (img_step && p.tile) {
+      for (int i = 0; i < G; i++) ia.u[i] = B[i];
+      image_kernel<<<1184, 256, 0, st>>>(ia);
+      img_launches++;
+    }
     for (int i = 0; i < G; i++) std::swap(A[i], B[i]);
   }
   timer.stop();
@@ -1617,7 +1650,7 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
     if (host) PW_TRY(to_host(img_out, dst, nvel * 4, true, st));
   }
   PW_CUDA(cudaStreamSynchronize(st));
-  timer.finish(nt, nt + aux_launches);
+  timer.finish(nt, nt + aux_launches + img_launches);
   return PW_OK;
 }
 
