@@ -728,6 +728,16 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
   // warp-uniform: every live lane free of masks, no lane tapered in z or x
   const bool warp_plain = __all_sync(full, !live || lane_plain);
   const bool warp_taper_zx = __any_sync(full, live && lane_taper);
+  // z-x edge cells (tapered along both z and x) need the factors one by one;
+  // elsewhere wz * wx has at most one factor != 1 and is exact
+  bool lane_edge = false;
+  float wzx[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    lane_edge |= wz4[e] != 1.f && wx != 1.f;
+    wzx[e] = fmul(wz4[e], wx);
+  }
+  const bool warp_edge_zx = __any_sync(full, live && lane_edge);
   const int erz = a.rz - iz0;
   const bool rec_zx = live && erz >= 0 && erz < 4 && ix >= a.rx0 && ix < a.rx0 + a.nrx;
   const bool warp_rec = __any_sync(full, rec_zx);
@@ -782,66 +792,151 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
         bool src_plane = false;
         if (!TRI)
           for (int s = 0; s < a.ns; s++) src_plane |= (y >= a.sy[s] - 1 && y <= a.sy[s] + 1);
-        const bool fast = warp_plain && lyok && !warp_taper_zx && wy == 1.f && !inj && !src_plane;
         float4 res;
-        if (fast) {
-#pragma unroll
-          for (int e = 0; e < 4; e++) {
-            const float cv = el(q2, e);
-            const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
-            const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
-            const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
-            const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
-            float tt = fmul(fmul(a.c0, cv), a.k0);
-            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
-            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
-            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
-            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
-            tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-            tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-            float v = fadd(cv, fsub(cv, el(pv, e)));
-            v = fadd(v, fmul(tt, el(vv4, e)));
-            set_el(res, e, v);
-          }
-        } else {
-#pragma unroll
-          for (int e = 0; e < 4; e++) {
-            const float cv = el(q2, e);
-            const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
-            const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
-            const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
-            const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
-            float tt = fmul(fmul(a.c0, cv), a.k0);
-            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
-            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
-            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
-            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
-            tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-            tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-            const float lap = (lzm[e] && lxm && lyok) ? tt : 0.f;
-            // prev = taper(u_{k-1} as stored); x1.0 outside the faces is exact
-            float p = fmul(el(pv, e), wz4[e]);
-            p = fmul(p, wx);
-            p = fmul(p, wy);
-            const float vve = el(vv4, e);
-            float v = fadd(cv, fsub(cv, p));
-            v = fadd(v, fmul(lap, vve));
-            if (TRI) {
-              if (inj && e == erz) v = fadd(v, fmul(vve, dval));
-            } else if (src_plane) {
-              const int iz = iz0 + e;
-              for (int s = 0; s < a.ns; s++) {
-                const int dz = iz - a.sz[s], dxs = ix - a.sx[s], dys = y - a.sy[s];
-                if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
-                  const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
-                  v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
+        if constexpr (TRI) {
+          // time reversal: one fast path (no taper, no mask) and the full one
+          const bool fast = warp_plain && lyok && !warp_taper_zx && wy == 1.f && !inj && !src_plane;
+          if (fast) {
+  #pragma unroll
+            for (int e = 0; e < 4; e++) {
+              const float cv = el(q2, e);
+              const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
+              const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
+              const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
+              const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
+              float tt = fmul(fmul(a.c0, cv), a.k0);
+              tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
+              tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
+              tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
+              tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
+              tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
+              tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
+              float v = fadd(cv, fsub(cv, el(pv, e)));
+              v = fadd(v, fmul(tt, el(vv4, e)));
+              set_el(res, e, v);
+            }
+          } else {
+  #pragma unroll
+            for (int e = 0; e < 4; e++) {
+              const float cv = el(q2, e);
+              const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
+              const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
+              const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
+              const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
+              float tt = fmul(fmul(a.c0, cv), a.k0);
+              tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
+              tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
+              tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
+              tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
+              tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
+              tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
+              const float lap = (lzm[e] && lxm && lyok) ? tt : 0.f;
+              // prev = taper(u_{k-1} as stored); x1.0 outside the faces is exact
+              float p = fmul(el(pv, e), wz4[e]);
+              p = fmul(p, wx);
+              p = fmul(p, wy);
+              const float vve = el(vv4, e);
+              float v = fadd(cv, fsub(cv, p));
+              v = fadd(v, fmul(lap, vve));
+              if (TRI) {
+                if (inj && e == erz) v = fadd(v, fmul(vve, dval));
+              } else if (src_plane) {
+                const int iz = iz0 + e;
+                for (int s = 0; s < a.ns; s++) {
+                  const int dz = iz - a.sz[s], dxs = ix - a.sx[s], dys = y - a.sy[s];
+                  if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
+                    const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
+                    v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
+                  }
                 }
               }
+              v = fmul(v, wz4[e]);
+              v = fmul(v, wx);
+              v = fmul(v, wy);
+              set_el(res, e, keep[e] ? v : 0.f);
             }
-            v = fmul(v, wz4[e]);
-            v = fmul(v, wx);
-            v = fmul(v, wy);
-            set_el(res, e, keep[e] ? v : 0.f);
+          }
+        } else {
+          // forward modelling: two more exact taper paths (measured faster here)
+          // warp-uniform path: no masks and at most one taper family -> FAST
+          // (none), YT (y only: x wy), ZXT (z / x only, no z-x edge: x wz*wx);
+          // FULL otherwise.  The multiplications equal the reference's
+          // face-by-face products because the skipped factors are exactly 1.
+          constexpr bool MULTI = true;
+          const bool clean = warp_plain && lyok && !src_plane;
+          const int path = !clean ? 3
+                           : (!warp_taper_zx ? (wy == 1.f ? 0 : (MULTI ? 1 : 3))
+                                             : (MULTI && wy == 1.f && !warp_edge_zx ? 2 : 3));
+          float4 lp;  // Laplacian sums in the reference's order
+  #pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const float cv = el(q2, e);
+            const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
+            const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
+            const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
+            const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
+            float tt = fmul(fmul(a.c0, cv), a.k0);
+            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
+            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
+            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
+            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
+            tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
+            tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
+            set_el(lp, e, tt);
+          }
+          if (path == 0) {
+  #pragma unroll
+            for (int e = 0; e < 4; e++) {
+              const float cv = el(q2, e);
+              float v = fadd(cv, fsub(cv, el(pv, e)));
+              set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
+            }
+            if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
+          } else if (MULTI && (path == 1 || path == 2)) {
+            float4 f;
+  #pragma unroll
+            for (int e = 0; e < 4; e++) set_el(f, e, path == 1 ? wy : wzx[e]);
+  #pragma unroll
+            for (int e = 0; e < 4; e++) {
+              const float cv = el(q2, e);
+              float v = fadd(cv, fsub(cv, fmul(el(pv, e), el(f, e))));
+              set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
+            }
+            if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
+  #pragma unroll
+            for (int e = 0; e < 4; e++) set_el(res, e, fmul(el(res, e), el(f, e)));
+          } else {
+  #pragma unroll
+            for (int e = 0; e < 4; e++) {
+              const float cv = el(q2, e);
+              const float lap = (lzm[e] && lxm && lyok) ? el(lp, e) : 0.f;
+              // prev = taper(u_{k-1} as stored), face by face
+              float p = fmul(el(pv, e), wz4[e]);
+              p = fmul(p, wx);
+              p = fmul(p, wy);
+              const float vve = el(vv4, e);
+              float v = fadd(cv, fsub(cv, p));
+              v = fadd(v, fmul(lap, vve));
+              if (!TRI && src_plane) {
+                const int iz = iz0 + e;
+                for (int s = 0; s < a.ns; s++) {
+                  const int dz = iz - a.sz[s], dxs = ix - a.sx[s], dys = y - a.sy[s];
+                  if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
+                    const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
+                    v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
+                  }
+                }
+              }
+              set_el(res, e, v);
+            }
+            if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
+  #pragma unroll
+            for (int e = 0; e < 4; e++) {
+              float v = fmul(el(res, e), wz4[e]);
+              v = fmul(v, wx);
+              v = fmul(v, wy);
+              set_el(res, e, keep[e] ? v : 0.f);
+            }
           }
         }
         if (live) *reinterpret_cast<float4 *>(pB) = res;
