@@ -348,7 +348,7 @@ def main():
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": f"step_kernel<3,{G},tri>", "kernel_ms": kern_ms,
+                         "kernel": f"tile_kernel<TRI> x{G} groups + image_kernel every 4th step", "kernel_ms": kern_ms,
                          "alg_bytes_per_launch": alg_bytes, "peak_source": peak_kind},
             "cpu_baseline": cpu,
             "clocks": clocks,

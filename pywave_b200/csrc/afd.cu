@@ -7,22 +7,23 @@
 //
 // Kernel axes.  z is contiguous; x is the tile axis; y is the marched axis.
 // 3-D maps (z,x,y) to the model's (z,x,y).  2-D maps the model's x to the
-// marched axis y and uses a dummy x axis of extent 1, so one kernel serves
-// both.  Field layout: a zero-haloed array
+// marched axis y and uses a dummy x axis of extent 1, so one field layout
+// serves both.  Field layout: a zero-haloed array
 //   off(iz,ix,iy) = (iz + HZ) + sx*(ix + hx) + sy*(iy + hy),
 // leading dimension a multiple of 32 floats; each thread owns one aligned
 // float4 of 4 consecutive z cells.  Halo cells are never written and stay
 // zero: that is the reference's zero border beyond the expanded grid.
 //
-// Data movement.  A CTA owns a z-x tile (ZW float4 x TX columns) and marches
-// it along y.  Each plane's tile (with a 1-float4 z halo and 2-column x halo),
-// the previous wavefield and vv are staged in shared memory by cp.async
-// 16-byte copies, P planes ahead of the plane being updated; the y neighbours
-// of a cell come from a 5-deep register queue.  Receiver groups of a TRI
-// image are processed one after another inside the CTA (one register queue
-// live at a time); at imaging steps the last group reads the other groups'
-// fresh values back (written by the same thread moments earlier, so L2 hits)
-// and accumulates prod_g u_g^2.
+// Kernels.  Each thread owns one float4 of z cells and marches it along y
+// with a 5-deep register queue of its own cells (the y neighbours).  3-D runs
+// use tile_kernel: a warp owns an 8-slot x 4-column patch and stages it (with
+// its z and x halo) per plane in a private cp.async ring in shared memory,
+// together with each lane's B and vv cells, several planes ahead; lanes read
+// their z / x neighbours there after a warp-level sync only.  2-D runs (no x
+// neighbours) use march_kernel: z neighbours by warp shuffle, the leading
+// plane, B and vv by a per-thread cp.async ring.  The TRI image of G receiver
+// groups is formed by image_kernel after each imaging step (3-D) or by
+// shuffles between the groups' lanes (2-D).
 //
 // Two buffers per wavefield: at step k the kernel reads A = u_k and B =
 // u_{k-1} (as stored, tapered once) and overwrites B with u_{k+1}.  The
@@ -102,287 +103,6 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// Per-thread constants of a tile column (z float4 x one x column).
-struct Col {
-  float wz[4];     // z taper factor per cell (1 outside the faces)
-  float wx;        // x taper factor
-  bool lz[4];      // Laplacian non-zero along z
-  bool lx;         // ... along x
-  int iz0, ix;
-};
-
-// Leapfrog update of one float4 of cells, in the reference's float order:
-//   wave = c0*u*k0 + c1*(y-1+y+1)*idy + c2*(y-2+y+2)*idy [+ x terms] + z terms
-//   u_new = (u + (u - taper(u_prev))) + wave*vv  [+ injection]  then taper.
-// MASKED handles the grid edges (Laplacian masks, cells past nz), receiver
-// rows and source cells; the plain path is branch-free.
-template <bool TWO_D, bool TRI, bool MASKED>
-__device__ __forceinline__ float4 update4(const StepArgs &a, const Col &col, int y, int gi,
-                                          bool lyok, bool taper, float wy, bool rec_here,
-                                          int r_idx, bool src_plane, const float4 &c,
-                                          const float4 &L, const float4 &R, const float4 &xm1,
-                                          const float4 &xp1, const float4 &xm2, const float4 &xp2,
-                                          const float4 &q0, const float4 &q1, const float4 &q3,
-                                          const float4 &q4, const float4 &pv, const float4 &vv4) {
-  float4 res;
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    const float cv = el(c, e);
-    const float zm1 = e == 0 ? L.w : el(c, e - 1);
-    const float zp1 = e == 3 ? R.x : el(c, e + 1);
-    const float zm2 = e == 0 ? L.z : (e == 1 ? L.w : el(c, e - 2));
-    const float zp2 = e == 2 ? R.x : (e == 3 ? R.y : el(c, e + 2));
-    float t = fmul(fmul(a.c0, cv), a.k0);
-    t = fadd(t, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
-    t = fadd(t, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
-    if (!TWO_D) {
-      t = fadd(t, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
-      t = fadd(t, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
-    }
-    t = fadd(t, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-    t = fadd(t, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-    float lap = t;
-    if (MASKED) lap = (col.lz[e] && col.lx && lyok) ? t : 0.f;
-    // prev = taper(u_{k-1} as stored)
-    float p = el(pv, e);
-    if (taper) {
-      p = fmul(p, col.wz[e]);
-      if (!TWO_D) p = fmul(p, col.wx);
-      p = fmul(p, wy);
-    }
-    const float vve = el(vv4, e);
-    float v = fadd(cv, fsub(cv, p));
-    v = fadd(v, fmul(lap, vve));
-    if (MASKED) {
-      const int iz = col.iz0 + e;
-      if (TRI) {
-        if (rec_here && iz == a.rz && (a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi))
-          v = fadd(v, fmul(vve, a.tri_dat[(size_t)a.it * a.nrx * a.nry + r_idx]));
-      } else if (src_plane) {
-        for (int s = 0; s < a.ns; s++) {
-          const int dz = iz - a.sz[s], dxs = TWO_D ? 0 : col.ix - a.sx[s], dys = y - a.sy[s];
-          if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
-            const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
-            v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
-          }
-        }
-      }
-    }
-    if (taper) {
-      v = fmul(v, col.wz[e]);
-      if (!TWO_D) v = fmul(v, col.wx);
-      v = fmul(v, wy);
-    }
-    if (MASKED && col.iz0 + e >= a.g.nz) v = 0.f;
-    set_el(res, e, v);
-  }
-  return res;
-}
-
-// TWO_D: dummy x axis (no x stencil terms, no x taper).
-// ZW: float4 columns along z per tile; TX: x columns per tile; P: prefetch depth.
-template <bool TWO_D, int ZW, int TX, int P, bool TRI>
-__global__ void __launch_bounds__(ZW *TX, TWO_D ? 1 : (ZW * TX >= 256 ? 2 : 3))
-    step_kernel(const StepArgs a) {
-  constexpr int NT = ZW * TX;
-  constexpr int W = ZW + 2;                 // smem row (float4) incl. z halo
-  constexpr int ROWS = TWO_D ? 1 : TX + 4;  // smem rows incl. x halo
-  constexpr int XH = TWO_D ? 0 : 2;         // x halo rows on each side
-  constexpr int CPL = W * ROWS;             // curr plane (float4)
-  constexpr int PPL = ZW * TX;              // prev / vv plane (float4)
-  // Slot reuse: the copy for plane i+P+4 is issued in iteration i, while
-  // other threads may still read planes i+1..i+4 (and planes 0..3 in
-  // iteration 0, for the queue); P+6 slots keep the writes clear of them.
-  constexpr int NC = P + 6;                 // curr planes in flight
-  constexpr int NP = P + 2;                 // prev / vv planes in flight
-  constexpr int NH = TWO_D ? 2 : (4 * ZW + 2 * TX);
-  constexpr int HK = (NH + NT - 1) / NT;
-  static_assert(TWO_D || ZW % 8 == 0, "3-D tiles need ZW % 8 == 0");
-  extern __shared__ float4 sm[];
-  float4 *s_cur = sm;
-  float4 *s_prev = sm + NC * CPL;
-  float4 *s_vv = s_prev + NP * PPL;
-
-  const Geo &g = a.g;
-  const int tid = threadIdx.x;
-  const int zl = TWO_D ? tid : (tid & 7) + 8 * (tid / (8 * TX));
-  const int xl = TWO_D ? 0 : (tid >> 3) % TX;
-  const int zt0 = blockIdx.z * ZW, xt0 = blockIdx.y * TX;
-  const int z4 = zt0 + zl;
-  Col col;
-  col.iz0 = 4 * z4;
-  col.ix = xt0 + xl;
-  const int iz0 = col.iz0, ix = col.ix;
-  const int y0 = blockIdx.x * a.ych;
-  const int y1 = min(g.ny, y0 + a.ych);
-  const int nplanes = y1 - y0;
-  const bool live = iz0 < g.nz && ix < g.nx;
-  const bool zx_ok = iz0 < g.nz && ix < g.nx + g.hx;  // the centre float4 is stored
-  const long long o_c = foff(g, iz0, ix, 0);
-  const int ci = (xl + XH) * W + zl + 1;  // centre slot in a curr plane
-  const int pi = xl * ZW + zl;            // slot in a prev / vv plane
-
-  // halo items of this thread: smem slot and global offset at y = 0
-  int h_slot[HK];
-  long long h_off[HK];
-  bool h_ok[HK];
-#pragma unroll
-  for (int k = 0; k < HK; k++) {
-    const int h = tid + k * NT;
-    int r = 0, c = 0;
-    if (h < NH) {
-      if (TWO_D) {
-        c = h == 0 ? 0 : ZW + 1;
-      } else if (h < 4 * ZW) {
-        const int rr = h / ZW;
-        r = rr < 2 ? rr : TX + rr;
-        c = 1 + h % ZW;
-      } else {
-        const int h2 = h - 4 * ZW;
-        r = 2 + (h2 >> 1);
-        c = (h2 & 1) ? ZW + 1 : 0;
-      }
-    }
-    const int z4g = zt0 + c - 1, xg = xt0 + r - XH;
-    h_slot[k] = h < NH ? r * W + c : -1;
-    h_ok[k] = h < NH && z4g >= -1 && z4g * 4 < g.nz && xg >= -g.hx && xg < g.nx + g.hx;
-    h_off[k] = h_ok[k] ? foff(g, z4g * 4, xg, 0) : 0;
-  }
-
-  bool zx_taper = false, lz_all = true;
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    const int iz = iz0 + e;
-    col.wz[e] = (live && iz < g.nz) ? a.wz[iz] : 1.f;
-    zx_taper |= col.wz[e] != 1.f;
-    col.lz[e] = iz >= g.lz0 && iz < g.lz1;
-    lz_all &= col.lz[e];
-  }
-  col.wx = (!TWO_D && live) ? a.wx[ix] : 1.f;
-  zx_taper |= col.wx != 1.f;
-  col.lx = TWO_D || (ix >= g.lx0 && ix < g.lx1);
-  const bool plain_zx = lz_all && col.lx && iz0 + 3 < g.nz;
-  const bool rec_zx = (a.rz >= iz0 && a.rz < iz0 + 4) && ix >= a.rx0 && ix < a.rx0 + a.nrx;
-  const bool in_zx = ix >= a.nbx && ix < a.nbx + a.nx1;
-  const bool img_step = a.img != nullptr;
-
-  for (int gi = 0; gi < a.ngroups; gi++) {
-    const float *cur = a.cur[gi];
-    float *nxt = a.nxt[gi];
-    const bool last = gi == a.ngroups - 1;
-    // curr plane k <-> y = y0 - 2 + k; prev/vv plane j <-> y = y0 + j
-    auto issue_cur = [&](int k) {
-      const int y = y0 - 2 + k;
-      const bool yok = y >= -g.hy && y < g.ny + g.hy;
-      float4 *dst = s_cur + (k % NC) * CPL;
-      const long long oy = g.sy * (long long)y;
-      cp16(dst + ci, cur + (zx_ok && yok ? o_c + oy : 0), zx_ok && yok);
-#pragma unroll
-      for (int q = 0; q < HK; q++)
-        if (h_slot[q] >= 0)
-          cp16(dst + h_slot[q], cur + (h_ok[q] && yok ? h_off[q] + oy : 0), h_ok[q] && yok);
-    };
-    auto issue_pv = [&](int j) {
-      const long long o = o_c + g.sy * (long long)(y0 + j);
-      cp16(s_prev + (j % NP) * PPL + pi, live ? nxt + o : nxt, live);
-      cp16(s_vv + (j % NP) * PPL + pi, live ? a.vv + o : a.vv, live);
-    };
-    for (int k = 0; k < 4; k++) issue_cur(k);
-#pragma unroll
-    for (int b = 0; b < P; b++) {
-      if (b < nplanes) {
-        issue_cur(b + 4);
-        issue_pv(b);
-      }
-      cp_commit();
-    }
-    float4 q0, q1, q2, q3, q4;
-    for (int i = 0; i < nplanes; i++) {
-      const int y = y0 + i;
-      if (i + P < nplanes) {
-        issue_cur(i + P + 4);
-        issue_pv(i + P);
-      }
-      cp_commit();
-      cp_wait<P>();
-      __syncthreads();
-      const float4 *pl = s_cur + ((i + 2) % NC) * CPL;
-      if (i == 0) {
-        q0 = s_cur[0 * CPL + ci];
-        q1 = s_cur[1 * CPL + ci];
-        q2 = s_cur[2 * CPL + ci];
-        q3 = s_cur[3 * CPL + ci];
-      }
-      q4 = s_cur[((i + 4) % NC) * CPL + ci];
-      if (live) {
-        const float4 L = pl[ci - 1], R = pl[ci + 1];
-        float4 xm1, xp1, xm2, xp2;
-        if (!TWO_D) {
-          xm1 = pl[ci - W];
-          xp1 = pl[ci + W];
-          xm2 = pl[ci - 2 * W];
-          xp2 = pl[ci + 2 * W];
-        }
-        const float4 pv = s_prev[(i % NP) * PPL + pi];
-        const float4 vv4 = s_vv[(i % NP) * PPL + pi];
-        const float wy = a.wy[y];
-        const bool taper = zx_taper || wy != 1.f;
-        const bool lyok = y >= g.ly0 && y < g.ly1;
-        const bool rec_here = rec_zx && y >= a.ry0 && y < a.ry0 + a.nry;
-        const int r_idx = rec_here ? (y - a.ry0) * a.nrx + (ix - a.rx0) : 0;
-        bool src_plane = false;
-        if (!TRI)
-          for (int s = 0; s < a.ns; s++) src_plane |= (y >= a.sy[s] - 1 && y <= a.sy[s] + 1);
-        float4 res;
-        if (plain_zx && lyok && !(TRI && rec_here) && !src_plane)
-          res = update4<TWO_D, TRI, false>(a, col, y, gi, lyok, taper, wy, rec_here, r_idx,
-                                           src_plane, q2, L, R, xm1, xp1, xm2, xp2, q0, q1, q3,
-                                           q4, pv, vv4);
-        else
-          res = update4<TWO_D, TRI, true>(a, col, y, gi, lyok, taper, wy, rec_here, r_idx,
-                                          src_plane, q2, L, R, xm1, xp1, xm2, xp2, q0, q1, q3,
-                                          q4, pv, vv4);
-        const long long o = o_c + g.sy * (long long)y;
-        *reinterpret_cast<float4 *>(nxt + o) = res;
-        if (gi == 0 && !TRI && rec_here && a.rec)
-          a.rec[(size_t)a.it * a.nrx * a.nry + r_idx] = el(res, a.rz - iz0);
-        const bool interior = in_zx && y >= a.nby && y < a.nby + a.ny1;
-        if (gi == 0 && a.wfd && interior) {
-#pragma unroll
-          for (int e = 0; e < 4; e++) {
-            const int iz = iz0 + e;
-            if (iz >= a.nbz && iz < a.nbz + a.nz1)
-              a.wfd[((size_t)(y - a.nby) * a.nx1 + (ix - a.nbx)) * a.nz1 + (iz - a.nbz)] = el(res, e);
-          }
-        }
-        if (last && img_step && interior) {
-          float4 prod = make_float4(1.f, 1.f, 1.f, 1.f);
-          for (int gg = 0; gg < a.ngroups; gg++) {
-            const float4 u = gg == gi ? res : *reinterpret_cast<const float4 *>(a.nxt[gg] + o);
-            prod.x = fmul(fmul(prod.x, u.x), u.x);
-            prod.y = fmul(fmul(prod.y, u.y), u.y);
-            prod.z = fmul(fmul(prod.z, u.z), u.z);
-            prod.w = fmul(fmul(prod.w, u.w), u.w);
-          }
-          float4 im = *reinterpret_cast<const float4 *>(a.img + o);
-#pragma unroll
-          for (int e = 0; e < 4; e++) {
-            const int iz = iz0 + e;
-            if (iz >= a.nbz && iz < a.nbz + a.nz1) set_el(im, e, fadd(el(im, e), el(prod, e)));
-          }
-          *reinterpret_cast<float4 *>(a.img + o) = im;
-        }
-      }
-      q0 = q1;
-      q1 = q2;
-      q2 = q3;
-      q3 = q4;
-    }
-    cp_wait_all();
-    __syncthreads();
-  }
-}
 
 // March kernel: register-marched, one float4 of z cells per thread.
 //
@@ -1088,19 +808,6 @@ __global__ void vel_stats_kernel(const float *v, long long n, unsigned int *out)
 
 // ------------------------------------------------------------------ host --
 
-// Compiled tile variants: 3-D (ZW, TX), 2-D (ZW); P = 2 stages of prefetch.
-constexpr int PF = 2;
-struct Variant {
-  int zw, tx;
-};
-static const Variant k3d[] = {{8, 16}, {16, 8}, {24, 8}, {32, 8}};
-static const Variant k2d[] = {{32, 1}, {64, 1}, {96, 1}, {128, 1}, {256, 1}};
-
-static size_t smem_bytes(bool two_d, int zw, int tx) {
-  const int W = zw + 2, rows = two_d ? 1 : tx + 4;
-  return sizeof(float4) * ((size_t)(PF + 6) * W * rows + 2ull * (PF + 2) * zw * tx);
-}
-
 struct Plan {
   int dim;
   int nz1, nx1, ny1, nb;
@@ -1108,7 +815,6 @@ struct Plan {
   int kbz, kbx, kby, knz1, knx1, kny1;
   Geo g;
   int nz2, nx2, ny2;  // the reference's padded sizes (model axes)
-  Variant v;
   int ych;
   dim3 grid;
   size_t smem;
@@ -1117,31 +823,6 @@ struct Plan {
   int threads;
   int S, ZS, KX, nzc, WPC, WZ, WX;
 };
-
-template <bool TWO_D, int ZW, int TX, bool TRI>
-static void *kernel_ptr() {
-  return (void *)step_kernel<TWO_D, ZW, TX, PF, TRI>;
-}
-
-static void *pick_kernel(bool two_d, Variant v, bool tri) {
-#define PW_K(D2, Z, T)                                                  \
-  if (two_d == D2 && v.zw == Z && v.tx == T)                           \
-    return tri ? kernel_ptr<D2, Z, T, true>() : kernel_ptr<D2, Z, T, false>();
-  PW_K(false, 8, 16) PW_K(false, 16, 8) PW_K(false, 24, 8) PW_K(false, 32, 8)
-  PW_K(true, 32, 1) PW_K(true, 64, 1) PW_K(true, 96, 1) PW_K(true, 128, 1) PW_K(true, 256, 1)
-#undef PW_K
-  return nullptr;
-}
-
-static int blocks_per_sm(void *fn, int threads, size_t smem) {
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem) != cudaSuccess) {
-    cudaGetLastError();
-    n = 1;
-  }
-  return std::max(n, 1);
-}
 
 template <bool TWO_D, bool TRI, bool SNAP>
 static void *march_ptr() {
@@ -1155,13 +836,9 @@ static void *march_ptr() {
   return f;
 }
 
-static void *march_fn(bool two_d, bool tri, bool snap) {
-  if (two_d) {
-    if (tri) return snap ? march_ptr<true, true, true>() : march_ptr<true, true, false>();
-    return snap ? march_ptr<true, false, true>() : march_ptr<true, false, false>();
-  }
-  if (tri) return snap ? march_ptr<false, true, true>() : march_ptr<false, true, false>();
-  return snap ? march_ptr<false, false, true>() : march_ptr<false, false, false>();
+static void *march_fn(bool tri, bool snap) {  // 2-D runs
+  if (tri) return snap ? march_ptr<true, true, true>() : march_ptr<true, true, false>();
+  return snap ? march_ptr<true, false, true>() : march_ptr<true, false, false>();
 }
 
 // Tile override for measurements: PW_AFD_TILE_G<G>="a,b" fixes the first two
@@ -1181,7 +858,7 @@ static void tile_override(int G, int &fa, int &fb) {
 static int plan_march(bool tri, int G, int nsm, Plan &p) {
   const Geo &g = p.g;
   const bool two_d = p.dim == 2;
-  void *fn = march_fn(two_d, tri, false);
+  void *fn = march_fn(tri, false);
   const int S = g.lz / 4;
   const int spw = 32 / G;
   const int live_slots = ceil_div(g.nz, 4);
@@ -1230,7 +907,7 @@ static int plan_march(bool tri, int G, int nsm, Plan &p) {
   }
   PW_CHECK(best > 0, PW_ERR_SHAPE, "no launchable tile for the step kernel");
   p.fn = fn;
-  p.fn_snap = march_fn(two_d, tri, true);
+  p.fn_snap = march_fn(tri, true);
   p.S = S;
   p.WPC = bw;
   p.ZS = bw * spw;
@@ -1371,53 +1048,12 @@ static int make_plan(const pw_afd_args *a, bool tri, int G, Plan &p) {
   }
   g.py = g.ny + 2 * g.hy;
 
-  // tile choice: fewest idle z lanes, then the largest tile
-  const int nz4 = ceil_div(enz, 4);
-  const Variant *list = two_d ? k2d : k3d;
-  const int nlist = two_d ? 5 : 4;
-  Variant best = list[0];
-  long long best_cover = -1;
-  for (int i = 0; i < nlist; i++) {
-    const long long cover = (long long)ceil_div(nz4, list[i].zw) * list[i].zw;
-    if (best_cover < 0 || cover < best_cover || (cover == best_cover && list[i].zw > best.zw)) {
-      best = list[i];
-      best_cover = cover;
-    }
-  }
-  p.v = best;
-  const int threads = best.zw * best.tx;
-  p.smem = smem_bytes(two_d, best.zw, best.tx);
-  void *fn = pick_kernel(two_d, best, tri);
-  PW_CHECK(fn != nullptr, PW_ERR_SHAPE, "no kernel variant");
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int slots = nsm * blocks_per_sm(fn, threads, p.smem);
-  const long long zx = (long long)ceil_div(nz4, best.zw) * ceil_div(g.nx, best.tx);
-  // planes per CTA: balance wave quantisation against the 4-plane prologue
-  double best_score = -1;
-  int best_ych = 8;
-  for (int ych : {64, 48, 40, 32, 24, 16, 12, 8, 6, 4}) {
-    const long long n = zx * ceil_div(g.ny, ych);
-    const long long waves = (n + slots - 1) / slots;
-    const double eff = (double)n / (double)(waves * slots);
-    const double pro = (double)ych / (ych + 1.0);
-    const double score = eff * pro;
-    if (score > best_score + 1e-9) {
-      best_score = score;
-      best_ych = ych;
-    }
-  }
-  p.ych = std::min(best_ych, g.ny);
-  p.grid = dim3(ceil_div(g.ny, p.ych), ceil_div(g.nx, best.tx), ceil_div(nz4, best.zw));
-  p.fn = p.fn_snap = fn;
-  p.tile = false;
-  p.threads = threads;
   p.S = p.ZS = p.KX = p.nzc = p.WPC = p.WZ = p.WX = 0;
-  if (getenv("PW_AFD_OLD") == nullptr) {
-    if (two_d || getenv("PW_AFD_MARCH")) PW_TRY(plan_march(tri, G, nsm, p));
-    else PW_TRY(plan_tile(tri, G, nsm, p));
-  }
+  if (two_d) PW_TRY(plan_march(tri, G, nsm, p));  // 2-D: no x neighbours to stage
+  else PW_TRY(plan_tile(tri, G, nsm, p));
   return PW_OK;
 }
 
