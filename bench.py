@@ -182,6 +182,23 @@ def _ref_worker(n, nt_s, seed):
     return wall, kind
 
 
+def max_over_ranks(x, world, device="cuda"):
+    """Largest value of x over the ranks (identity on one rank)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def job_rate(units_per_rank_step, steps, world, ms_max):
+    """Whole-job throughput: the units every rank processed over the
+    slowest rank's time (weak scaling: each rank has the same work)."""
+    return units_per_rank_step * steps * world / (ms_max / 1e3)
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -265,14 +282,10 @@ def main():
     if world > 1:
         dist.barrier()
     clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
     ms_step = ms / args.steps
     pts = (n + 2 * NBT) ** 3 * nt * G
-    value = pts * args.steps * world / (ms / 1e3) / 1e9
+    value = job_rate(pts, args.steps, world, ms) / 1e9
 
     # e2e: the same C-ABI call with pinned host buffers (copies inside the timed region)
     e2e = None
@@ -298,12 +311,8 @@ def main():
             step_host()
         h1.record()
         torch.cuda.synchronize()
-        ems = max(h0.elapsed_time(h1), (time.perf_counter() - t0) * 1e3)
-        if world > 1:
-            tt = torch.tensor([ems], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ems = float(tt.item())
-        e2e = {"value": pts * args.steps * world / (ems / 1e3) / 1e9, "unit": "Gpt/s",
+        ems = max_over_ranks(max(h0.elapsed_time(h1), (time.perf_counter() - t0) * 1e3), world)
+        e2e = {"value": job_rate(pts, args.steps, world, ems) / 1e9, "unit": "Gpt/s",
                "h2d_bytes_per_step": int(vel.nbytes + dat_h.numel() * 4 + groups.nbytes),
                "d2h_bytes_per_step": int(img_h.numel() * 4)}
 
