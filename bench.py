@@ -45,6 +45,10 @@ def parse():
     p.add_argument("--groups", type=int, default=4)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", default="tri3d", choices=["tri3d", "fwi2d"],
+                   help="tri3d: the 3-D TRI image (default); fwi2d: 2-D FWI gradients/s")
+    p.add_argument("--shots", type=int, default=32, help="fwi2d: shots per gradient")
+    p.add_argument("--fwi-nt", type=int, default=2000, help="fwi2d: time samples")
     return p.parse_args()
 
 
@@ -227,11 +231,234 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------
+# fwi2d: FWI gradients/s on a 300 x 600 model at 10 m (km units as pfwi uses)
+# --------------------------------------------------------------------------
+FWI_NZ, FWI_NX, FWI_H, FWI_DT, FWI_NB, FWI_COEF, FWI_F0 = 300, 600, 0.01, 0.001, 60, 0.005, 10.0
+
+
+def fwi2d_models(seed):
+    """True model: 8 seeded layers with velocities in [1.5, 4.5] km/s growing
+    with depth, plus two Gaussian anomalies of +10% and -10%; start model:
+    the true model Gaussian-smoothed with sigma = 15 points."""
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    z = np.arange(FWI_NZ)[:, None] + np.zeros((1, FWI_NX))
+    x = np.zeros((FWI_NZ, 1)) + np.arange(FWI_NX)[None, :]
+    ifaces = np.sort(rng.choice(np.arange(20, FWI_NZ - 10), 7, replace=False))
+    vals = np.sort(rng.uniform(1.5, 4.5, 8))
+    v = np.full((FWI_NZ, FWI_NX), vals[0])
+    for val, zi in zip(vals[1:], ifaces):
+        v[z >= zi] = val
+    for sign in (1.0, -1.0):
+        cz, cx = rng.uniform(0.3, 0.8) * FWI_NZ, rng.uniform(0.2, 0.8) * FWI_NX
+        v *= 1.0 + 0.1 * sign * np.exp(-((z - cz) ** 2 + (x - cx) ** 2) / (2 * 20.0 ** 2))
+    v = np.clip(v, 1.5, 4.5).astype(np.float32)
+    return v, gaussian_filter(v.astype(np.float64), 15.0).astype(np.float32)
+
+
+def fwi2d_par(ns, nt):
+    ds = FWI_NX * FWI_H / ns
+    return dict(nz=FWI_NZ, nx=FWI_NX, dz=FWI_H, dx=FWI_H, oz=0.0, ox=0.0, nt=nt, dt=FWI_DT,
+                ot=0.0, ns=ns, ds=ds, os=ds / 2, nb=FWI_NB, coef=FWI_COEF, f0=FWI_F0,
+                acqui_type=1, interval=1, niter=1)
+
+
+def fwi2d_wavelet(nt):
+    t = np.arange(nt) * FWI_DT - 1.2 / FWI_F0
+    a = (np.pi * FWI_F0 * t) ** 2
+    return ((1 - 2 * a) * np.exp(-a)).astype(np.float32)
+
+
+def _fwi_ref_worker(nt_s, seed):
+    """The reference's gradient_av (oracle/_ref/libpwref.so, built from its
+    sources) for one shot over nt_s steps on the full grid; wall seconds."""
+    sys.path.insert(0, ROOT)
+    import ctypes
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    L = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libpwref.so"))
+    f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+    L.refdrv_gradient.argtypes = [f32p, f32p, f32p, f32p, f32p, ctypes.c_int, f32p, f32p]
+    vt, vs = fwi2d_models(seed)
+    par = fwi2d_par(1, nt_s)
+    # the driver's parameter layout (oracle/ref_driver.c fill_acpar)
+    parr = np.array([par[k] for k in ("nz", "nx", "dz", "dx", "oz", "ox", "nt", "dt", "ot", "ns",
+                                      "ds", "os", "nb", "coef", "f0", "acqui_type", "interval")],
+                    np.float32)
+    wav = fwi2d_wavelet(nt_s)
+    dobs = np.zeros(nt_s * FWI_NX, np.float32)
+    q = np.ones(FWI_NZ * FWI_NX, np.float32)
+    g = np.zeros(FWI_NZ * FWI_NX, np.float32)
+    fc = np.zeros(1, np.float32)
+    t0 = time.perf_counter()
+    L.refdrv_gradient(parr, np.ascontiguousarray(vs.flatten(order="F")), q, wav, dobs, 1, g, fc)
+    return time.perf_counter() - t0
+
+
+def _fwi_ref_worker_spawned(nt_s):
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(1) as pool:
+        return pool.apply(_fwi_ref_worker, (nt_s, 7))
+
+
+def run_fwi2d(args, world, rank, local):
+    ns, nt = args.shots, args.fwi_nt
+    pad = (FWI_NZ + 2 * FWI_NB) * (FWI_NX + 2 * FWI_NB)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        import multiprocessing as mp
+        nt_s, workers = 200, max(1, min(os.cpu_count() or 1, 16))
+        rates = []
+        with mp.get_context("spawn").Pool(workers) as pool:
+            for i in range(args.warmup + args.steps):
+                walls = pool.starmap(_fwi_ref_worker, [(nt_s, 7)] * workers)
+                if i >= args.warmup:
+                    rates.append(workers / max(walls) * nt_s / (ns * nt))
+        value = statistics.median(rates)
+        print(json.dumps({
+            "impl": "reference", "metric": f"FWI gradients/s (2-D, {ns} shots)", "value": value,
+            "unit": "gradients/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": f"2-D FWI gradient {FWI_NZ}x{FWI_NX} h=10m "
+                                                         f"nt={nt} shots={ns} nb={FWI_NB}"},
+            "cpu_baseline": {"value": value, "unit": "gradients/s", "cores": workers,
+                             "kind": "reference",
+                             "sample": f"gradient_av of 1 shot, {nt_s} of {nt} steps, {workers} "
+                                       f"independent single-threaded processes, scaled to "
+                                       f"{ns} shots x {nt} steps"},
+            "e2e": {"value": value, "unit": "gradients/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import ctypes
+    import torch
+    import torch.distributed as dist
+    from pywave_b200 import _lib as L
+    from pywave_b200 import build as B
+    from pywave_b200 import fwi
+    B.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    st = torch.cuda.current_stream().cuda_stream
+    lib = L.lib()
+    vt, vs = fwi2d_models(11 + rank)
+    par = fwi2d_par(ns, nt)
+    wav = fwi2d_wavelet(nt)
+    a = fwi.fwi_args(par, 0)
+    dev = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).cuda()
+    vt_d = dev(vt.flatten(order="F"))
+    vs_d = dev(vs.flatten(order="F"))
+    wav_d = dev(wav)
+    dobs_d = torch.empty(ns * FWI_NX * nt, device="cuda")
+    L.check(lib.pw_pfwi_forward(a, vt_d.data_ptr(), wav_d.data_ptr(), dobs_d.data_ptr(), st))
+    g_d = torch.empty(FWI_NZ * FWI_NX, device="cuda")
+    J = ctypes.c_double(0.0)
+
+    def grad(flags, mode):
+        a.flags = flags
+        L.check(lib.pw_pfwi_gradient(a, mode, vs_d.data_ptr(), wav_d.data_ptr(), dobs_d.data_ptr(),
+                                     None, g_d.data_ptr(), ctypes.byref(J), 0, st))
+        return L.last_timing()
+
+    def timed(flags, steps, mode=L.PW_GRAD_EXACT):
+        for _ in range(args.warmup):
+            grad(flags, mode)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        loops, launches = [], 0
+        e0.record()
+        for _ in range(steps):
+            ms, nst, tot = grad(flags, mode)
+            loops.append(ms)
+            launches += tot
+        e1.record()
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), world), statistics.median(loops), launches
+
+    clk = Clocks(local)
+    clk.start()
+    ms_b, loop_b, launches = timed(0, args.steps)
+    clocks = clk.stop()
+    value = job_rate(1, args.steps, world, ms_b)
+    nplain = max(1, args.steps // 2)
+    ms_p, _, _ = timed(L.PW_PER_SHOT, nplain)
+    plain = job_rate(1, nplain, world, ms_p)
+    ms_r, _, _ = timed(0, args.steps, L.PW_GRAD_REFERENCE)
+    ref_mode = job_rate(1, args.steps, world, ms_r)
+
+    e2e = None
+    if not args.no_e2e:
+        vs_h = torch.from_numpy(np.ascontiguousarray(vs.flatten(order="F"))).pin_memory()
+        dobs_h = dobs_d.cpu().pin_memory()
+        g_h = torch.empty(FWI_NZ * FWI_NX).pin_memory()
+        ah = fwi.fwi_args(par, L.PW_HOST_PTRS)
+        wav_h = torch.from_numpy(wav).pin_memory()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            L.check(lib.pw_pfwi_gradient(ah, L.PW_GRAD_EXACT, vs_h.data_ptr(), wav_h.data_ptr(),
+                                         dobs_h.data_ptr(), None, g_h.data_ptr(), ctypes.byref(J),
+                                         0, st))
+        torch.cuda.synchronize()
+        ems = max_over_ranks((time.perf_counter() - t0) * 1e3, world)
+        e2e = {"value": job_rate(1, args.steps, world, ems), "unit": "gradients/s",
+               "h2d_bytes_per_step": int(vs.nbytes + wav.nbytes + dobs_h.numel() * 4),
+               "d2h_bytes_per_step": int(g_h.numel() * 4 + 8)}
+
+    peak, peak_kind = peaks()
+    alg = 52.0 * pad * nt * ns  # forward 16 B + exact adjoint 36 B per point-step-shot
+    achieved = alg / (loop_b / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            wall = _fwi_ref_worker_spawned(200)
+            cpu = {"value": 200 / (ns * nt) / wall, "unit": "gradients/s", "cores": 1,
+                   "kind": "reference",
+                   "sample": f"gradient_av of 1 shot, 200 of {nt} steps, 1 core ({wall:.1f} s), "
+                             f"scaled to {ns} shots x {nt} steps"}
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "unit": "gradients/s", "cores": 1, "kind": "reference",
+                   "sample": f"failed: {ex!r}"[:200]}
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"FWI gradients/s (2-D exact adjoint, {ns} shots batched)", "value": value,
+            "unit": "gradients/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 misfit)",
+            "data": "synthetic (seeded layered model, start = smoothed true model)",
+            "config": {"workload": f"2-D FWI gradient {FWI_NZ}x{FWI_NX} h=10m nt={nt} dt=1ms "
+                                   f"shots={ns} nb={FWI_NB} 10 Hz Ricker, exact adjoint with "
+                                   f"checkpoints", "padded_cells": pad,
+                       "l2": "inputs larger than L2 (observed data "
+                             f"{dobs_d.numel() * 4 / 1e6:.0f} MB)"},
+            "plain_per_shot": {"value": plain, "unit": "gradients/s"},
+            "batched_over_plain": value / plain,
+            "reference_mode_gradient": {"value": ref_mode, "unit": "gradients/s",
+                                        "note": "gradient_av imaging, batched"},
+            "e2e": e2e, "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "pf_step_kernel FWD + ADJ_EXACT (whole gradient loop)",
+                         "alg_bytes_per_gradient": alg, "loop_ms": loop_b,
+                         "peak_source": peak_kind},
+            "cpu_baseline": cpu, "clocks": clocks}), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "fwi2d":
+        return run_fwi2d(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, rank)
 
