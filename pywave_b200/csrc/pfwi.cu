@@ -61,6 +61,7 @@ struct PfArgs {
   float wdt2;
   const float *vint;          // interior velocity [nx][nz]
   float *grad;                // [nx][nz] (ADJ_REF) or field layout (ADJ_EXACT: sum phi*term)
+  long long gstride;          // floats between the shots' gradient slices (0: one accumulator)
   const float *tin;           // ADJ_EXACT: term of the forward step [shot] (field layout)
   long long tin_stride;
   int imaging;                // this step images
@@ -110,16 +111,18 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
   float4 *s_t = s_V + NP * ZW;  // ADJ_EXACT: forward term tile
 
   const int tid = threadIdx.x;
-  const int z4 = blockIdx.y * ZW + tid;
+  const int s = blockIdx.x;  // shot of the batch: fastest, so the shots of one x chunk
+                             // run together and share V through L2
+  const int z4 = blockIdx.z * ZW + tid;
   const int iz0 = 4 * z4;
-  const int x0 = blockIdx.x * xch;
+  const int x0 = blockIdx.y * xch;
   const int x1 = min(a.pnx, x0 + xch);
   const int nplanes = x1 - x0;
   const int lz = a.lz;
   const bool live = iz0 < a.pnz;
   const long long o_c = pfoff(lz, iz0, 0);
   const int ci = tid + 1;
-  const int hz4 = tid == 0 ? blockIdx.y * ZW - 1 : blockIdx.y * ZW + ZW;  // halo float4 (threads 0, 1)
+  const int hz4 = tid == 0 ? blockIdx.z * ZW - 1 : blockIdx.z * ZW + ZW;  // halo float4 (threads 0, 1)
   const bool has_h = tid < 2;
   const int hslot = tid == 0 ? 0 : ZW + 1;
   const bool h_ok = has_h && hz4 >= -1 && hz4 * 4 < a.pnz;
@@ -136,7 +139,8 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
   }
   const bool rec_row = a.rz >= iz0 && a.rz < iz0 + 4;
 
-  for (int s = 0; s < a.nshots; s++) {
+  float *const gs = a.grad + s * a.gstride;  // this shot's gradient accumulator
+  {
     const float *cur = a.cur[s];
     float *nxt = a.nxt[s];
     const float *tin = MODE == ADJ_EXACT ? a.tin + s * a.tin_stride : nullptr;
@@ -240,12 +244,12 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
         if (MODE == ADJ_EXACT && a.imaging) {
           // dJ/dV accumulates phi_n * term_n (divided by V at the end)
           const float4 tf = s_t[(i % NP) * ZW + tid];
-          float4 gacc = *reinterpret_cast<const float4 *>(a.grad + o);
+          float4 gacc = *reinterpret_cast<const float4 *>(gs + o);
           gacc.x = fadd(gacc.x, fmul(c.x, tf.x));
           gacc.y = fadd(gacc.y, fmul(c.y, tf.y));
           gacc.z = fadd(gacc.z, fmul(c.z, tf.z));
           gacc.w = fadd(gacc.w, fmul(c.w, tf.w));
-          *reinterpret_cast<float4 *>(a.grad + o) = gacc;
+          *reinterpret_cast<float4 *>(gs + o) = gacc;
         }
         if (MODE == ADJ_REF && a.imaging && interior) {
           // gradient_av (wave_fwigradient.c:221-230), evaluated in double as
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
               const double w1 = a.wnext[s * a.wstride + k], w0 = a.wcur[s * a.wstride + k],
                            wm = a.wprev[s * a.wstride + k];
               const double gsum = (w1 - 2. * w0 + wm) / (double)a.wdt2 * (double)el(c, e) * (double)temp;
-              a.grad[k] = (float)((double)a.grad[k] + gsum);
+              gs[k] = (float)((double)gs[k] + gsum);
             }
           }
         }
@@ -305,6 +309,16 @@ __global__ void residual_kernel(const float *d, const float *dobs, const float *
     double v = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (threadIdx.x == 0) atomicAdd(misfit, v);
+  }
+}
+
+// total[i] += slice_0[i] + slice_1[i] + ... in shot order (deterministic)
+__global__ void sum_slices_kernel(const float *slices, int nb, long long n, float *total) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    float v = total[i];
+    for (int s = 0; s < nb; s++) v = fadd(v, slices[s * n + i]);
+    total[i] = v;
   }
 }
 
@@ -505,8 +519,7 @@ struct Setup {
   int nr, rz, drv, sz;
   std::vector<ShotGeo> geo;
   std::vector<float> bz, bx;
-  int zw, xch;
-  dim3 grid;
+  int zw, ztiles, nsm;
   size_t smem;
 };
 
@@ -578,11 +591,8 @@ static int setup(const pw_fwi_args *a, Setup &S) {
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  // planes per CTA: enough CTAs to fill every SM a few times
-  int xch = 64;
-  while (xch > 8 && (long long)ztiles * ceil_div(S.pnx, xch) < 4LL * nsm) xch /= 2;
-  S.xch = xch;
-  S.grid = dim3(ceil_div(S.pnx, xch), ztiles);
+  S.ztiles = ztiles;
+  S.nsm = nsm;
   return PW_OK;
 }
 
@@ -602,7 +612,12 @@ static int launch_one(const Setup &S, const PfArgs &p, cudaStream_t st) {
                          (int)smem);
     attr = true;
   }
-  pf_step_kernel<ZW, PFP, MODE><<<S.grid, ZW, smem, st>>>(p, S.xch);
+  // x planes per CTA: long enough to amortise the 8-plane prologue, short
+  // enough that shots x chunks x z tiles fill every SM a few times
+  int xch = 128;
+  while (xch > 16 && (long long)p.nshots * S.ztiles * ceil_div(S.pnx, xch) < 6LL * S.nsm) xch /= 2;
+  const dim3 grid(p.nshots, ceil_div(S.pnx, xch), S.ztiles);
+  pf_step_kernel<ZW, PFP, MODE><<<grid, ZW, smem, st>>>(p, xch);
   PW_CUDA(cudaGetLastError());
   return PW_OK;
 }
@@ -834,7 +849,7 @@ static void plan_exact(const Setup &S, int ckpt_k, int &k, int &nsb) {
   nsb = std::min(S.a.ns, MAXS);
   while (nsb > 1) {
     const int nck = (nt + k - 1) / k;
-    const double need = fb * nsb * (4.0 + 2.0 * nck + k) + fb * 2;
+    const double need = fb * nsb * (5.0 + 2.0 * nck + k) + fb * 2;
     if (need <= budget) break;
     nsb = (nsb + 1) / 2;
   }
@@ -876,6 +891,10 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   const size_t o_ck = cv.add(exact ? (size_t)nsb * nck * 2 * S.fstride * 4 : 0);
   const size_t o_tb = cv.add(exact ? (size_t)nsb * k * S.fstride * 4 : 0);
   const size_t o_ga = cv.add(exact ? (size_t)S.fstride * 4 : 0);
+  // shots of one launch run in different CTAs: each accumulates its gradient
+  // in its own slice, summed into the total in shot order after the batch
+  const size_t gslice = exact ? (size_t)S.fstride : nvel;
+  const size_t o_gs = cv.add(nsb > 1 ? (size_t)nsb * gslice * 4 : 0);
   const size_t o_grad = cv.add(nvel * 4);
   const size_t o_mis = cv.add(16);
   const size_t o_mx = cv.add(16);
@@ -921,7 +940,10 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   p.wav = at<float>(base, o_wav);
   p.vint = d_vel;
   p.wdt2 = (a->dt * interval) * (a->dt * interval);
-  p.grad = exact ? gacc : gdev;
+  float *gtotal = exact ? gacc : gdev;
+  float *gslices = at<float>(base, o_gs);
+  p.grad = nsb > 1 ? gslices : gtotal;
+  p.gstride = nsb > 1 ? (long long)gslice : 0;
   const size_t fs = (size_t)S.fstride;
   long long launches = 0;
   LoopTimer timer(st);
@@ -1048,6 +1070,12 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
       }
       p.tin = nullptr;
       p.imaging = 0;
+    }
+    if (nsb > 1) {
+      sum_slices_kernel<<<592, 256, 0, st>>>(gslices, nb_, (long long)gslice, gtotal);
+      PW_CUDA(cudaGetLastError());
+      PW_CUDA(cudaMemsetAsync(gslices, 0, (size_t)nb_ * gslice * 4, st));
+      launches++;
     }
   }
   timer.stop();
