@@ -28,6 +28,7 @@ constexpr int MAXSRCW = 16;  // source-map cells per shot
 struct ShotGeo {
   int r0v, r02, nr2;          // receivers rx = r0v + ir*drv, ir < nr2, stored at trace r02 + ir
   int nsrc;                   // non-zero source-map cells
+  int sx0, sx1, sz0, sz1;     // bounding box of those cells
   int scell[MAXSRCW];         // (ix << 16) | iz of each cell
   float sw[MAXSRCW];          // source-map weight rr
 };
@@ -145,6 +146,9 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
     float *nxt = a.nxt[s];
     const float *tin = MODE == ADJ_EXACT ? a.tin + s * a.tin_stride : nullptr;
     const ShotGeo &sg = a.geo[s];
+    const int r0v = sg.r0v, r02 = sg.r02, nr2 = sg.nr2;
+    const int sx0 = sg.sx0, sx1 = sg.sx1;
+    const bool src_z = MODE == FWD && iz0 <= sg.sz1 && iz0 + 3 >= sg.sz0;
     auto issue_cur = [&](int k) {  // plane x = x0 - 4 + k
       const int x = x0 - 4 + k;
       const bool xok = x >= -HX && x < a.pnx + HX;
@@ -195,9 +199,13 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
         // receivers read the field before the update (wave_fwimodeling.c:76-79)
         int rir = -1;
         if (rec_row) {
-          const int d = x - sg.r0v;
-          if (d >= 0 && d % a.drv == 0 && d / a.drv < sg.nr2) rir = sg.r02 + d / a.drv;
+          const int d = x - r0v;
+          if (d >= 0) {
+            const int ir = a.drv == 1 ? d : (d % a.drv == 0 ? d / a.drv : -1);
+            if (ir >= 0 && ir < nr2) rir = r02 + ir;
+          }
         }
+        const bool src_here = src_z && x >= sx0 && x <= sx1;
         if (MODE == FWD && rir >= 0 && a.rec)
           a.rec[((size_t)s * a.nt + a.it) * a.nr + rir] = el(c, a.rz - iz0);
         const bool interior = x >= a.nb && x < a.nb + a.nx;
@@ -226,8 +234,9 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
           tz = fadd(tz, fmul(a.c4, fadd(znb(L, c, R, e, 4), znb(L, c, R, e, -4))));
           float t = (lz_ok[e] && lx_ok) ? fadd(fdiv(tx, a.dx2), fdiv(tz, a.dz2)) : 0.f;
           if (MODE == FWD) {
-            for (int k = 0; k < sg.nsrc; k++)
-              if (sg.scell[k] == ((x << 16) | iz)) t = fadd(t, fmul(sg.sw[k], a.wav[a.it]));
+            if (src_here)
+              for (int k = 0; k < sg.nsrc; k++)
+                if (sg.scell[k] == ((x << 16) | iz)) t = fadd(t, fmul(sg.sw[k], a.wav[a.it]));
           } else if (rir >= 0 && iz == a.rz) {
             t = fadd(t, a.res[((size_t)s * a.nt + a.it) * a.nr + rir]);
           }
@@ -496,6 +505,8 @@ static int source_map(int sx, int sz, int pnz, int pnx, ShotGeo &sg) {
   for (int j = 0; j < nxw; j++) smooth_line_host(2, nzw, m.data(), (long long)j * nzw, 1, tmp);
   for (int j = 0; j < nzw; j++) smooth_line_host(2, nxw, m.data(), j, nzw, tmp);
   sg.nsrc = 0;
+  sg.sx0 = sg.sz0 = 1 << 30;
+  sg.sx1 = sg.sz1 = -1;
   for (int ix = 0; ix < nxw; ix++)
     for (int iz = 0; iz < nzw; iz++) {
       const float w = m[(size_t)ix * nzw + iz];
@@ -507,6 +518,10 @@ static int source_map(int sx, int sz, int pnz, int pnx, ShotGeo &sg) {
         sg.scell[sg.nsrc] = (gx << 16) | gz;
         sg.sw[sg.nsrc] = w;
         sg.nsrc++;
+        sg.sx0 = std::min(sg.sx0, gx);
+        sg.sx1 = std::max(sg.sx1, gx);
+        sg.sz0 = std::min(sg.sz0, gz);
+        sg.sz1 = std::max(sg.sz1, gz);
       }
     }
   return PW_OK;
