@@ -66,6 +66,21 @@ typedef struct pw_afd_args {
 int pw_afd(const pw_afd_args *a, const float *vel, const float *src, const float *wavelet,
            float *dat, float *wfd, void *stream);
 
+/* Forward modelling of nshot 2-D shots of uneven size and length in one
+ * lockstep time loop: the reference's afd2d forward (afd.c:316, wave_fdm.c:
+ * 397-686) run for many shots at once, one kernel launch per time step over
+ * the tiles of every shot still running (shots end at their own nt), with
+ * the tile shape picked by timing candidates on the first steps and the
+ * remaining steps replayed as one CUDA graph (when `stream` is not the
+ * legacy default stream).  Traces are bit-identical to pw_afd per shot.
+ *   args[k]      each shot's pw_afd_args (dim 2, tri 0, jsnap 0; one
+ *                PW_HOST_PTRS setting for all shots)
+ *   vel[k], src[k], wavelet[k] (wavelet may be NULL, or wavelet[k] NULL:
+ *                the Ricker table), dat[k] [nx][nt] traces, as in pw_afd */
+int pw_afd_batch(int nshot, const pw_afd_args *args, const float *const *vel,
+                 const float *const *src, const float *const *wavelet, float *const *dat,
+                 void *stream);
+
 /* Size of the fixed device scratch array behind pw_afd_noalloc (32 MiB). */
 #define PW_NOALLOC_SCRATCH_BYTES (32u << 20)
 

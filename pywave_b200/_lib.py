@@ -73,6 +73,7 @@ _vp = C.c_void_p
 _SIGS = {
     "pw_afd": (C.c_int, [C.POINTER(AfdArgs), _vp, _vp, _vp, _vp, _vp, _vp]),
     "pw_afd_noalloc": (C.c_int, [C.POINTER(AfdArgs), _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pw_afd_batch": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp]),
     "pw_tri_image": (C.c_int, [C.POINTER(AfdArgs), C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp]),
     "pw_fwi_args_from_pararray": (C.c_int, [_vp, C.c_int, C.POINTER(FwiArgs)]),
     "pw_pfwi_forward": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp]),

@@ -117,3 +117,47 @@ def tri_image(vel, dat, dt=0.001, d=None, ngroups=4, groups=None, nbt=30, ct=0.0
     L.check(L.lib().pw_tri_image(a, int(ngroups), L.ptr(groups), L.ptr(vflat), L.ptr(src),
                                  L.ptr(img), 1 if normalize else 0, None))
     return img.reshape((nz, nx) if dim == 2 else (nz, nx, ny), order="F")
+
+
+def afd2d_batch(shots, stream=None):
+    """Forward modelling of many 2-D shots of uneven size and length in one
+    lockstep time loop (pw_afd_batch).  ``shots`` is a list of dicts with
+    afd2d's keywords: ``vel`` [nz, nx], ``nt``, ``dt``, ``ax``, ``az``, ``ns``,
+    ``sx``, ``sz``, ``f``, ``t``, ``A``, ``nbt``, ``ct`` and optionally ``gz``
+    and ``wavelet`` [ns][nt].  Returns the list of gathers (nt, nx), each
+    identical to what afd2d(..., jsnap=0) returns for that shot."""
+    import ctypes as C
+    n = len(shots)
+    args = (L.AfdArgs * n)()
+    keep, vp, sp, wp, dp = [], [], [], [], []
+    outs = []
+    any_wav = any(sh.get("wavelet") is not None for sh in shots)
+    for k, sh in enumerate(shots):
+        vel = L.f32(np.asarray(sh["vel"]).flatten(order="F"))
+        ox, dx, nx = sh["ax"]
+        oz, dz, nz = sh["az"]
+        nt, ns = sh["nt"], sh["ns"]
+        src = L.f32(np.concatenate([np.asarray(sh[key], np.float32).reshape(-1)
+                                    for key in ("sx", "sz", "f", "t", "A")]))
+        a = args[k]
+        a.dim, a.nz, a.nx, a.ny, a.nt = 2, nz, nx, 1, nt
+        a.nbt, a.ct, a.dt, a.dz, a.dx, a.dy = sh.get("nbt", 30), sh.get("ct", 0.01), sh["dt"], dz, dx, dx
+        a.ns, a.tri, a.jsnap, a.gz, a.flags = ns, 0, 0, sh.get("gz", 0), L.PW_HOST_PTRS
+        wav = sh.get("wavelet")
+        wav = None if wav is None else L.f32(wav)
+        out = np.empty(nt * nx, np.float32)
+        keep += [vel, src, wav, out]
+        vp.append(vel.ctypes.data)
+        sp.append(src.ctypes.data)
+        wp.append(None if wav is None else wav.ctypes.data)
+        dp.append(out.ctypes.data)
+        outs.append((out, nt, nx))
+    VP = (C.c_void_p * n)(*vp)
+    SP = (C.c_void_p * n)(*sp)
+    WP = (C.c_void_p * n)(*wp) if any_wav else None
+    DP = (C.c_void_p * n)(*dp)
+    L.check(L.lib().pw_afd_batch(n, C.cast(args, C.c_void_p), C.cast(VP, C.c_void_p),
+                                 C.cast(SP, C.c_void_p),
+                                 None if WP is None else C.cast(WP, C.c_void_p),
+                                 C.cast(DP, C.c_void_p), stream))
+    return [o.reshape(nt, nx, order="F") for o, nt, nx in outs]

@@ -131,9 +131,10 @@ __device__ __forceinline__ void cp16ca(float4 *dst, const float *src, bool valid
                : "memory");
 }
 
+// One CTA's work: (bx, by) = (z chunk + x tile, y chunk) of the field that
+// `a` describes; `ring` is the CTA's dynamic shared memory.
 template <bool TWO_D, bool TRI, bool SNAP>
-__global__ void __launch_bounds__(MARCH_MAXT) march_kernel(const StepArgs a) {
-  extern __shared__ float4 ring[];
+__device__ __forceinline__ void march_body(const StepArgs &a, int bx, int by, float4 *ring) {
   constexpr int NS = MARCH_NS, D = NS - 1;
   const Geo &g = a.g;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
@@ -144,8 +145,8 @@ __global__ void __launch_bounds__(MARCH_MAXT) march_kernel(const StepArgs a) {
   const int sl = lane / G;
   const int xl = w / a.WPC;
   const int zs = (w - xl * a.WPC) * spw + sl;
-  const int slot = (blockIdx.x % a.nzc) * a.ZS + zs;
-  const int ix = TWO_D ? 0 : (int)(blockIdx.x / a.nzc) * a.KX + xl;
+  const int slot = (bx % a.nzc) * a.ZS + zs;
+  const int ix = TWO_D ? 0 : (bx / a.nzc) * a.KX + xl;
   const bool valid = sl < spw && zs < a.ZS && slot < a.S && xl < a.KX && ix < g.nx;
   const int iz0 = 4 * slot - HZ;
   const bool live = valid && slot >= 1 && iz0 < g.nz;
@@ -179,7 +180,7 @@ __global__ void __launch_bounds__(MARCH_MAXT) march_kernel(const StepArgs a) {
   const bool in_zx = ix >= a.nbx && ix < a.nbx + a.nx1;
   const int nrec = a.nrx * a.nry;
 
-  const int y0 = blockIdx.y * a.ych;
+  const int y0 = by * a.ych;
   const int y1 = min(g.ny, y0 + a.ych);
   float4 *rA = ring, *rB = ring + NS * nth, *rV = ring + 2 * NS * nth;
   // plane y's copies: A at y+2 (the queue's leading plane), B and vv at y
@@ -333,6 +334,40 @@ __global__ void __launch_bounds__(MARCH_MAXT) march_kernel(const StepArgs a) {
     q3 = q4;
   }
   cp_wait_all();
+}
+
+template <bool TWO_D, bool TRI, bool SNAP>
+__global__ void __launch_bounds__(MARCH_MAXT) march_kernel(const StepArgs a) {
+  extern __shared__ float4 ring[];
+  march_body<TWO_D, TRI, SNAP>(a, blockIdx.x, blockIdx.y, ring);
+}
+
+// Batched 2-D forward modelling of shots of uneven size and length: one
+// launch per time step covers the tiles of every shot still running.  Item
+// i = (shot, tile) with tile = z chunk + nzc * y chunk; items are ordered by
+// decreasing shot length so that the launch at step `it` takes a prefix.
+// The shot's arguments are copied into shared memory; A and B of a shot swap
+// roles with the parity of the step.
+__global__ void __launch_bounds__(MARCH_MAXT) batch_kernel(const StepArgs *args, const int2 *items,
+                                                           int it) {
+  extern __shared__ float4 ring[];
+  __shared__ StepArgs sa;
+  const int2 item = items[blockIdx.x];
+  const int *src = reinterpret_cast<const int *>(args + item.x);
+  int *dst = reinterpret_cast<int *>(&sa);
+  for (int i = threadIdx.x; i < (int)(sizeof(StepArgs) / sizeof(int)); i += blockDim.x)
+    dst[i] = src[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sa.it = it;
+    if (it & 1) {
+      float *t = sa.nxt[0];
+      sa.nxt[0] = const_cast<float *>(sa.cur[0]);
+      sa.cur[0] = t;
+    }
+  }
+  __syncthreads();
+  march_body<true, false, false>(sa, item.y % sa.nzc, item.y / sa.nzc, ring);
 }
 
 // Warp-tile kernel (3-D): each warp owns an 8-slot x 4-column patch of one
@@ -1385,6 +1420,359 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   return PW_OK;
 }
 
+
+// ------------------------------------------------- batched 2-D forward --
+// pw_afd_batch: forward modelling of many 2-D shots of uneven size and nt in
+// lockstep, one batch_kernel launch per time step over all running shots.
+
+struct BatchShot {
+  Plan p;
+  int ns;
+  std::vector<int> ksz, ksy;
+  std::vector<float> rick, wz, wy;
+  size_t nvel, nrec, nfield;
+  size_t o_vv, o_A, o_B, o_t, o_rick, o_vel, o_rec, o_dat, o_mx;
+};
+
+// Host part of run()'s set-up for one forward 2-D shot: plan, sources,
+// wavelets and taper tables, and its slices of the workspace.
+static int batch_setup(const pw_afd_args *a, const float *src, const float *wavelet, bool host,
+                       Carve &cv, BatchShot &b) {
+  PW_CHECK(a->dim == 2, PW_ERR_SHAPE, "pw_afd_batch runs 2-D shots only (dim=%d)", a->dim);
+  PW_CHECK(a->tri == 0, PW_ERR_VALUE, "pw_afd_batch runs forward modelling only (tri = 0)");
+  PW_CHECK(a->jsnap == 0, PW_ERR_VALUE, "pw_afd_batch records traces only (jsnap = 0)");
+  PW_CHECK(a->gz >= 0 && a->gz < a->nz, PW_ERR_SHAPE, "receiver depth gz=%d outside [0,%d)", a->gz,
+           a->nz);
+  Plan &p = b.p;
+  PW_TRY(make_plan(a, false, 1, p));
+  const Geo &g = p.g;
+  const int nt = a->nt;
+  b.ns = a->ns;
+  PW_CHECK(b.ns >= 0 && b.ns <= MAXSRC, PW_ERR_SHAPE, "ns must be in [0,%d] (got %d)", MAXSRC,
+           b.ns);
+  std::vector<float> s((size_t)5 * b.ns);
+  if (b.ns > 0) {
+    PW_CHECK(src != nullptr, PW_ERR_VALUE, "source array is null");
+    if (host) memcpy(s.data(), src, s.size() * sizeof(float));
+    else PW_CUDA(cudaMemcpy(s.data(), src, s.size() * sizeof(float), cudaMemcpyDeviceToHost));
+  }
+  b.rick.assign((size_t)std::max(b.ns, 1) * nt, 0.f);
+  for (int i = 0; i < b.ns; i++) {
+    // afd.c:416-425: positions are truncated to int
+    const int spx = (int)s[i], spz = (int)s[b.ns + i];
+    const float f0 = s[2 * b.ns + i], t0 = s[3 * b.ns + i], A = s[4 * b.ns + i];
+    PW_CHECK(spx >= 0 && spx < p.nx1 && spz >= 0 && spz < p.nz1, PW_ERR_SHAPE,
+             "source %d at (z=%d,x=%d) outside the model", i, spz, spx);
+    PW_CHECK(p.nb >= 1 || (spx > 0 && spx < p.nx1 - 1 && spz > 0 && spz < p.nz1 - 1),
+             PW_ERR_SHAPE, "source %d stencil leaves the grid", i);
+    b.ksz.push_back(spz + p.nb);
+    b.ksy.push_back(spx + p.nb);
+    if (wavelet == nullptr) {
+      PW_CHECK(t0 >= 0.f && (int)(t0 / a->dt) < nt, PW_ERR_VALUE,
+               "source %d onset t=%g outside [0, nt*dt)", i, t0);
+      ricker_table(nt, a->dt, f0, t0, A, b.rick.data() + (size_t)i * nt);
+    }
+  }
+  if (wavelet != nullptr && b.ns > 0) {
+    if (host) memcpy(b.rick.data(), wavelet, (size_t)b.ns * nt * sizeof(float));
+    else PW_CUDA(cudaMemcpy(b.rick.data(), wavelet, (size_t)b.ns * nt * sizeof(float),
+                            cudaMemcpyDeviceToHost));
+  }
+  std::vector<float> w(std::max(p.nb, 1));
+  // abc_cal (wave_abc.c:141-143): float product, double exp, stored as float
+  for (int ib = 0; ib < p.nb; ib++)
+    w[ib] = (float)exp(-a->ct * a->ct * (p.nb - 1 - ib) * (p.nb - 1 - ib));
+  taper_axis(g.nz, p.nz2, p.nb, w, b.wz);
+  taper_axis(g.ny, p.nx2, p.nb, w, b.wy);
+  b.nvel = (size_t)p.nz1 * p.nx1;
+  b.nrec = (size_t)p.nx1;
+  b.nfield = (size_t)g.sy * g.py + 64;
+  b.o_vv = cv.add(b.nfield * 4);
+  b.o_A = cv.add(b.nfield * 4);
+  b.o_B = cv.add(b.nfield * 4);
+  b.o_t = cv.add((b.wz.size() + 1 + b.wy.size()) * 4);
+  b.o_rick = cv.add(b.rick.size() * 4 + 4);
+  b.o_vel = cv.add(host ? b.nvel * 4 : 0);
+  b.o_rec = cv.add((size_t)nt * b.nrec * 4);
+  b.o_dat = cv.add(host ? (size_t)nt * b.nrec * 4 : 0);
+  b.o_mx = cv.add(16);
+  return PW_OK;
+}
+
+// run()'s step arguments for one forward 2-D shot (tile fields set later)
+static void batch_args(const pw_afd_args *a, const BatchShot &b, char *base, StepArgs &s) {
+  const Plan &p = b.p;
+  memset(&s, 0, sizeof s);
+  s.g = p.g;
+  s.ngroups = 1;
+  const float c0 = -30. / 12., c1 = +16. / 12., c2 = -1. / 12.;  // wave_fdm.c:15
+  s.c0 = c0;
+  s.c1 = c1;
+  s.c2 = c2;
+  const float idz = 1 / (a->dz * a->dz), idx = 1 / (a->dx * a->dx);
+  s.idz = idz;
+  s.idy = idx;  // the model's x is the marched axis
+  s.idx = 0.f;
+  s.k0 = idx + idz;
+  s.cur[0] = at<float>(base, b.o_A);
+  s.nxt[0] = at<float>(base, b.o_B);
+  s.vv = at<float>(base, b.o_vv);
+  float *tb = at<float>(base, b.o_t);
+  s.wz = tb;
+  s.wx = tb + b.wz.size();
+  s.wy = tb + b.wz.size() + 1;
+  s.nt = a->nt;
+  s.ns = b.ns;
+  for (int i = 0; i < b.ns; i++) {
+    s.sz[i] = b.ksz[i];
+    s.sx[i] = 0;
+    s.sy[i] = b.ksy[i];
+  }
+  s.rick = at<float>(base, b.o_rick);
+  s.rz = p.nb + a->gz;
+  s.rx0 = 0;
+  s.nrx = 1;
+  s.ry0 = p.nb;
+  s.nry = p.nx1;
+  s.rec = at<float>(base, b.o_rec);
+  s.nbz = p.kbz;
+  s.nbx = p.kbx;
+  s.nby = p.kby;
+  s.nz1 = p.knz1;
+  s.nx1 = p.knx1;
+  s.ny1 = p.kny1;
+  s.S = p.g.lz / 4;
+  s.KX = 1;
+}
+
+// A batch tile: WPC warps per z chunk (ZS = 32 * WPC slots), ych planes.
+struct BatchTile {
+  int wpc, ych;
+};
+
+// Sets the tile fields of every shot and builds the (shot, tile) items in
+// decreasing shot length; cum[k] = items of the k longest shots.
+static void batch_items(const BatchTile &t, const std::vector<int> &order,
+                        std::vector<StepArgs> &args, std::vector<int2> &items,
+                        std::vector<int> &cum) {
+  items.clear();
+  cum.assign(1, 0);
+  for (int k : order) {
+    StepArgs &s = args[k];
+    s.WPC = t.wpc;
+    s.ZS = 32 * t.wpc;
+    s.nzc = ceil_div(s.S, s.ZS);
+    s.ych = std::min(t.ych, s.g.ny);
+    const int tiles = s.nzc * ceil_div(s.g.ny, s.ych);
+    for (int i = 0; i < tiles; i++) items.push_back(make_int2(k, i));
+    cum.push_back((int)items.size());
+  }
+}
+
+static int run_batch(int nshot, const pw_afd_args *args, const float *const *vel,
+                     const float *const *src, const float *const *wavelet, float *const *dat,
+                     cudaStream_t st) {
+  PW_CHECK(nshot >= 1 && nshot <= 65536, PW_ERR_SHAPE, "nshot must be in [1,65536] (got %d)",
+           nshot);
+  PW_CHECK(args && vel && src && dat, PW_ERR_VALUE, "null argument array");
+  const bool host = (args[0].flags & PW_HOST_PTRS) != 0;
+  std::vector<BatchShot> shots(nshot);
+  Carve cv;
+  int ntmax = 0;
+  for (int k = 0; k < nshot; k++) {
+    PW_CHECK(((args[k].flags & PW_HOST_PTRS) != 0) == host, PW_ERR_VALUE,
+             "shot %d: every shot must use the same PW_HOST_PTRS flag", k);
+    PW_CHECK(vel[k] && dat[k], PW_ERR_VALUE, "shot %d: velocity or trace pointer is null", k);
+    const int rc = batch_setup(&args[k], src[k], wavelet ? wavelet[k] : nullptr, host, cv, shots[k]);
+    if (rc != PW_OK) {
+      set_error("shot %d: %s", k, std::string(pw_last_error()).c_str());
+      return rc;
+    }
+    ntmax = std::max(ntmax, args[k].nt);
+  }
+  const size_t o_args = cv.add((size_t)nshot * sizeof(StepArgs));
+  size_t max_items = 0;
+  const BatchTile cands[] = {{1, 16}, {1, 32}, {2, 32}, {2, 64}, {4, 32}, {4, 64}};
+  const int ncand = (int)(sizeof cands / sizeof cands[0]);
+  for (const BatchTile &t : cands) {
+    size_t n = 0;
+    for (int k = 0; k < nshot; k++) {
+      const Geo &g = shots[k].p.g;
+      n += (size_t)ceil_div(g.lz / 4, 32 * t.wpc) * ceil_div(g.ny, std::min(t.ych, g.ny));
+    }
+    max_items = std::max(max_items, n);
+  }
+  PW_CHECK(max_items < (1u << 31), PW_ERR_SHAPE, "too many tiles");
+  const size_t o_items = cv.add(max_items * sizeof(int2));
+
+  Workspace &ws = Workspace::for_current_device();
+  std::lock_guard<std::mutex> lock(ws.mutex());
+  PW_TRY(ws.reserve(cv.total()));
+  char *base = ws.base();
+  PW_CUDA(cudaMemsetAsync(base, 0, cv.total(), st));
+  std::vector<StepArgs> sargs(nshot);
+  for (int k = 0; k < nshot; k++) {
+    const BatchShot &b = shots[k];
+    const pw_afd_args *a = &args[k];
+    const Plan &p = b.p;
+    const float *d_vel = vel[k];
+    if (host) {
+      PW_TRY(to_device(at<float>(base, b.o_vel), vel[k], b.nvel * 4, true, st));
+      d_vel = at<float>(base, b.o_vel);
+    }
+    const int rc = check_velocity(a, d_vel, b.nvel, at<unsigned int>(base, b.o_mx), st);
+    if (rc != PW_OK) {
+      set_error("shot %d: %s", k, std::string(pw_last_error()).c_str());
+      return rc;
+    }
+    std::vector<float> tab(b.wz);
+    tab.push_back(1.f);
+    tab.insert(tab.end(), b.wy.begin(), b.wy.end());
+    PW_CUDA(cudaMemcpyAsync(at<float>(base, b.o_t), tab.data(), tab.size() * 4,
+                            cudaMemcpyHostToDevice, st));
+    if (b.ns > 0)
+      PW_CUDA(cudaMemcpyAsync(at<float>(base, b.o_rick), b.rick.data(),
+                              (size_t)b.ns * a->nt * 4, cudaMemcpyHostToDevice, st));
+    expand_vv_kernel<<<1184, 256, 0, st>>>(p.g, d_vel, p.knz1, p.knx1, p.kny1, p.kbz, p.kbx,
+                                           p.kby, a->dt, at<float>(base, b.o_vv));
+    PW_CUDA(cudaGetLastError());
+    batch_args(a, b, base, sargs[k]);
+    PW_CUDA(cudaStreamSynchronize(st));  // tab and rick are host temporaries
+  }
+  // longest shots first: the launch at step it covers a prefix of the items
+  std::vector<int> order(nshot);
+  for (int k = 0; k < nshot; k++) order[k] = k;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return args[x].nt > args[y].nt; });
+  std::vector<int> nt_sorted(nshot);
+  for (int k = 0; k < nshot; k++) nt_sorted[k] = args[order[k]].nt;
+  StepArgs *d_args = at<StepArgs>(base, o_args);
+  int2 *d_items = at<int2>(base, o_items);
+  std::vector<int2> items;
+  std::vector<int> cum;
+  {
+    static bool attr = [] {
+      cudaFuncSetAttribute((const void *)batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           3 * MARCH_NS * MARCH_MAXT * (int)sizeof(float4));
+      return true;
+    }();
+    (void)attr;
+  }
+  auto use_tile = [&](const BatchTile &t) -> int {
+    batch_items(t, order, sargs, items, cum);
+    PW_CUDA(cudaMemcpyAsync(d_args, sargs.data(), sargs.size() * sizeof(StepArgs),
+                            cudaMemcpyHostToDevice, st));
+    PW_CUDA(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(int2),
+                            cudaMemcpyHostToDevice, st));
+    PW_CUDA(cudaStreamSynchronize(st));  // host vectors are reused
+    return PW_OK;
+  };
+  int tile_threads = 32;
+  size_t tile_smem = 0;
+  // running shots at step it: the first n with nt_sorted[n - 1] > it
+  int running = nshot;
+  auto step = [&](int it) -> int {
+    while (running > 0 && nt_sorted[running - 1] <= it) running--;
+    const int n = cum[running];
+    if (n == 0) return PW_OK;
+    batch_kernel<<<n, tile_threads, tile_smem, st>>>(d_args, d_items, it);
+    PW_CUDA(cudaGetLastError());
+    return PW_OK;
+  };
+
+  // Online tile tuning on the first real steps: every tile computes the same
+  // values, so each candidate simply takes two steps, timed by events; the
+  // fastest runs the rest.  Short runs keep the first candidate.
+  const int tune_steps = 2;
+  int best = 0;
+  int it = 0;
+  LoopTimer timer(st);
+  timer.start();
+  long long launches = 0;
+  if (ntmax >= 8 * ncand * tune_steps) {
+    float best_ms = 1e30f;
+    cudaEvent_t e0, e1;
+    PW_CUDA(cudaEventCreate(&e0));
+    PW_CUDA(cudaEventCreate(&e1));
+    int rc = PW_OK;
+    for (int c = 0; c < ncand && rc == PW_OK; c++) {
+      rc = use_tile(cands[c]);
+      if (rc != PW_OK) break;
+      tile_threads = 32 * cands[c].wpc;
+      tile_smem = (size_t)3 * MARCH_NS * tile_threads * sizeof(float4);
+      cudaEventRecord(e0, st);
+      for (int j = 0; j < tune_steps && rc == PW_OK; j++, it++, launches++) rc = step(it);
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      // per cell-update (later steps may have fewer running shots)
+      double cells = 0;
+      for (int k = 0; k < nshot; k++)
+        if (args[k].nt > it - tune_steps) cells += (double)shots[k].p.g.nz * shots[k].p.g.ny;
+      const float norm = cells > 0 ? (float)(ms / cells) : ms;
+      if (norm < best_ms) {
+        best_ms = norm;
+        best = c;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    PW_TRY(rc);
+  }
+  PW_TRY(use_tile(cands[best]));
+  tile_threads = 32 * cands[best].wpc;
+  tile_smem = (size_t)3 * MARCH_NS * tile_threads * sizeof(float4);
+  if (getenv("PW_AFD_VERBOSE"))
+    fprintf(stderr, "afd batch: %d shots, tile wpc=%d ych=%d, %zu items\n", nshot,
+            cands[best].wpc, cands[best].ych, items.size());
+  // the remaining steps replay as one CUDA graph (direct launches on the
+  // legacy default stream, which cannot be captured)
+  bool graphed = false;
+  if (st != nullptr && it < ntmax) {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      int rc = PW_OK;
+      const int it0 = it;
+      const int running0 = running;
+      for (int j = it0; j < ntmax && rc == PW_OK; j++) rc = step(j);
+      const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+      if (rc == PW_OK && ec == cudaSuccess &&
+          cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess &&
+          cudaGraphLaunch(exec, st) == cudaSuccess) {
+        graphed = true;
+        launches += ntmax - it0;
+        it = ntmax;
+      } else {
+        running = running0;
+      }
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+    } else {
+      cudaGetLastError();
+    }
+  }
+  if (!graphed)
+    for (; it < ntmax; it++, launches++) PW_TRY(step(it));
+  timer.stop();
+
+  // traces [nt][nrec] -> [nrec][nt] per shot
+  for (int k = 0; k < nshot; k++) {
+    const BatchShot &b = shots[k];
+    const int nt = args[k].nt;
+    float *out = host ? at<float>(base, b.o_dat) : dat[k];
+    dim3 tb2(32, 8), tg(ceil_div((long long)b.nrec, 32), ceil_div(nt, 32));
+    transpose_kernel<<<tg, tb2, 0, st>>>(at<float>(base, b.o_rec), out, nt, (long long)b.nrec);
+    PW_CUDA(cudaGetLastError());
+    if (host) PW_TRY(to_host(dat[k], out, (size_t)nt * b.nrec * 4, true, st));
+  }
+  PW_CUDA(cudaStreamSynchronize(st));
+  timer.finish(launches, launches + 2LL * nshot);
+  return PW_OK;
+}
+
 }  // namespace afd
 }  // namespace pw
 
@@ -1392,6 +1780,12 @@ extern "C" int pw_afd(const pw_afd_args *a, const float *vel, const float *src,
                       const float *wavelet, float *dat, float *wfd, void *stream) {
   return pw::afd::run(a, 1, nullptr, vel, src, wavelet, dat, wfd, nullptr, 0,
                       (cudaStream_t)stream);
+}
+
+extern "C" int pw_afd_batch(int nshot, const pw_afd_args *args, const float *const *vel,
+                            const float *const *src, const float *const *wavelet,
+                            float *const *dat, void *stream) {
+  return pw::afd::run_batch(nshot, args, vel, src, wavelet, dat, (cudaStream_t)stream);
 }
 
 extern "C" int pw_tri_image(const pw_afd_args *a, int ngroups, const int *group,
