@@ -45,8 +45,9 @@ def parse():
     p.add_argument("--groups", type=int, default=4)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="tri3d", choices=["tri3d", "fwi2d"],
-                   help="tri3d: the 3-D TRI image (default); fwi2d: 2-D FWI gradients/s")
+    p.add_argument("--workload", default="tri3d", choices=["tri3d", "fwi2d", "batch2d"],
+                   help="tri3d: the 3-D TRI image (default); fwi2d: 2-D FWI gradients/s; "
+                        "batch2d: uneven 2-D forward shots in one batch")
     p.add_argument("--shots", type=int, default=32, help="fwi2d: shots per gradient")
     p.add_argument("--fwi-nt", type=int, default=2000, help="fwi2d: time samples")
     return p.parse_args()
@@ -146,14 +147,25 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def pool_map(fn, arglist, timeout_s=600):
+    """fn(*args) for each args in independent spawned processes, bounded in
+    time: a worker that dies or stalls raises instead of hanging the run."""
+    import multiprocessing as mp
+    pool = mp.get_context("spawn").Pool(len(arglist))
+    try:
+        res = pool.starmap_async(fn, arglist).get(timeout=timeout_s)
+        pool.close()
+        return res
+    finally:
+        pool.terminate()
+        pool.join()
+
+
 def reference_sample(n, nt_s, seed, workers):
     """The reference's own afd3dc (compiled from its sources into oracle/_ref;
     the oracle port when that is absent), time-reversing one receiver group
     for nt_s steps on the full grid, in `workers` independent processes."""
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(workers) as pool:
-        res = pool.starmap(_ref_worker, [(n, nt_s, seed + w) for w in range(workers)])
+    res = pool_map(_ref_worker, [(n, nt_s, seed + w) for w in range(workers)])
     wall = max(r[0] for r in res)
     kind = res[0][1]
     pts = (n + 2 * NBT) ** 3 * nt_s * workers
@@ -297,9 +309,7 @@ def _fwi_ref_worker(nt_s, seed):
 
 
 def _fwi_ref_worker_spawned(nt_s):
-    import multiprocessing as mp
-    with mp.get_context("spawn").Pool(1) as pool:
-        return pool.apply(_fwi_ref_worker, (nt_s, 7))
+    return pool_map(_fwi_ref_worker, [(nt_s, 7)])[0]
 
 
 def run_fwi2d(args, world, rank, local):
@@ -308,14 +318,12 @@ def run_fwi2d(args, world, rank, local):
     if args.impl == "reference":
         if rank != 0:
             return
-        import multiprocessing as mp
         nt_s, workers = 200, max(1, min(os.cpu_count() or 1, 16))
         rates = []
-        with mp.get_context("spawn").Pool(workers) as pool:
-            for i in range(args.warmup + args.steps):
-                walls = pool.starmap(_fwi_ref_worker, [(nt_s, 7)] * workers)
-                if i >= args.warmup:
-                    rates.append(workers / max(walls) * nt_s / (ns * nt))
+        for i in range(args.warmup + args.steps):
+            walls = pool_map(_fwi_ref_worker, [(nt_s, 7)] * workers)
+            if i >= args.warmup:
+                rates.append(workers / max(walls) * nt_s / (ns * nt))
         value = statistics.median(rates)
         print(json.dumps({
             "impl": "reference", "metric": f"FWI gradients/s (2-D, {ns} shots)", "value": value,
@@ -452,6 +460,228 @@ def run_fwi2d(args, world, rank, local):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------------------
+# batch2d: uneven 2-D forward shots in one lockstep time loop
+# --------------------------------------------------------------------------
+B2_NSHOT, B2_H, B2_DT, B2_NBT = 64, 10.0, 0.001, 30
+
+
+def batch2d_shots(seed, nshot=B2_NSHOT, scale=1.0):
+    """Seeded shots: grids (nz, nx) in [256,1024] x [256,2048] (times
+    `scale`), nt in [1000, 4000], layered velocity plus a smooth anomaly in
+    [1500, 4500] m/s, one Ricker source of 10-30 Hz near the surface."""
+    rng = np.random.default_rng(seed)
+    shots = []
+    for _ in range(nshot):
+        nz = max(16, int(rng.integers(256, 1025) * scale))
+        nx = max(16, int(rng.integers(256, 2049) * scale))
+        nt = int(rng.integers(1000, 4001))
+        z = np.arange(nz)[:, None]
+        x = np.arange(nx)[None, :]
+        nl = int(rng.integers(3, 8))
+        ifaces = np.sort(rng.integers(1, nz, nl))
+        vals = np.sort(rng.uniform(1500, 4000, nl + 1))
+        v = np.full((nz, nx), vals[0])
+        for val, zi in zip(vals[1:], ifaces):
+            v = np.where(z >= zi, val, v)
+        cz, cx, r = rng.uniform(0.3, 0.7) * nz, rng.uniform(0.2, 0.8) * nx, 0.1 * min(nz, nx)
+        v = v * (1 + 0.1 * np.exp(-((z - cz) ** 2 + (x - cx) ** 2) / (2 * r * r)))
+        v = np.clip(v, 1500, 4500).astype(np.float32)
+        f0 = float(rng.uniform(10, 30))
+        shots.append(dict(vel=v, nt=nt, dt=B2_DT, ax=[0, B2_H, nx], az=[0, B2_H, nz], ns=1,
+                          sx=[int(rng.integers(nx // 4, 3 * nx // 4))], sz=[5], f=[f0],
+                          t=[1.2 / f0], A=[1.0], nbt=B2_NBT, ct=0.01, gz=5))
+    return shots
+
+
+def _b2_cells(sh):
+    return (sh["az"][2] + 2 * B2_NBT) * (sh["ax"][2] + 2 * B2_NBT) * sh["nt"]
+
+
+B2_CROP = 400  # the reference's afd2dc corrupts its heap on the largest shots
+
+
+def _b2_ref_worker(nt_s, seed, kind="reference"):
+    """The reference's afd2dc (oracle/_ref; kind "port": the oracle's C
+    restatement) on a B2_CROP^2 crop of the largest seeded shot for nt_s
+    steps; returns (cell-updates, wall seconds)."""
+    sys.path.insert(0, ROOT)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    sh = max(batch2d_shots(seed), key=lambda s: s["az"][2] * s["ax"][2])
+    vel = np.ascontiguousarray(sh["vel"][:B2_CROP, :B2_CROP])
+    nz, nx = vel.shape
+    src = dict(sx=[nx // 2], sz=sh["sz"], f=sh["f"], t=sh["t"], A=sh["A"])
+    t0 = time.perf_counter()
+    if kind == "reference":
+        sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+        import afdcfun  # the reference's own extension module
+        s = np.array(src["sx"] + src["sz"] + src["f"] + src["t"] + src["A"], np.float32)
+        afdcfun.afd2dc(vel.flatten(order="F"), s, 0, nt_s, nx, nz, 1, 0, nt_s, 0, 1, B2_NBT,
+                       0.01, B2_DT, 0.0, B2_H, 0.0, B2_H)
+    else:
+        from oracle import oracle as O
+        O.afd(vel, nt_s, B2_DT, (B2_H, B2_H), nbt=B2_NBT, ct=0.01, src=src)
+    wall = time.perf_counter() - t0
+    return (nz + 2 * B2_NBT) * (nx + 2 * B2_NBT) * nt_s, wall
+
+
+def _b2_cpu_sample(workers, nt_s=100):
+    """(Gpt/s, kind) of the CPU path on `workers` processes: the reference,
+    or the oracle port when the reference's run fails."""
+    for kind in ("reference", "port"):
+        try:
+            res = pool_map(_b2_ref_worker, [(nt_s, 5, kind)] * workers, timeout_s=300)
+            return sum(r[0] for r in res) / max(r[1] for r in res) / 1e9, kind
+        except Exception:  # noqa: BLE001
+            continue
+    raise RuntimeError("neither the reference nor the port ran")
+
+
+def run_batch2d(args, world, rank, local):
+    shots = batch2d_shots(5 + rank)
+    cells = sum(_b2_cells(sh) for sh in shots)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        workers = max(1, min(os.cpu_count() or 1, 16))
+        rates = []
+        for i in range(args.warmup + args.steps):
+            v, kind = _b2_cpu_sample(workers)
+            if i >= args.warmup:
+                rates.append(v)
+        value = statistics.median(rates)
+        print(json.dumps({
+            "impl": "reference", "metric": "Gpt-updates/s (2-D uneven shot batch)",
+            "value": value, "unit": "Gpt/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{len(shots)} 2-D shots, grids 256-1024 x 256-2048, "
+                                   f"nt 1000-4000, h=10m, nbt={B2_NBT}"},
+            "cpu_baseline": {"value": value, "unit": "Gpt/s", "cores": workers, "kind": kind,
+                             "sample": f"afd2dc on a {B2_CROP}^2 crop of the largest shot, 100 "
+                                       f"steps, {workers} independent single-threaded processes"},
+            "e2e": {"value": value, "unit": "Gpt/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+    from pywave_b200 import _lib as L
+    from pywave_b200 import build as B
+    from pywave_b200.afd import afd2d_batch
+    B.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lib = L.lib()
+    n = len(shots)
+    a = (L.AfdArgs * n)()
+    keep, vp, sp, dp = [], [], [], []
+    for k, sh in enumerate(shots):
+        nz, nx = sh["az"][2], sh["ax"][2]
+        x = a[k]
+        x.dim, x.nz, x.nx, x.ny, x.nt, x.nbt, x.ct = 2, nz, nx, 1, sh["nt"], B2_NBT, 0.01
+        x.dt, x.dz, x.dx, x.dy, x.ns, x.tri, x.jsnap, x.gz, x.flags = (
+            B2_DT, B2_H, B2_H, B2_H, 1, 0, 0, sh["gz"], 0)
+        v = torch.from_numpy(np.ascontiguousarray(sh["vel"].flatten(order="F"))).cuda()
+        s = torch.tensor(sh["sx"] + sh["sz"] + sh["f"] + sh["t"] + sh["A"], dtype=torch.float32,
+                         device="cuda")
+        d = torch.empty(sh["nt"] * nx, device="cuda")
+        keep += [v, s, d]
+        vp.append(v.data_ptr())
+        sp.append(s.data_ptr())
+        dp.append(d.data_ptr())
+    VP, SP, DP = ((C.c_void_p * n)(*q) for q in (vp, sp, dp))
+    side = torch.cuda.Stream()
+
+    def batch():
+        L.check(lib.pw_afd_batch(n, C.cast(a, C.c_void_p), C.cast(VP, C.c_void_p),
+                                 C.cast(SP, C.c_void_p), None, C.cast(DP, C.c_void_p),
+                                 side.cuda_stream))
+        return L.last_timing()
+
+    def plain():
+        for k in range(n):
+            L.check(lib.pw_afd(C.byref(a[k]), vp[k], sp[k], None, dp[k], None, side.cuda_stream))
+
+    with torch.cuda.stream(side):
+        for _ in range(args.warmup):
+            batch()
+        clk = Clocks(local)
+        clk.start()
+        if world > 1:
+            dist.barrier()
+        side.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        loops, launches = [], 0
+        e0.record(side)
+        for _ in range(args.steps):
+            ms, nst, tot = batch()
+            loops.append(ms)
+            launches += tot
+        e1.record(side)
+        side.synchronize()
+        clocks = clk.stop()
+        ms_b = max_over_ranks(e0.elapsed_time(e1), world)
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(side)
+        plain()
+        p1.record(side)
+        side.synchronize()
+        ms_p = max_over_ranks(p0.elapsed_time(p1), world)
+    value = job_rate(cells, args.steps, world, ms_b) / 1e9
+    plain_v = job_rate(cells, 1, world, ms_p) / 1e9
+    e2e = None
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            afd2d_batch(shots, stream=side.cuda_stream)
+        side.synchronize()
+        ems = max_over_ranks((time.perf_counter() - t0) * 1e3, world)
+        e2e = {"value": job_rate(cells, args.steps, world, ems) / 1e9, "unit": "Gpt/s",
+               "h2d_bytes_per_step": int(sum(sh["vel"].nbytes + 20 for sh in shots)),
+               "d2h_bytes_per_step": int(sum(sh["nt"] * sh["ax"][2] * 4 for sh in shots))}
+    peak, peak_kind = peaks()
+    loop_ms = statistics.median(loops)
+    achieved = cells * 16 / (loop_ms / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, kind = _b2_cpu_sample(1)
+            cpu = {"value": v, "unit": "Gpt/s", "cores": 1, "kind": kind,
+                   "sample": f"afd2dc on a {B2_CROP}^2 crop of the largest shot, 100 steps, "
+                             f"1 core"}
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "unit": "Gpt/s", "cores": 1, "kind": "reference",
+                   "sample": f"failed: {ex!r}"[:200]}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Gpt-updates/s (2-D uneven shot batch)", "value": value, "unit": "Gpt/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded layered models, Ricker sources)",
+            "config": {"workload": f"{n} 2-D shots, grids 256-1024 x 256-2048, nt 1000-4000, "
+                                   f"h=10m dt=1ms nbt={B2_NBT}, one lockstep batch",
+                       "cell_updates_per_step": cells,
+                       "l2": "inputs larger than L2 (fields of all shots)"},
+            "plain_per_shot": {"value": plain_v, "unit": "Gpt/s",
+                               "note": "pw_afd one shot after another"},
+            "batched_over_plain": value / plain_v,
+            "e2e": e2e, "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "batch_kernel (2-D march, all running shots)",
+                         "loop_ms": loop_ms, "alg_bytes_per_step": cells * 16,
+                         "peak_source": peak_kind},
+            "cpu_baseline": cpu, "clocks": clocks}), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -459,6 +689,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "fwi2d":
         return run_fwi2d(args, world, rank, local)
+    if args.workload == "batch2d":
+        return run_batch2d(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, rank)
 

@@ -1,10 +1,12 @@
 // Status, workspace and host-side helpers of libpywave_b200.
 #include "pw_common.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <map>
 #include <memory>
+#include <thread>
 
 namespace pw {
 
@@ -86,18 +88,40 @@ void ricker_table(int nt, float dt, float f0, float t0, float A, float *out) {
     shape[k] = (double)(w * expf(1 - w) / nfft);
   }
   for (int j = 0; j < nfft; j++) ctab[j] = std::cos(2.0 * M_PI * (double)j / (double)nfft);
-  for (int n = 0; n < nt; n++) {
-    const long m = n - k0;
-    double s = shape[0];
-    for (int k = 1; k < nfft / 2; k++) {
-      long ph = ((long)k * m) % nfft;
-      if (ph < 0) ph += nfft;
-      s += 2.0 * shape[k] * ctab[ph];
+  std::vector<double> two_shape(nw);
+  for (int k = 0; k < nw; k++) two_shape[k] = 2.0 * shape[k];  // exact
+  // samples are independent: split them over host threads; the phase k*m
+  // mod nfft advances by m mod nfft per term (same terms, same order)
+  auto rows = [&](int n0, int n1) {
+    for (int n = n0; n < n1; n++) {
+      const long m = n - k0;
+      const long mm = ((m % nfft) + nfft) % nfft;
+      double s = shape[0];
+      long ph = 0;
+      for (int k = 1; k < nfft / 2; k++) {
+        ph += mm;
+        if (ph >= nfft) ph -= nfft;
+        s += two_shape[k] * ctab[ph];
+      }
+      long ph2 = ((long)(nfft / 2) * m) % nfft;
+      if (ph2 < 0) ph2 += nfft;
+      s += shape[nfft / 2] * ctab[ph2];
+      out[n] = (float)((double)A * s);
     }
-    long ph = ((long)(nfft / 2) * m) % nfft;
-    if (ph < 0) ph += nfft;
-    s += shape[nfft / 2] * ctab[ph];
-    out[n] = (float)((double)A * s);
+  };
+  const long long work = (long long)nt * nfft;
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nthr = (int)std::min<long long>(std::min(hw, 32), std::max(1LL, work >> 22));
+  if (nthr <= 1) {
+    rows(0, nt);
+  } else {
+    std::vector<std::thread> th;
+    const int chunk = (nt + nthr - 1) / nthr;
+    for (int i = 0; i < nthr; i++) {
+      const int n0 = i * chunk, n1 = std::min(nt, n0 + chunk);
+      if (n0 < n1) th.emplace_back(rows, n0, n1);
+    }
+    for (auto &t : th) t.join();
   }
 }
 
