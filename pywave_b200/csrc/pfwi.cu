@@ -14,6 +14,9 @@
 #include "pw_common.cuh"
 
 #include <algorithm>
+#include <cfloat>
+#include <map>
+#include <mutex>
 #include <cmath>
 
 namespace pw {
@@ -35,12 +38,36 @@ struct ShotGeo {
 
 enum Mode { FWD = 0, ADJ_REF = 1, ADJ_EXACT = 2 };
 
+// Division by a constant d > 0 with the method of Brisebarre, Muller and
+// Raina ("Accelerating correctly rounded floating-point division when the
+// divisor is known in advance", IEEE Trans. Computers 53(8), 2004):
+//   zh = RN(1/d), zl = RN(1/d - zh),  q = RN(x*zh + RN(x*zl))  (one FMA).
+// It returns the correctly rounded x/d for every x only for some d, so each
+// divisor is checked on the GPU against __fdiv_rn for all 2^23 significands
+// of x in one binade; scaling x by 2^k scales every step exactly while the
+// intermediate values stay normal, which |x| in [xmin, xmax] ensures.
+// Below xmin (the tiny values at the edge of a wavefield, subnormal ones
+// included) div_small scales x by 2^89 into that range, divides, and scales
+// back, which is exact unless the quotient is subnormal and the scaled
+// quotient sits exactly on a tie of the subnormal grid; there the sign of
+// the exact remainder xs - qs*d (one FMA) picks the side.  The setup checks
+// it against __fdiv_rn for every float in (0, xmin) as well.
+// Above xmax, for NaN or infinity, or when a check fails: __fdiv_rn.
+struct DivC {
+  float d, zh, zl, xmin, xmax;
+  int ok;
+  unsigned int umin, uspan, umax;  // bits of xmin; of xmax minus xmin; of xmax
+  float sup, sdn, sgrid;           // 2^K, 2^-K, 2^(149-K) for div_small
+};
+constexpr int DIV_SMALL_K = 89;
+
 struct PfArgs {
   int pnz, pnx;               // padded grid
   int lz;                     // leading dimension of the field layout
   int nb, nz, nx;             // sponge width, interior
   float c0, c1, c2, c3, c4;   // 8th-order coefficients (wave_fwiutil.c:17)
   float dx2, dz2;
+  DivC divx, divz;            // fast exact division by dx2 / dz2
   int nshots;
   const float *cur[MAXS];
   float *nxt[MAXS];
@@ -97,6 +124,69 @@ __device__ __forceinline__ float znb(const float4 &L, const float4 &c, const flo
   if (j < 0) return el(L, j + 4);
   if (j > 3) return el(R, j - 4);
   return el(c, j);
+}
+
+__device__ __forceinline__ float div_bmr(float x, const DivC &c) {
+  // copysignf keeps the sign of a zero quotient (d > 0)
+  return copysignf(__fmaf_rn(x, c.zh, __fmul_rn(x, c.zl)), x);
+}
+
+__device__ __forceinline__ float div_small(float x, const DivC &c) {
+  const float xs = __fmul_rn(x, c.sup);  // exact, inside [xmin, xmax]
+  const float qs = __fmaf_rn(xs, c.zh, __fmul_rn(xs, c.zl));
+  const float q = copysignf(__fmul_rn(qs, c.sdn), x);
+  const float t = fabsf(__fmul_rn(qs, c.sgrid));  // |qs| in units of 2^-149 (exact)
+  const float n = truncf(t);
+  if (t - n == 0.5f) {
+    const float r = __fmaf_rn(-qs, c.d, xs);  // exact remainder
+    if (r != 0.f)
+      return __uint_as_float((__float2uint_rz(n) + ((r > 0.f) == (x > 0.f) ? 1u : 0u)) |
+                             (__float_as_uint(x) & 0x80000000u));
+  }
+  return q;
+}
+
+// tx[e]/cx.d and tz[e]/cz.d for the 4 cells of a float4, correctly rounded.
+// The lanes of `mask` vote once: every numerator zero or in [xmin, xmax]
+// runs div_bmr; every one below xmax runs div_small or div_bmr per value;
+// otherwise __fdiv_rn (a per-value choice of all three would be if-converted
+// into every sequence).  Any grouping of lanes is correct, as every lane's
+// own vote is in its group.
+__device__ __forceinline__ void div4x2(const float (&tx)[4], const float (&tz)[4],
+                                       const DivC &cx, const DivC &cz, unsigned mask,
+                                       float (&qx)[4], float (&qz)[4]) {
+  // |x| in [xmin, xmax] is one unsigned compare on the bits of |x| (positive
+  // floats order as their bit patterns); bits 0 (x = +-0) are in range too
+  const bool ok = cx.ok && cz.ok;
+  bool in = ok, below = ok;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const unsigned int ux = __float_as_uint(tx[e]) & 0x7fffffffu;
+    const unsigned int uz = __float_as_uint(tz[e]) & 0x7fffffffu;
+    in = in && (ux - cx.umin <= cx.uspan || ux == 0u) && (uz - cz.umin <= cz.uspan || uz == 0u);
+    below = below && ux <= cx.umax && uz <= cz.umax;
+  }
+  if (__all_sync(mask, in)) {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      qx[e] = div_bmr(tx[e], cx);
+      qz[e] = div_bmr(tz[e], cz);
+    }
+  } else if (__all_sync(mask, below)) {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const bool sx = (__float_as_uint(tx[e]) & 0x7fffffffu) < cx.umin;
+      const bool sz = (__float_as_uint(tz[e]) & 0x7fffffffu) < cz.umin;
+      qx[e] = sx ? div_small(tx[e], cx) : div_bmr(tx[e], cx);
+      qz[e] = sz ? div_small(tz[e], cz) : div_bmr(tz[e], cz);
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      qx[e] = __fdiv_rn(tx[e], cx.d);
+      qz[e] = __fdiv_rn(tz[e], cz.d);
+    }
+  }
 }
 
 // One pfwi step over a z column segment of ZW float4 marching along x.
@@ -218,9 +308,9 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
           }
         }
         float4 term4, res4;
+        float txs[4], tzs[4], qx[4], qz[4];
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-          const int iz = iz0 + e;
           const float cv = el(c, e);
           float tx = fmul(a.c0, cv);
           tx = fadd(tx, fmul(a.c1, fadd(el(q[5], e), el(q[3], e))));
@@ -232,7 +322,16 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
           tz = fadd(tz, fmul(a.c2, fadd(znb(L, c, R, e, 2), znb(L, c, R, e, -2))));
           tz = fadd(tz, fmul(a.c3, fadd(znb(L, c, R, e, 3), znb(L, c, R, e, -3))));
           tz = fadd(tz, fmul(a.c4, fadd(znb(L, c, R, e, 4), znb(L, c, R, e, -4))));
-          float t = (lz_ok[e] && lx_ok) ? fadd(fdiv(tx, a.dx2), fdiv(tz, a.dz2)) : 0.f;
+          const bool lap = lz_ok[e] && lx_ok;  // skipped cells vote with zeros
+          txs[e] = lap ? tx : 0.f;
+          tzs[e] = lap ? tz : 0.f;
+        }
+        div4x2(txs, tzs, a.divx, a.divz, __activemask(), qx, qz);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int iz = iz0 + e;
+          const float cv = el(c, e);
+          float t = (lz_ok[e] && lx_ok) ? fadd(qx[e], qz[e]) : 0.f;
           if (MODE == FWD) {
             if (src_here)
               for (int k = 0; k < sg.nsrc; k++)
@@ -286,6 +385,7 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
     __syncthreads();
   }
 }
+
 
 // FP64 misfit and residual, one thread per (shot, it, ir):
 //   REFERENCE: r = dobs - d, J += 0.5 r^2 (unweighted), adjoint source r*w
@@ -527,8 +627,106 @@ static int source_map(int sx, int sz, int pnz, int pnx, ShotGeo &sg) {
   return PW_OK;
 }
 
+// Exhaustive check of DivC against __fdiv_rn over the 2^23 significands of
+// x in [scale, 2*scale) (a binade where every intermediate value is normal).
+__device__ unsigned int fastdiv_bad;
+__global__ void fastdiv_check_kernel(float d, float zh, float zl, float scale) {
+  const unsigned int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= (1u << 23)) return;
+  const float x = __fmul_rn(scale, __uint_as_float(0x3f800000u | m));  // exact (power of 2)
+  const float q = __fmaf_rn(x, zh, __fmul_rn(x, zl));
+  if (__float_as_uint(q) != __float_as_uint(__fdiv_rn(x, d))) atomicAdd(&fastdiv_bad, 1u);
+}
+
+// div_small against __fdiv_rn for every float with bits in [1, umin), both signs
+__global__ void smalldiv_check_kernel(DivC c) {
+  const unsigned int stride = gridDim.x * blockDim.x;
+  unsigned int bad = 0;
+  for (unsigned int u = 1 + blockIdx.x * blockDim.x + threadIdx.x; u < c.umin; u += stride) {
+    const float x = __uint_as_float(u), y = -x;
+    bad += __float_as_uint(div_small(x, c)) != __float_as_uint(__fdiv_rn(x, c.d));
+    bad += __float_as_uint(div_small(y, c)) != __float_as_uint(__fdiv_rn(y, c.d));
+  }
+  if (bad) atomicAdd(&fastdiv_bad, bad);
+}
+
+// DivC for d (cached per process: the result depends on d only).
+static int prepare_div(float d, DivC &c) {
+  static std::mutex mu;
+  static std::map<unsigned int, DivC> cache;
+  unsigned int key;
+  memcpy(&key, &d, 4);
+  std::lock_guard<std::mutex> lock(mu);
+  auto hit = cache.find(key);
+  if (hit != cache.end()) {
+    c = hit->second;
+    return PW_OK;
+  }
+  c.d = d;
+  c.ok = 0;
+  c.zh = c.zl = 0.f;
+  c.xmin = 1.f;
+  c.xmax = 0.f;
+  c.umin = c.uspan = c.umax = 0;
+  if (d > 0.f && std::isfinite(d)) {
+    // zh: the float nearest 1/d (float x float products are exact in double,
+    // and 1 - zh*d is exact by Sterbenz's lemma)
+    const float z0 = (float)(1.0 / (double)d);
+    float zh = z0;
+    double err = std::fabs(1.0 - (double)z0 * d);
+    for (float cand : {std::nextafter(z0, 0.f), std::nextafter(z0, INFINITY)}) {
+      const double e = std::fabs(1.0 - (double)cand * d);
+      unsigned int cb;
+      memcpy(&cb, &cand, 4);
+      if (e < err || (e == err && (cb & 1u) == 0)) {
+        zh = cand;
+        err = e;
+      }
+    }
+    const float zl = (float)((1.0 - (double)zh * d) / (double)d);
+    // keep x*zh, x*zl and x/d normal and finite with a factor-4 margin
+    const double fmin = (double)FLT_MIN, fmax = (double)FLT_MAX;
+    double lo = std::max(fmin / zh, fmin * d);
+    if (zl != 0.f) lo = std::max(lo, fmin / std::fabs((double)zl));
+    lo *= 4;
+    const double hi = std::min(fmax / 4 / zh, fmax / 4 * d);
+    if (lo * 4 < hi) {
+      c.zh = zh;
+      c.zl = zl;
+      c.xmin = (float)lo;
+      c.xmax = (float)hi;
+      memcpy(&c.umin, &c.xmin, 4);
+      memcpy(&c.umax, &c.xmax, 4);
+      c.uspan = c.umax - c.umin;
+      c.sup = std::ldexp(1.f, DIV_SMALL_K);
+      c.sdn = std::ldexp(1.f, -DIV_SMALL_K);
+      c.sgrid = std::ldexp(1.f, 149 - DIV_SMALL_K);
+      // x in (0, xmin) scales into [2^(K-149), xmin * 2^K], inside [xmin, xmax]
+      const bool small_ok = lo <= std::ldexp(1.0, DIV_SMALL_K - 149) &&
+                            lo * std::ldexp(1.0, DIV_SMALL_K) <= hi;
+      const double scale = std::ldexp(1.0, (int)std::ceil(std::log2(lo)));
+      unsigned int bad = 0;
+      PW_CUDA(cudaMemcpyToSymbol(fastdiv_bad, &bad, sizeof bad));
+      fastdiv_check_kernel<<<(1u << 23) / 256, 256>>>(d, zh, zl, (float)scale);
+      PW_CUDA(cudaGetLastError());
+      if (small_ok) {
+        smalldiv_check_kernel<<<4 * 148, 256>>>(c);
+        PW_CUDA(cudaGetLastError());
+      }
+      PW_CUDA(cudaMemcpyFromSymbol(&bad, fastdiv_bad, sizeof bad));
+      c.ok = small_ok && bad == 0;
+    }
+  }
+  if (getenv("PW_PFWI_VERBOSE"))
+    fprintf(stderr, "pfwi: division by %.9g: zh %.9g zl %.9g range [%.3g, %.3g] fast %d\n", d,
+            c.zh, c.zl, c.xmin, c.xmax, c.ok);
+  cache[key] = c;
+  return PW_OK;
+}
+
 struct Setup {
   pw_fwi_args a;
+  DivC divx, divz;
   int pnz, pnx, lz;
   long long fstride;  // floats per field (incl. halo)
   int nr, rz, drv, sz;
@@ -550,6 +748,8 @@ static int setup(const pw_fwi_args *a, Setup &S) {
   S.pnx = a->nx + 2 * nb;
   PW_CHECK(S.pnx < 65536 && S.pnz < 65536, PW_ERR_SHAPE, "grid too large");
   S.lz = (int)round_up(HZ + round_up(S.pnz, 4) + 4, 32);
+  PW_TRY(prepare_div(a->dx * a->dx, S.divx));
+  PW_TRY(prepare_div(a->dz * a->dz, S.divz));
   S.fstride = (long long)S.lz * (S.pnx + 2 * HX) + 64;
   // preparation (wave_fwiutil.c:31-71) with pfwi.c's fixed acquisition
   std::vector<float> bc(nb);
@@ -660,6 +860,8 @@ static void base_args(const Setup &S, PfArgs &p) {
   p.c0 = c0; p.c1 = c1; p.c2 = c2; p.c3 = c3; p.c4 = c4;
   p.dx2 = S.a.dx * S.a.dx;
   p.dz2 = S.a.dz * S.a.dz;
+  p.divx = S.divx;
+  p.divz = S.divz;
   p.nt = S.a.nt;
   p.rz = S.rz;
   p.drv = S.drv;
