@@ -200,6 +200,7 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
   float4 *s_prev = sm + NC * W;
   float4 *s_V = s_prev + NP * ZW;
   float4 *s_t = s_V + NP * ZW;  // ADJ_EXACT: forward term tile
+  float4 *s_g = s_t + NP * ZW;  // ADJ_EXACT: this shot's gradient slice
 
   const int tid = threadIdx.x;
   const int s = blockIdx.x;  // shot of the batch: fastest, so the shots of one x chunk
@@ -251,7 +252,10 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
       const long long o = o_c + (long long)lz * (x0 + j);
       cp16(s_prev + (j % NP) * ZW + tid, live ? nxt + o : nxt, live);
       cp16(s_V + (j % NP) * ZW + tid, live ? a.V + o : a.V, live);
-      if (MODE == ADJ_EXACT) cp16(s_t + (j % NP) * ZW + tid, live ? tin + o : tin, live && a.imaging);
+      if (MODE == ADJ_EXACT) {
+        cp16(s_t + (j % NP) * ZW + tid, live ? tin + o : tin, live && a.imaging);
+        cp16(s_g + (j % NP) * ZW + tid, live ? gs + o : gs, live && a.imaging);
+      }
     };
     for (int k = 0; k < 8; k++) issue_cur(k);
 #pragma unroll
@@ -352,7 +356,7 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
         if (MODE == ADJ_EXACT && a.imaging) {
           // dJ/dV accumulates phi_n * term_n (divided by V at the end)
           const float4 tf = s_t[(i % NP) * ZW + tid];
-          float4 gacc = *reinterpret_cast<const float4 *>(gs + o);
+          float4 gacc = s_g[(i % NP) * ZW + tid];  // read P planes ahead (cp.async)
           gacc.x = fadd(gacc.x, fmul(c.x, tf.x));
           gacc.y = fadd(gacc.y, fmul(c.y, tf.y));
           gacc.z = fadd(gacc.z, fmul(c.z, tf.z));
@@ -814,7 +818,7 @@ static int setup(const pw_fwi_args *a, Setup &S) {
 constexpr int PFP = 3;  // prefetch depth (planes)
 
 static size_t smem_for(int zw, int mode) {
-  return sizeof(float4) * ((size_t)(PFP + 10) * (zw + 2) + (size_t)(mode == ADJ_EXACT ? 3 : 2) *
+  return sizeof(float4) * ((size_t)(PFP + 10) * (zw + 2) + (size_t)(mode == ADJ_EXACT ? 4 : 2) *
                                                                (PFP + 2) * zw);
 }
 
@@ -1048,14 +1052,15 @@ extern "C" int pw_pfwi_forward(const pw_fwi_args *a, const float *vel, const flo
   return PW_OK;
 }
 
-// Checkpoint interval of the exact gradient: the segment buffer holds k term
-// fields per shot and the checkpoints two fields every k steps, so
-// k = sqrt(2 nt) minimises their sum; the shot batch shrinks until the whole
-// working set fits the HBM budget (80% of the free memory).
+// Checkpoint interval of the exact gradient.  The segment buffer holds k term
+// fields per shot and the checkpoints two fields every k steps.  The forward
+// pass keeps the terms of the last segment, so the backward pass recomputes
+// nt - k steps: k is the largest interval whose working set fits the HBM
+// budget (80% of the free memory; k = nt recomputes nothing).  When not even
+// k = sqrt(2 nt), the interval of the smallest working set, fits, the shot
+// batch shrinks first.
 static void plan_exact(const Setup &S, int ckpt_k, int &k, int &nsb) {
   const int nt = S.a.nt;
-  k = ckpt_k > 0 ? ckpt_k : std::max(1, (int)std::lround(std::sqrt(2.0 * nt)));
-  k = std::min(k, nt);
   size_t freeb = 0, totb = 0;
   if (cudaMemGetInfo(&freeb, &totb) != cudaSuccess) {
     cudaGetLastError();
@@ -1063,13 +1068,27 @@ static void plan_exact(const Setup &S, int ckpt_k, int &k, int &nsb) {
   }
   const double budget = 0.8 * (double)freeb;
   const double fb = (double)S.fstride * 4;
+  auto need = [&](int kk, int nb) {
+    const int nck = (nt + kk - 1) / kk;
+    return fb * nb * (5.0 + 2.0 * nck + kk) + fb * 2;
+  };
+  const int kmin = std::min(nt, std::max(1, (int)std::lround(std::sqrt(2.0 * nt))));
+  k = ckpt_k > 0 ? std::min(ckpt_k, nt) : kmin;
   nsb = std::min(S.a.ns, MAXS);
-  while (nsb > 1) {
-    const int nck = (nt + k - 1) / k;
-    const double need = fb * nsb * (5.0 + 2.0 * nck + k) + fb * 2;
-    if (need <= budget) break;
-    nsb = (nsb + 1) / 2;
+  while (nsb > 1 && need(k, nsb) > budget) nsb = (nsb + 1) / 2;
+  if (ckpt_k > 0) return;
+  if (need(nt, nsb) <= budget) {
+    k = nt;
+    return;
   }
+  // need() rises with k above kmin: the largest k in [kmin, nt) that fits
+  int lo = kmin, hi = nt;
+  while (hi - lo > 1) {
+    const int mid = lo + (hi - lo) / 2;
+    if (need(mid, nsb) <= budget) lo = mid;
+    else hi = mid;
+  }
+  k = lo;
 }
 
 extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const float *wav,
@@ -1200,8 +1219,10 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
     p.rec = dd;
     p.tout = nullptr;
     p.snap_stride = (long long)wnt * nvel;
+    const int n_last = exact ? (nck - 1) * k : nt;  // first step of the last segment
+    p.tout_stride = (long long)k * fs;
     for (int it = 0; it < nt; it++) {
-      if (exact && it % k == 0) {
+      if (exact && it % k == 0 && it < n_last) {
         const int m = it / k;
         for (int s = 0; s < nb_; s++) {
           float *c = ck + ((size_t)s * nck + m) * 2 * fs;
@@ -1210,10 +1231,13 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
         }
       }
       p.snap = (!exact && it % interval == 0) ? snap + (size_t)(it / interval) * nvel : nullptr;
+      // the last segment's terms, which the backward pass reads first
+      p.tout = it >= n_last ? tb + (size_t)(it - n_last) * fs : nullptr;
       PW_TRY(step(FWD, it));
     }
     p.rec = nullptr;
     p.snap = nullptr;
+    p.tout = nullptr;
     // ---- residual and FP64 misfit
     residual_kernel<<<592, 256, 0, st>>>(dd, at<float>(base, o_dobs) + (size_t)s0 * nt * nr,
                                          at<float>(base, o_w), res, nb_, nt, nr, exact ? 1 : 0, dmis);
@@ -1260,7 +1284,7 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
           FA[s] = ck + ((size_t)s * nck + m) * 2 * fs;
           FB[s] = FA[s] + fs;
         }
-        for (int n = n0; n < n1; n++) {
+        for (int n = n0; n < n1 && m < nck - 1; n++) {  // the last segment is kept
           p.it = n;
           for (int s = 0; s < nb_; s++) {
             p.cur[s] = FA[s];
