@@ -87,7 +87,7 @@ struct PfArgs {
   const float *wprev, *wcur, *wnext;  // snapshots wit-1, wit, wit+1 [shot][nx][nz]
   long long wstride;
   float wdt2;
-  const float *vint;          // interior velocity [nx][nz]
+  const float *m2v3;          // (float)(-2/(double)v^3) per interior cell [nx][nz]
   float *grad;                // [nx][nz] (ADJ_REF) or field layout (ADJ_EXACT: sum phi*term)
   long long gstride;          // floats between the shots' gradient slices (0: one accumulator)
   const float *tin;           // ADJ_EXACT: term of the forward step [shot] (field layout)
@@ -269,6 +269,28 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
     float4 q[9];
     for (int i = 0; i < nplanes; i++) {
       const int x = x0 + i;
+      // ADJ_REF imaging operands of this plane, loaded before the stencil so
+      // their latency hides behind it
+      double rw[4];
+      float rt[4], rg[4];
+      const bool img = MODE == ADJ_REF && a.imaging && live && x >= a.nb && x < a.nb + a.nx;
+      if (MODE == ADJ_REF) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int iz = iz0 + e;
+          rw[e] = 0.;
+          rt[e] = rg[e] = 0.f;
+          if (img && iz >= a.nb && iz < a.nb + a.nz) {
+            const size_t k = (size_t)(x - a.nb) * a.nz + (iz - a.nb);
+            const size_t ks = s * a.wstride + k;
+            // wave[wit+1] - 2.*wave[wit] + wave[wit-1] in double, left to right
+            rw[e] = __dadd_rn(__dsub_rn((double)a.wnext[ks], __dmul_rn(2., (double)a.wcur[ks])),
+                              (double)a.wprev[ks]);
+            rt[e] = a.m2v3[k];
+            rg[e] = gs[k];
+          }
+        }
+      }
       if (i + P < nplanes) {
         issue_cur(i + P + 8);
         issue_pv(i + P);
@@ -363,21 +385,18 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
           gacc.w = fadd(gacc.w, fmul(c.w, tf.w));
           *reinterpret_cast<float4 *>(gs + o) = gacc;
         }
-        if (MODE == ADJ_REF && a.imaging && interior) {
-          // gradient_av (wave_fwigradient.c:221-230), evaluated in double as
-          // the C expression is, accumulated into the float gradient
+        if (MODE == ADJ_REF && img) {
+          // gradient_av (wave_fwigradient.c:221-230): the C expression in
+          // double, unfused, added to the float gradient
 #pragma unroll
           for (int e = 0; e < 4; e++) {
             const int iz = iz0 + e;
             if (iz >= a.nb && iz < a.nb + a.nz) {
               const size_t k = (size_t)(x - a.nb) * a.nz + (iz - a.nb);
-              float temp = a.vint[k];
-              temp = fmul(fmul(temp, temp), temp);
-              temp = (float)(-2. / (double)temp);
-              const double w1 = a.wnext[s * a.wstride + k], w0 = a.wcur[s * a.wstride + k],
-                           wm = a.wprev[s * a.wstride + k];
-              const double gsum = (w1 - 2. * w0 + wm) / (double)a.wdt2 * (double)el(c, e) * (double)temp;
-              gs[k] = (float)((double)gs[k] + gsum);
+              const double gsum = __dmul_rn(__dmul_rn(__ddiv_rn(rw[e], (double)a.wdt2),
+                                                      (double)el(c, e)),
+                                            (double)rt[e]);
+              gs[k] = __double2float_rn(__dadd_rn((double)rg[e], gsum));
             }
           }
         }
@@ -466,6 +485,16 @@ __global__ void transpose_kernel(const float *in, float *out, long long rows, lo
 // Exact gradient: dJ/dv_pad = 2 * sum(phi*term) / v_pad, folded back through
 // pad2d's edge replication onto the interior (one thread per interior cell,
 // summing the padded cells that copy it, in a fixed order).
+// (float)(-2./temp) with temp = v*v*v in float (wave_fwigradient.c:224-226),
+// once per call instead of per cell and step
+__global__ void m2v3_kernel(const float *vel, size_t n, float *out) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const float v = vel[k];
+    out[k] = __double2float_rn(__ddiv_rn(-2., (double)__fmul_rn(__fmul_rn(v, v), v)));
+  }
+}
+
 __global__ void fold_grad_kernel(const float *gacc, const float *vel, int nz, int nx, int nb,
                                  int pnz, int pnx, int lz, float *grad) {
   const long long n = (long long)nz * nx;
@@ -1132,6 +1161,7 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   const size_t gslice = exact ? (size_t)S.fstride : nvel;
   const size_t o_gs = cv.add(nsb > 1 ? (size_t)nsb * gslice * 4 : 0);
   const size_t o_grad = cv.add(nvel * 4);
+  const size_t o_m2v3 = cv.add(exact ? 0 : nvel * 4);
   const size_t o_mis = cv.add(16);
   const size_t o_mx = cv.add(16);
   Workspace &ws = Workspace::for_current_device();
@@ -1174,7 +1204,11 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   p.bz = at<float>(base, o_bz);
   p.bx = at<float>(base, o_bx);
   p.wav = at<float>(base, o_wav);
-  p.vint = d_vel;
+  if (!exact) {
+    m2v3_kernel<<<592, 256, 0, st>>>(d_vel, nvel, at<float>(base, o_m2v3));
+    PW_CUDA(cudaGetLastError());
+    p.m2v3 = at<float>(base, o_m2v3);
+  }
   p.wdt2 = (a->dt * interval) * (a->dt * interval);
   float *gtotal = exact ? gacc : gdev;
   float *gslices = at<float>(base, o_gs);
