@@ -419,7 +419,17 @@ def run_fwi2d(args, world, rank, local):
                "d2h_bytes_per_step": int(g_h.numel() * 4 + 8)}
 
     peak, peak_kind = peaks()
-    alg = 52.0 * pad * nt * ns  # forward 16 B + exact adjoint 36 B per point-step-shot
+    # forward 20 B (cur, prev, V read; next, term write) + exact adjoint 28 B
+    # (cur, prev, V, term, gradient read; next, gradient write) per
+    # point-step-shot: the planner keeps every forward term at this size
+    alg = 48.0 * pad * nt * ns
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            per_step = json.load(fh).get(f"fwi2d_s{ns}_step")
+        traffic = per_step * nt if per_step else None
+    except (OSError, ValueError):
+        pass
     achieved = alg / (loop_b / 1e3) / 1e9
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -450,7 +460,9 @@ def run_fwi2d(args, world, rank, local):
                                         "note": "gradient_av imaging, batched"},
             "e2e": e2e, "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "traffic_unit": "bytes per gradient (ncu, one FWD + one ADJ_EXACT "
+                                         "launch per step)",
                          "kernel": "pf_step_kernel FWD + ADJ_EXACT (whole gradient loop)",
                          "alg_bytes_per_gradient": alg, "loop_ms": loop_b,
                          "peak_source": peak_kind},

@@ -1085,17 +1085,18 @@ extern "C" int pw_pfwi_forward(const pw_fwi_args *a, const float *vel, const flo
 // fields per shot and the checkpoints two fields every k steps.  The forward
 // pass keeps the terms of the last segment, so the backward pass recomputes
 // nt - k steps: k is the largest interval whose working set fits the HBM
-// budget (80% of the free memory; k = nt recomputes nothing).  When not even
+// budget (80% of the free memory plus the workspace this call reuses; k = nt
+// recomputes nothing).  When not even
 // k = sqrt(2 nt), the interval of the smallest working set, fits, the shot
 // batch shrinks first.
-static void plan_exact(const Setup &S, int ckpt_k, int &k, int &nsb) {
+static void plan_exact(const Setup &S, int ckpt_k, size_t held, int &k, int &nsb) {
   const int nt = S.a.nt;
   size_t freeb = 0, totb = 0;
   if (cudaMemGetInfo(&freeb, &totb) != cudaSuccess) {
     cudaGetLastError();
     freeb = (size_t)32 << 30;
   }
-  const double budget = 0.8 * (double)freeb;
+  const double budget = 0.8 * (double)(freeb + held);
   const double fb = (double)S.fstride * 4;
   auto need = [&](int kk, int nb) {
     const int nck = (nt + kk - 1) / kk;
@@ -1134,9 +1135,11 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   const bool exact = mode == PW_GRAD_EXACT;
   const int interval = std::max(1, a->interval);
   const int wnt = (nt - 1) / interval + 1;
+  Workspace &ws = Workspace::for_current_device();
+  std::lock_guard<std::mutex> lock(ws.mutex());
   int k = 0, nsb = per_shot ? 1 : std::min(ns, MAXS);
   if (exact) {
-    plan_exact(S, ckpt_k, k, nsb);
+    plan_exact(S, ckpt_k, ws.capacity(), k, nsb);
     if (per_shot) nsb = 1;
   }
   const int nck = exact ? (nt + k - 1) / k : 0;
@@ -1164,11 +1167,12 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   const size_t o_m2v3 = cv.add(exact ? 0 : nvel * 4);
   const size_t o_mis = cv.add(16);
   const size_t o_mx = cv.add(16);
-  Workspace &ws = Workspace::for_current_device();
-  std::lock_guard<std::mutex> lock(ws.mutex());
   PW_TRY(ws.reserve(cv.total()));
   char *base = ws.base();
-  PW_CUDA(cudaMemsetAsync(base, 0, cv.total(), st));
+  // snapshots, checkpoints and segment terms are written before they are
+  // read: zero the rest only (the term buffer alone is tens of GB)
+  PW_CUDA(cudaMemsetAsync(base, 0, o_snap, st));
+  PW_CUDA(cudaMemsetAsync(base + o_ga, 0, cv.total() - o_ga, st));
   const float *d_vel = vel;
   if (host) {
     PW_TRY(to_device(base + o_vel, vel, nvel * 4, true, st));

@@ -55,6 +55,7 @@ class Workspace {
   // Reserve `bytes` (rounded); returns PW_OK or PW_ERR_OOM.
   int reserve(size_t bytes);
   char *base() const { return base_; }
+  size_t capacity() const { return cap_; }
   void release();
   std::mutex &mutex() { return mu_; }
 
