@@ -45,9 +45,9 @@ def parse():
     p.add_argument("--groups", type=int, default=4)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="tri3d", choices=["tri3d", "fwi2d", "batch2d"],
+    p.add_argument("--workload", default="tri3d", choices=["tri3d", "fwi2d", "batch2d", "c1"],
                    help="tri3d: the 3-D TRI image (default); fwi2d: 2-D FWI gradients/s; "
-                        "batch2d: uneven 2-D forward shots in one batch")
+                        "batch2d: uneven 2-D forward shots in one batch; c1: one 2-D shot")
     p.add_argument("--shots", type=int, default=32, help="fwi2d: shots per gradient")
     p.add_argument("--fwi-nt", type=int, default=2000, help="fwi2d: time samples")
     return p.parse_args()
@@ -694,6 +694,167 @@ def run_batch2d(args, world, rank, local):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------------------
+# c1: one 2-D shot, three-layer 201x201 model, receivers at depth 5
+
+C1_N, C1_NT = 201, 1501
+
+
+def c1_model():
+    vel = np.full((C1_N, C1_N), 1500, np.float32)
+    vel[60:130] = 2200
+    vel[130:] = 3000
+    kw = dict(nt=C1_NT, dt=0.001, ax=[0, 10, C1_N], az=[0, 10, C1_N], ns=1, sx=[100], sz=[5],
+              f=[20], t=[0.05], A=[1], nbt=NBT, ct=CT, jsnap=0, gz=5)
+    return vel, kw
+
+
+def _c1_ref_worker(kind="reference"):
+    """One whole C1 propagation by the reference's afd2dc (oracle/_ref; kind
+    "port": the oracle's C restatement), receivers at z=0 and no snapshots
+    (afd2dc has no depth receivers; the propagation work is the same)."""
+    sys.path.insert(0, ROOT)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    vel, kw = c1_model()
+    t0 = time.perf_counter()
+    if kind == "reference":
+        sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+        import afdcfun  # the reference's own extension module
+        s = np.array(kw["sx"] + kw["sz"] + kw["f"] + kw["t"] + kw["A"], np.float32)
+        afdcfun.afd2dc(vel.flatten(order="F"), s, 0, C1_NT, C1_N, C1_N, 1, 0, C1_NT, 0, 1, NBT,
+                       CT, 0.001, 0.0, 10.0, 0.0, 10.0)
+    else:
+        from oracle import oracle as O
+        O.afd(vel, C1_NT, 0.001, (10.0, 10.0), nbt=NBT, ct=CT,
+              src=dict(sx=kw["sx"], sz=kw["sz"], f=kw["f"], t=kw["t"], A=kw["A"]))
+    return (C1_N + 2 * NBT) ** 2 * C1_NT, time.perf_counter() - t0
+
+
+def _c1_cpu(workers):
+    for kind in ("reference", "port"):
+        try:
+            res = pool_map(_c1_ref_worker, [(kind,)] * workers, timeout_s=300)
+            return sum(r[0] for r in res) / max(r[1] for r in res) / 1e9, kind
+        except Exception:  # noqa: BLE001
+            continue
+    raise RuntimeError("neither the reference nor the port ran")
+
+
+def run_c1(args, world, rank, local):
+    pts = (C1_N + 2 * NBT) ** 2 * C1_NT
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        workers = max(1, min(os.cpu_count() or 1, 16))
+        rates = []
+        for i in range(args.warmup + args.steps):
+            v, kind = _c1_cpu(workers)
+            if i >= args.warmup:
+                rates.append(v)
+        value = statistics.median(rates)
+        print(json.dumps({
+            "impl": "reference", "metric": "Gpt-updates/s (2-D single shot)", "value": value,
+            "unit": "Gpt/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": f"2-D shot {C1_N}^2 three layers h=10m "
+                                                        f"nt={C1_NT} nbt={NBT}"},
+            "cpu_baseline": {"value": value, "unit": "Gpt/s", "cores": workers, "kind": kind,
+                             "sample": f"whole afd2dc propagation, {workers} independent "
+                                       "single-threaded processes"},
+            "e2e": {"value": value, "unit": "Gpt/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+    import pywave_b200 as pw
+    from pywave_b200 import _lib as L
+    from pywave_b200 import build as B
+    B.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lib = L.lib()
+    vel, kw = c1_model()
+    a = L.AfdArgs(dim=2, nz=C1_N, nx=C1_N, ny=1, nt=C1_NT, nbt=NBT, ct=CT, dt=0.001, dz=10.0,
+                  dx=10.0, dy=10.0, ns=1, tri=0, jsnap=0, gz=5, flags=0)
+    v_d = torch.from_numpy(np.ascontiguousarray(vel.flatten(order="F"))).cuda()
+    s_d = torch.tensor(kw["sx"] + kw["sz"] + kw["f"] + kw["t"] + kw["A"], dtype=torch.float32,
+                       device="cuda")
+    d_d = torch.empty(C1_NT * C1_N, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+
+    def shot():
+        L.check(lib.pw_afd(C.byref(a), v_d.data_ptr(), s_d.data_ptr(), None, d_d.data_ptr(),
+                           None, st))
+        return L.last_timing()
+
+    for _ in range(args.warmup):
+        shot()
+    clk = Clocks(local)
+    clk.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    loops, launches = [], 0
+    e0.record()
+    for _ in range(args.steps):
+        ms, nst, tot = shot()
+        loops.append(ms)
+        launches += tot
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms_b = max_over_ranks(e0.elapsed_time(e1), world)
+    value = job_rate(pts, args.steps, world, ms_b) / 1e9
+    e2e = None
+    if not args.no_e2e:
+        pw.afd2d(vel, **kw)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            pw.afd2d(vel, **kw)
+        ems = max_over_ranks((time.perf_counter() - t0) * 1e3, world)
+        e2e = {"value": job_rate(pts, args.steps, world, ems) / 1e9, "unit": "Gpt/s",
+               "h2d_bytes_per_step": int(vel.nbytes + 20),
+               "d2h_bytes_per_step": int(C1_NT * C1_N * 4)}
+    peak, peak_kind = peaks()
+    loop_ms = statistics.median(loops)
+    achieved = pts * 16 / (loop_ms / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, kind = _c1_cpu(1)
+            cpu = {"value": v, "unit": "Gpt/s", "cores": 1, "kind": kind,
+                   "sample": "the whole C1 propagation by afd2dc, 1 core"}
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "unit": "Gpt/s", "cores": 1, "kind": "reference",
+                   "sample": f"failed: {ex!r}"[:200]}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Gpt-updates/s (2-D single shot)", "value": value, "unit": "Gpt/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (three-layer model)",
+            "config": {"workload": f"2-D shot {C1_N}^2 h=10m nt={C1_NT} dt=1ms nbt={NBT}, 20 Hz "
+                                   "source at (5,100), receivers at z=5",
+                       "points_per_step": pts,
+                       "l2": "working set (3 fields, 0.8 MB) inside L2: no flush, "
+                             "an L2-resident latency/launch-bound case"},
+            "e2e": e2e, "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "march_kernel<TWO_D> (whole time loop)", "loop_ms": loop_ms,
+                         "alg_bytes_per_step": pts * 16, "peak_source": peak_kind},
+            "cpu_baseline": cpu, "clocks": clocks}), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -703,6 +864,8 @@ def main():
         return run_fwi2d(args, world, rank, local)
     if args.workload == "batch2d":
         return run_batch2d(args, world, rank, local)
+    if args.workload == "c1":
+        return run_c1(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, rank)
 

@@ -342,6 +342,234 @@ __global__ void __launch_bounds__(MARCH_MAXT) march_kernel(const StepArgs a) {
   march_body<TWO_D, TRI, SNAP>(a, blockIdx.x, blockIdx.y, ring);
 }
 
+// Cluster-resident 2-D propagation for grids that fit in the distributed
+// shared memory of one thread-block cluster: ONE launch runs every time step.
+// CTA r of the cluster owns columns [r*w, r*w + w) of the kernel y axis (the
+// model's x) with all z; its shared memory holds, per group, the current and
+// the next/previous field of those columns plus two halo columns on each
+// side, and vv.  A step updates the owned cells in place over the previous
+// field (each cell reads its own previous value only), writes the two edge
+// columns also into the neighbours' halo columns (distributed shared memory
+// stores), and ends with one cluster barrier; the next step reads the halos
+// locally.  Domain edges keep zero halos, as the global layout does.  The
+// arithmetic per cell is march_body's, term by term, so results are
+// bit-identical to the step-per-launch path.
+constexpr int RES_NTH = 512;   // threads per CTA
+constexpr int RES_MAXIPT = 8;  // items (float4 of z cells) per thread, at most
+
+struct ResArgs {
+  StepArgs s;    // it, wfd and img are set per step inside the kernel
+  int w;         // owned columns per CTA
+  int nsl;       // live z float4 slots per column (slot 0 is the zero halo)
+  int LZ;        // floats per shared-memory column
+  int jsnap;
+  float *wfd0;   // snapshot base [ntsnap][interior] or null
+  size_t nvel;   // floats per snapshot
+  float *img0;   // TRI image accumulator (field layout) or null
+};
+
+__device__ __forceinline__ float4 *dsmem_map(float4 *p, unsigned rank) {
+  // address of the same shared-memory offset in CTA `rank` of the cluster
+  unsigned long long r;
+  asm volatile("mapa.u64 %0, %1, %2;\n" : "=l"(r) : "l"(p), "r"(rank));
+  return reinterpret_cast<float4 *>(r);
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release;\n"
+               "barrier.cluster.wait.acquire;\n" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_size() {
+  unsigned n;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(n));
+  return n;
+}
+
+template <bool TRI, int IPT>
+__global__ void __launch_bounds__(RES_NTH) resident_kernel(const __grid_constant__ ResArgs r) {
+  extern __shared__ float4 res_sm[];
+  const StepArgs &a = r.s;
+  const Geo &g = a.g;
+  const int G = TRI ? a.ngroups : 1;
+  const unsigned rank = cluster_rank(), nrank = cluster_size();
+  const int w = r.w, W4 = w + 4, LZ4 = r.LZ / 4;  // columns incl. halos; float4 per column
+  const int arr4 = W4 * LZ4;                       // float4 per array
+  const int y0 = (int)rank * w;
+  float4 *vvs = res_sm + 2 * G * arr4;
+  // taper factors: z for every row (1 beyond nz), y for the owned columns
+  float4 *swz4 = vvs + arr4;
+  float *swz = reinterpret_cast<float *>(swz4);
+  float *swy = swz + r.LZ;
+  for (int i = threadIdx.x; i < r.LZ; i += blockDim.x)
+    swz[i] = (i >= HZ && i - HZ < g.nz) ? a.wz[i - HZ] : 1.f;
+  for (int i = threadIdx.x; i < w; i += blockDim.x) swy[i] = y0 + i < g.ny ? a.wy[y0 + i] : 1.f;
+  // zero the fields and halos, load vv of the owned columns
+  for (int i = threadIdx.x; i < 2 * G * arr4; i += blockDim.x)
+    res_sm[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = threadIdx.x; i < arr4; i += blockDim.x) {
+    const int c = i / LZ4, sl = i - c * LZ4;
+    const int y = y0 + c - 2;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c >= 2 && c < w + 2 && y < g.ny && sl >= 1 && 4 * sl - HZ < g.nz)
+      v = *reinterpret_cast<const float4 *>(a.vv + foff(g, 4 * sl - HZ, 0, y));
+    vvs[i] = v;
+  }
+  // this thread's items (fixed for the whole run): shared-memory offset, and
+  // flag bits 0 live, 1-4 Laplacian rows, 5-8 kept rows, 9 Laplacian
+  // column, 10 receiver row, 11 source column, 12 interior column, 13/14 edge
+  // column copied to the left / right neighbour
+  const int items = w * r.nsl;
+  int po4[IPT], pc[IPT];
+  unsigned pf[IPT];
+#pragma unroll
+  for (int j = 0; j < IPT; j++) {
+    const int item = threadIdx.x + j * RES_NTH;
+    const int c = item / r.nsl;
+    const int slot = item - c * r.nsl + 1;
+    const int y = y0 + c;
+    const int iz0 = 4 * slot - HZ;
+    unsigned f = 0;
+    if (item < items && y < g.ny) {
+      f = 1u;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int iz = iz0 + e;
+        if (iz >= g.lz0 && iz < g.lz1) f |= 2u << e;
+        if (iz < g.nz) f |= 32u << e;
+      }
+      if (y >= g.ly0 && y < g.ly1) f |= 1u << 9;
+      const int erz = a.rz - iz0;
+      if (erz >= 0 && erz < 4 && a.rx0 == 0 && a.nrx >= 1 && y >= a.ry0 && y < a.ry0 + a.nry)
+        f |= 1u << 10;
+      bool sp = false;
+      if (!TRI)
+        for (int sidx = 0; sidx < a.ns; sidx++) sp |= (y >= a.sy[sidx] - 1 && y <= a.sy[sidx] + 1);
+      if (sp) f |= 1u << 11;
+      if (y >= a.nby && y < a.nby + a.ny1 && 0 >= a.nbx && 0 < a.nbx + a.nx1) f |= 1u << 12;
+      if (c < 2 && rank > 0) f |= 1u << 13;
+      if (c >= w - 2 && rank + 1 < nrank) f |= 1u << 14;
+    }
+    po4[j] = (c + 2) * LZ4 + slot;
+    pc[j] = c;
+    pf[j] = f;
+  }
+  cluster_sync_all();  // every CTA's arrays are zeroed before any halo store
+  const int nrec = a.nrx * a.nry;
+  for (int k = 0; k < a.nt; k++) {
+    const int it = TRI ? a.nt - 1 - k : k;
+    const bool snap = r.jsnap > 0 && it % r.jsnap == 0;
+    float *wfd = (snap && r.wfd0) ? r.wfd0 + (size_t)(it / r.jsnap) * r.nvel : nullptr;
+    float *img = (TRI && snap) ? r.img0 : nullptr;
+    const int par = k & 1;  // array 2g+par is the current field of group g
+#pragma unroll
+    for (int j = 0; j < IPT; j++) {
+      const unsigned f = pf[j];
+      if (!(f & 1u)) continue;
+      const int o4 = po4[j], c = pc[j];
+      const int slot = o4 - (c + 2) * LZ4;
+      const int y = y0 + c;
+      const int iz0 = 4 * slot - HZ;
+      const float4 wz4 = swz4[slot];
+      const float wz[4] = {wz4.x, wz4.y, wz4.z, wz4.w};
+      const float wy = swy[c];
+      const bool lyok = f & (1u << 9);
+      const bool rec_here = f & (1u << 10);
+      const bool src_plane = f & (1u << 11);
+      const int erz = a.rz - iz0;
+      const int r_idx = rec_here ? (y - a.ry0) * a.nrx : 0;
+      const float4 vv4 = vvs[o4];
+      float4 prod = make_float4(1.f, 1.f, 1.f, 1.f);
+      float4 res0 = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int gi = 0; gi < G; gi++) {
+        const float4 *cur = res_sm + (2 * gi + par) * arr4;
+        float4 *nxt = res_sm + (2 * gi + 1 - par) * arr4;
+        const float4 q0 = cur[o4 - 2 * LZ4], q1 = cur[o4 - LZ4], q2 = cur[o4];
+        const float4 q3 = cur[o4 + LZ4], q4 = cur[o4 + 2 * LZ4];
+        const float4 L = cur[o4 - 1], R = cur[o4 + 1];
+        const float Lz = L.z, Lw = L.w, Rx = R.x, Ry = R.y;
+        const float4 pv = nxt[o4];
+        bool inj = false;
+        float dval = 0.f;
+        if (TRI && rec_here) {
+          inj = a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi;
+          if (inj) dval = a.tri_dat[(size_t)it * nrec + r_idx];
+        }
+        float4 res;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const float cv = el(q2, e);
+          const float zm1 = e == 0 ? Lw : el(q2, e - 1);
+          const float zp1 = e == 3 ? Rx : el(q2, e + 1);
+          const float zm2 = e == 0 ? Lz : (e == 1 ? Lw : el(q2, e - 2));
+          const float zp2 = e == 2 ? Rx : (e == 3 ? Ry : el(q2, e + 2));
+          float tt = fmul(fmul(a.c0, cv), a.k0);
+          tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
+          tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
+          tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
+          tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
+          const float lap = ((f & (2u << e)) && lyok) ? tt : 0.f;
+          float pp = fmul(el(pv, e), wz[e]);
+          pp = fmul(pp, wy);
+          const float vve = el(vv4, e);
+          float v = fadd(cv, fsub(cv, pp));
+          v = fadd(v, fmul(lap, vve));
+          if (TRI) {
+            if (inj && e == erz) v = fadd(v, fmul(vve, dval));
+          } else if (src_plane) {
+            const int iz = iz0 + e;
+            for (int sidx = 0; sidx < a.ns; sidx++) {
+              const int dz = iz - a.sz[sidx], dys = y - a.sy[sidx];
+              if (dz >= -1 && dz <= 1 && dys >= -1 && dys <= 1) {
+                const float den = (float)(abs(dys) + abs(dz) + 1);
+                v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)sidx * a.nt + it]), den));
+              }
+            }
+          }
+          v = fmul(v, wz[e]);
+          v = fmul(v, wy);
+          set_el(res, e, (f & (32u << e)) ? v : 0.f);
+        }
+        nxt[o4] = res;
+        // the neighbours' halo copies of the two edge columns
+        if (f & (1u << 13)) *dsmem_map(nxt + o4 + w * LZ4, rank - 1) = res;
+        if (f & (1u << 14)) *dsmem_map(nxt + o4 - w * LZ4, rank + 1) = res;
+        if (gi == 0) res0 = res;
+        if (TRI) {
+          prod.x = fmul(fmul(prod.x, res.x), res.x);
+          prod.y = fmul(fmul(prod.y, res.y), res.y);
+          prod.z = fmul(fmul(prod.z, res.z), res.z);
+          prod.w = fmul(fmul(prod.w, res.w), res.w);
+        }
+      }
+      if (!TRI && rec_here && a.rec) a.rec[(size_t)it * nrec + r_idx] = el(res0, erz);
+      const bool interior = f & (1u << 12);
+      if (wfd && interior) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int iz = iz0 + e;
+          if (iz >= a.nbz && iz < a.nbz + a.nz1)
+            wfd[((size_t)(y - a.nby) * a.nx1 + (0 - a.nbx)) * a.nz1 + (iz - a.nbz)] = el(res0, e);
+        }
+      }
+      if (TRI && img && interior) {
+        float4 *ip = reinterpret_cast<float4 *>(img + foff(g, iz0, 0, y));
+        float4 im = *ip;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int iz = iz0 + e;
+          if (iz >= a.nbz && iz < a.nbz + a.nz1) set_el(im, e, fadd(el(im, e), el(prod, e)));
+        }
+        *ip = im;
+      }
+    }
+    cluster_sync_all();
+  }
+}
+
 // Batched 2-D forward modelling of shots of uneven size and length: one
 // launch per time step covers the tiles of every shot still running.  Item
 // i = (shot, tile) with tile = z chunk + nzc * y chunk; items are ordered by
@@ -1132,6 +1360,81 @@ static int check_velocity(const pw_afd_args *a, const float *vel_dev, size_t n, 
 }
 
 // Shared driver of pw_afd / pw_tri_image.
+// Cluster shape for resident_kernel: the largest cluster (16, 8, 4 or 2
+// CTAs, one per SM) whose column bands of at least 2 columns fit in shared
+// memory and that the device can schedule.  Returns false when the grid is
+// too large (the step-per-launch path then runs).
+struct ResPlan {
+  int C, w, nsl, LZ, threads;
+  size_t smem;
+  void *fn;
+};
+
+template <bool TRI>
+static void *resident_fn_t(int ipt) {
+  switch (ipt) {
+    case 1: return (void *)resident_kernel<TRI, 1>;
+    case 2: return (void *)resident_kernel<TRI, 2>;
+    case 3: return (void *)resident_kernel<TRI, 3>;
+    case 4: return (void *)resident_kernel<TRI, 4>;
+    case 5: case 6: return (void *)resident_kernel<TRI, 6>;
+    default: return (void *)resident_kernel<TRI, 8>;
+  }
+}
+static void *resident_fn(bool tri, int ipt) {
+  return tri ? resident_fn_t<true>(ipt) : resident_fn_t<false>(ipt);
+}
+
+static bool plan_resident(const Geo &g, int G, bool tri, ResPlan &rp) {
+  const char *env = getenv("PW_AFD_RESIDENT");
+  if (env && env[0] == '0') return false;
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  rp.nsl = (g.nz + HZ + 3) / 4 - 1;
+  rp.LZ = 4 * (rp.nsl + 2);
+  rp.threads = RES_NTH;
+  const int narr = 2 * (tri ? G : 1) + 1;
+  for (int C : {16, 8, 4, 2}) {
+    const int w = (g.ny + C - 1) / C;
+    if (w < 2) continue;
+    const int ipt = (w * rp.nsl + RES_NTH - 1) / RES_NTH;
+    if (ipt > RES_MAXIPT) break;  // smaller clusters only need more
+    rp.fn = resident_fn(tri, ipt);
+    const size_t smem = ((size_t)narr * (w + 4) * rp.LZ + rp.LZ + w) * sizeof(float);
+    if (smem > (size_t)maxsm) break;  // smaller clusters only need more
+    if (cudaFuncSetAttribute(rp.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        (C > 8 && cudaFuncSetAttribute(rp.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                      cudaSuccess)) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(rp.threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, rp.fn, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (nclusters < 1) continue;
+    rp.C = C;
+    rp.w = w;
+    rp.smem = smem;
+    return true;
+  }
+  return false;
+}
+
 static int run(const pw_afd_args *a, int G, const int *group, const float *vel, const float *src,
                const float *wavelet, float *dat, float *wfd, float *img_out, int normalize,
                cudaStream_t st) {
@@ -1366,10 +1669,41 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   ia.nz1 = p.knz1; ia.nx1 = p.knx1; ia.ny1 = p.kny1;
   ia.s0 = (p.kbz + HZ) / 4;
   ia.ns4 = (p.kbz + p.knz1 - 1 + HZ) / 4 - ia.s0 + 1;
-  long long img_launches = 0;
+  long long img_launches = 0, step_launches = nt;
+  ResPlan rp{};
+  const bool resident = two_d && plan_resident(g, G, tri, rp);
+  if (getenv("PW_AFD_VERBOSE") && resident)
+    fprintf(stderr, "afd resident plan: cluster %d x %d threads, %d columns per CTA, %zu B smem\n",
+            rp.C, rp.threads, rp.w, rp.smem);
   LoopTimer timer(st);
   timer.start();
-  for (int k = 0; k < nt; k++) {
+  if (resident) {
+    ResArgs ra{};
+    ra.s = s;
+    ra.w = rp.w;
+    ra.nsl = rp.nsl;
+    ra.LZ = rp.LZ;
+    ra.jsnap = a->jsnap;
+    ra.wfd0 = wfd_dev;
+    ra.nvel = nvel;
+    ra.img0 = img;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = rp.C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(rp.C);
+    cfg.blockDim = dim3(rp.threads);
+    cfg.dynamicSmemBytes = rp.smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *args[] = {(void *)&ra};
+    PW_CUDA(cudaLaunchKernelExC(&cfg, rp.fn, args));
+    step_launches = 1;
+  }
+  for (int k = 0; k < nt && !resident; k++) {
     const int it = tri ? nt - 1 - k : k;
     s.it = it;
     for (int i = 0; i < G; i++) {
@@ -1416,7 +1750,7 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
     if (host) PW_TRY(to_host(img_out, dst, nvel * 4, true, st));
   }
   PW_CUDA(cudaStreamSynchronize(st));
-  timer.finish(nt, nt + aux_launches + img_launches);
+  timer.finish(step_launches, step_launches + aux_launches + img_launches);
   return PW_OK;
 }
 
