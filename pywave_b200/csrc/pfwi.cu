@@ -722,7 +722,7 @@ static int prepare_div(float d, DivC &c) {
     double lo = std::max(fmin / zh, fmin * d);
     if (zl != 0.f) lo = std::max(lo, fmin / std::fabs((double)zl));
     lo *= 4;
-    const double hi = std::min(fmax / 4 / zh, fmax / 4 * d);
+    const double hi = std::min({fmax / 4 / zh, fmax / 4 * d, fmax});  // finite numerators only
     if (lo * 4 < hi) {
       c.zh = zh;
       c.zl = zl;
