@@ -90,15 +90,47 @@ void ricker_table(int nt, float dt, float f0, float t0, float A, float *out) {
   for (int j = 0; j < nfft; j++) ctab[j] = std::cos(2.0 * M_PI * (double)j / (double)nfft);
   std::vector<double> two_shape(nw);
   for (int k = 0; k < nw; k++) two_shape[k] = 2.0 * shape[k];  // exact
-  // samples are independent: split them over host threads; the phase k*m
-  // mod nfft advances by m mod nfft per term (same terms, same order)
+  // the shape underflows to exactly 0 beyond some k (expf(1-w) < 2^-149):
+  // those terms add +-0, which leaves every partial sum unchanged (a sum
+  // starting at +0 never becomes -0), so the loops stop at the last nonzero
+  int kend = nfft / 2;
+  while (kend > 1 && two_shape[kend - 1] == 0.0) kend--;
+  // samples are independent: split them over host threads, and sum four
+  // samples side by side (four independent chains); the phase k*m mod nfft
+  // advances by m mod nfft per term (same terms, same order per sample)
   auto rows = [&](int n0, int n1) {
-    for (int n = n0; n < n1; n++) {
+    int n = n0;
+    for (; n + 4 <= n1; n += 4) {
+      long mm[4], ph[4];
+      double s[4];
+      for (int i = 0; i < 4; i++) {
+        const long m = n + i - k0;
+        mm[i] = ((m % nfft) + nfft) % nfft;
+        ph[i] = 0;
+        s[i] = shape[0];
+      }
+      for (int k = 1; k < kend; k++) {
+        const double t = two_shape[k];
+        for (int i = 0; i < 4; i++) {
+          ph[i] += mm[i];
+          if (ph[i] >= nfft) ph[i] -= nfft;
+          s[i] += t * ctab[ph[i]];
+        }
+      }
+      for (int i = 0; i < 4; i++) {
+        const long m = n + i - k0;
+        long ph2 = ((long)(nfft / 2) * m) % nfft;
+        if (ph2 < 0) ph2 += nfft;
+        s[i] += shape[nfft / 2] * ctab[ph2];
+        out[n + i] = (float)((double)A * s[i]);
+      }
+    }
+    for (; n < n1; n++) {
       const long m = n - k0;
       const long mm = ((m % nfft) + nfft) % nfft;
       double s = shape[0];
       long ph = 0;
-      for (int k = 1; k < nfft / 2; k++) {
+      for (int k = 1; k < kend; k++) {
         ph += mm;
         if (ph >= nfft) ph -= nfft;
         s += two_shape[k] * ctab[ph];
@@ -109,9 +141,9 @@ void ricker_table(int nt, float dt, float f0, float t0, float A, float *out) {
       out[n] = (float)((double)A * s);
     }
   };
-  const long long work = (long long)nt * nfft;
+  const long long work = (long long)nt * kend * 2;
   const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-  const int nthr = (int)std::min<long long>(std::min(hw, 32), std::max(1LL, work >> 22));
+  const int nthr = (int)std::min<long long>(std::min(hw, 32), std::max(1LL, work >> 19));
   if (nthr <= 1) {
     rows(0, nt);
   } else {
