@@ -36,6 +36,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <map>
+#include <tuple>
 
 namespace pw {
 namespace afd {
@@ -1403,30 +1405,43 @@ static bool plan_resident(const Geo &g, int G, bool tri, ResPlan &rp) {
     rp.fn = resident_fn(tri, ipt);
     const size_t smem = ((size_t)narr * (w + 4) * rp.LZ + rp.LZ + w) * sizeof(float);
     if (smem > (size_t)maxsm) break;  // smaller clusters only need more
-    if (cudaFuncSetAttribute(rp.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess ||
-        (C > 8 && cudaFuncSetAttribute(rp.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-                      cudaSuccess)) {
-      cudaGetLastError();
-      continue;
+    // the attribute set-up and the occupancy query, once per (kernel,
+    // shared memory, cluster size) and device
+    static std::mutex mu;
+    static std::map<std::tuple<int, void *, size_t, int>, bool> seen;
+    bool ok;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      const auto key = std::make_tuple(dev, rp.fn, smem, C);
+      auto hit = seen.find(key);
+      if (hit != seen.end()) {
+        ok = hit->second;
+      } else {
+        ok = cudaFuncSetAttribute(rp.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+                 cudaSuccess &&
+             (C <= 8 || cudaFuncSetAttribute(rp.fn, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                                             1) == cudaSuccess);
+        if (ok) {
+          cudaLaunchConfig_t cfg = {};
+          cudaLaunchAttribute attr[1];
+          attr[0].id = cudaLaunchAttributeClusterDimension;
+          attr[0].val.clusterDim.x = C;
+          attr[0].val.clusterDim.y = 1;
+          attr[0].val.clusterDim.z = 1;
+          cfg.gridDim = dim3(C);
+          cfg.blockDim = dim3(rp.threads);
+          cfg.dynamicSmemBytes = smem;
+          cfg.attrs = attr;
+          cfg.numAttrs = 1;
+          int nclusters = 0;
+          ok = cudaOccupancyMaxActiveClusters(&nclusters, rp.fn, &cfg) == cudaSuccess &&
+               nclusters >= 1;
+        }
+        cudaGetLastError();
+        seen[key] = ok;
+      }
     }
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = C;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(C);
-    cfg.blockDim = dim3(rp.threads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, rp.fn, &cfg) != cudaSuccess) {
-      cudaGetLastError();
-      continue;
-    }
-    if (nclusters < 1) continue;
+    if (!ok) continue;
     rp.C = C;
     rp.w = w;
     rp.smem = smem;
