@@ -1405,41 +1405,46 @@ static bool plan_resident(const Geo &g, int G, bool tri, ResPlan &rp) {
     rp.fn = resident_fn(tri, ipt);
     const size_t smem = ((size_t)narr * (w + 4) * rp.LZ + rp.LZ + w) * sizeof(float);
     if (smem > (size_t)maxsm) break;  // smaller clusters only need more
-    // the attribute set-up and the occupancy query, once per (kernel,
-    // shared memory, cluster size) and device
+    // the kernel's shared-memory limit only grows (it is per kernel, and a
+    // cached smaller value must not shadow a larger one set since); the
+    // cluster occupancy query runs once per (kernel, shared memory, cluster)
     static std::mutex mu;
+    static std::map<std::pair<int, void *>, size_t> attr_max;
     static std::map<std::tuple<int, void *, size_t, int>, bool> seen;
-    bool ok;
+    bool ok = true;
     {
       std::lock_guard<std::mutex> lock(mu);
-      const auto key = std::make_tuple(dev, rp.fn, smem, C);
-      auto hit = seen.find(key);
-      if (hit != seen.end()) {
-        ok = hit->second;
-      } else {
+      size_t &am = attr_max[std::make_pair(dev, rp.fn)];
+      if (smem > am) {
         ok = cudaFuncSetAttribute(rp.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
-                 cudaSuccess &&
-             (C <= 8 || cudaFuncSetAttribute(rp.fn, cudaFuncAttributeNonPortableClusterSizeAllowed,
-                                             1) == cudaSuccess);
-        if (ok) {
-          cudaLaunchConfig_t cfg = {};
-          cudaLaunchAttribute attr[1];
-          attr[0].id = cudaLaunchAttributeClusterDimension;
-          attr[0].val.clusterDim.x = C;
-          attr[0].val.clusterDim.y = 1;
-          attr[0].val.clusterDim.z = 1;
-          cfg.gridDim = dim3(C);
-          cfg.blockDim = dim3(rp.threads);
-          cfg.dynamicSmemBytes = smem;
-          cfg.attrs = attr;
-          cfg.numAttrs = 1;
-          int nclusters = 0;
-          ok = cudaOccupancyMaxActiveClusters(&nclusters, rp.fn, &cfg) == cudaSuccess &&
-               nclusters >= 1;
-        }
-        cudaGetLastError();
+             cudaSuccess;
+        if (ok) am = smem;
+      }
+      if (ok && C > 8)
+        ok = cudaFuncSetAttribute(rp.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+             cudaSuccess;
+      const auto key = std::make_tuple(dev, rp.fn, smem, C);
+      const auto hit = seen.find(key);
+      if (ok && hit != seen.end()) {
+        ok = hit->second;
+      } else if (ok) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(C);
+        cfg.blockDim = dim3(rp.threads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        ok = cudaOccupancyMaxActiveClusters(&nclusters, rp.fn, &cfg) == cudaSuccess &&
+             nclusters >= 1;
         seen[key] = ok;
       }
+      cudaGetLastError();
     }
     if (!ok) continue;
     rp.C = C;
