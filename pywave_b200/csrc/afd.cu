@@ -427,6 +427,8 @@ __global__ void __launch_bounds__(RES_NTH) resident_kernel(const __grid_constant
   const int items = w * r.nsl;
   int po4[IPT], pc[IPT];
   unsigned pf[IPT];
+  float4 pwz[IPT];
+  float pwy[IPT];
 #pragma unroll
   for (int j = 0; j < IPT; j++) {
     const int item = threadIdx.x + j * RES_NTH;
@@ -459,6 +461,14 @@ __global__ void __launch_bounds__(RES_NTH) resident_kernel(const __grid_constant
     pc[j] = c;
     pf[j] = f;
   }
+  __syncthreads();  // the taper tables
+#pragma unroll
+  for (int j = 0; j < IPT; j++) {
+    const bool live = pf[j] & 1u;
+    const int slot = po4[j] - (pc[j] + 2) * LZ4;
+    pwz[j] = live ? swz4[slot] : make_float4(1.f, 1.f, 1.f, 1.f);
+    pwy[j] = live ? swy[pc[j]] : 1.f;
+  }
   cluster_sync_all();  // every CTA's arrays are zeroed before any halo store
   const int nrec = a.nrx * a.nry;
   for (int k = 0; k < a.nt; k++) {
@@ -475,9 +485,8 @@ __global__ void __launch_bounds__(RES_NTH) resident_kernel(const __grid_constant
       const int slot = o4 - (c + 2) * LZ4;
       const int y = y0 + c;
       const int iz0 = 4 * slot - HZ;
-      const float4 wz4 = swz4[slot];
-      const float wz[4] = {wz4.x, wz4.y, wz4.z, wz4.w};
-      const float wy = swy[c];
+      const float wz[4] = {pwz[j].x, pwz[j].y, pwz[j].z, pwz[j].w};
+      const float wy = pwy[j];
       const bool lyok = f & (1u << 9);
       const bool rec_here = f & (1u << 10);
       const bool src_plane = f & (1u << 11);
@@ -487,8 +496,8 @@ __global__ void __launch_bounds__(RES_NTH) resident_kernel(const __grid_constant
       float4 prod = make_float4(1.f, 1.f, 1.f, 1.f);
       float4 res0 = make_float4(0.f, 0.f, 0.f, 0.f);
       for (int gi = 0; gi < G; gi++) {
-        const float4 *cur = res_sm + (2 * gi + par) * arr4;
-        float4 *nxt = res_sm + (2 * gi + 1 - par) * arr4;
+        const float4 *__restrict__ cur = res_sm + (2 * gi + par) * arr4;
+        float4 *__restrict__ nxt = res_sm + (2 * gi + 1 - par) * arr4;
         const float4 q0 = cur[o4 - 2 * LZ4], q1 = cur[o4 - LZ4], q2 = cur[o4];
         const float4 q3 = cur[o4 + LZ4], q4 = cur[o4 + 2 * LZ4];
         const float4 L = cur[o4 - 1], R = cur[o4 + 1];
