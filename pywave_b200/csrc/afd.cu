@@ -1252,8 +1252,11 @@ static int plan_tile(bool tri, int G, int nsm, Plan &p) {
         const long long waves = (ctas + slots - 1) / slots;
         const double cap = (double)waves * slots * threads * (yc + 2);
         const double score = useful / cap * lat;
-        if (score > best + 1e-9) {
-          best = score;
+        // forward runs (one group): among equal scores the larger CTA, which
+        // measured faster (201^3: 4 warps 112.8 us per step, 1 warp 121.8)
+        const bool wider = G == 1 && score > best - 1e-9 && threads > 32 * bz * bx;
+        if (score > best + 1e-9 || wider) {
+          best = std::max(best, score);
           bz = WZ;
           bx = WX;
           by = yc;
