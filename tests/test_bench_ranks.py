@@ -49,3 +49,23 @@ def test_reference_arm_is_rank0_only(capsys):
         n, nt, groups, steps, warmup, gpus = 201, 1501, 4, 1, 0, 2
     assert bench.run_reference(A(), rank=1) is None
     assert capsys.readouterr().out == ""
+
+
+def test_c1_reference_arm_line():
+    """`bench.py --workload c1 --impl reference` on the host cores: one JSON
+    line with the arm's keys (the reference's afd2dc, or the oracle port when
+    the reference build is absent)."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "bench.py", "--workload", "c1", "--impl", "reference",
+                          "--steps", "1", "--warmup", "0"], cwd=root, capture_output=True,
+                         text=True, timeout=600, check=True).stdout
+    lines = [json.loads(x) for x in out.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    d = lines[0]
+    assert d["impl"] == "reference" and d["unit"] == "Gpt/s" and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": "Gpt/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
