@@ -39,8 +39,10 @@ def build(force: bool = False) -> str:
 
 
 def build_ref() -> bool:
-    """Compile the reference itself into oracle/_ref (needs its sources)."""
-    if not os.path.isdir("/root/reference/pywave/src"):
+    """Compile the reference itself into oracle/_ref from the sources under
+    $PYWAVE_REF (the pywave checkout); False when they are not there."""
+    root = os.environ.get("PYWAVE_REF", "")
+    if not root or not os.path.isdir(os.path.join(root, "pywave", "src")):
         return False
     subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
     return True

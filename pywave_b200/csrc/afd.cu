@@ -85,6 +85,9 @@ struct StepArgs {
   int nbz, nbx, nby, nz1, nx1, ny1;  // interior = [nb, nb+n1) per kernel axis
   float *wfd;                  // this step's snapshot [ny1][nx1][nz1] (group 0) or null
   float *img;                  // image accumulator (field layout) or null
+  // warp-plane counts of the 3-D step paths, or null (tile_kernel only):
+  // [0] TRI fast, [1] TRI full, [2..5] forward paths 0..3
+  unsigned long long *stats;
 };
 
 __device__ __forceinline__ float el(const float4 &v, int e) {
@@ -739,6 +742,9 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
   const int nrec = a.nrx * a.nry;
   const int ci = (xl + 2) * TILE_TZ + zl + 1;  // centre in the patch
 
+  // per-warp path counts (16 bits per path; a launch gives a warp at most
+  // ych < 65536 planes), flushed to a.stats at the end when requested
+  unsigned long long pcount = 0;
   // queue: plane y-2+k sits in q[(y - y0 + k) % 5]
   float4 q[5];
   q[4] = zero4;
@@ -790,6 +796,7 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
         if constexpr (TRI) {
           // time reversal: one fast path (no taper, no mask) and the full one
           const bool fast = warp_plain && lyok && !warp_taper_zx && wy == 1.f && !inj && !src_plane;
+          pcount += fast ? 1ull : (1ull << 16);
           if (fast) {
   #pragma unroll
             for (int e = 0; e < 4; e++) {
@@ -861,6 +868,7 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
           const int path = !clean ? 3
                            : (!warp_taper_zx ? (wy == 1.f ? 0 : (MULTI ? 1 : 3))
                                              : (MULTI && wy == 1.f && !warp_edge_zx ? 2 : 3));
+          pcount += 1ull << (16 * path);
           float4 lp;  // Laplacian sums in the reference's order
   #pragma unroll
           for (int e = 0; e < 4; e++) {
@@ -953,6 +961,13 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
     }
   }
   cp_wait_all();
+  if (a.stats != nullptr && lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const unsigned long long c = (pcount >> (16 * k)) & 0xffffull;
+      if (c) atomicAdd(a.stats + (TRI ? k : 2 + k), c);
+    }
+  }
 }
 
 // TRI image of one imaging step: img += prod_g u_g^2 over the interior cells
@@ -1573,6 +1588,9 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   const size_t o_gid = cv.add(use_gid ? nrec * 4 : 0);
   const size_t o_wfd = cv.add(wfd && host ? (size_t)ntsnap * nvel * 4 : 0);
   const size_t o_mx = cv.add(16);
+  // PW_AFD_VERBOSE: also count which paths the 3-D step kernels took
+  const bool want_stats = p.tile && getenv("PW_AFD_VERBOSE") != nullptr;
+  const size_t o_stats = cv.add(want_stats ? 8 * sizeof(unsigned long long) : 0);
 
   Workspace &ws = Workspace::for_current_device();
   std::lock_guard<std::mutex> lock(ws.mutex());
@@ -1690,6 +1708,7 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   s.rec = (!tri && dat) ? rec : nullptr;
   s.nbz = p.kbz; s.nbx = p.kbx; s.nby = p.kby;
   s.nz1 = p.knz1; s.nx1 = p.knx1; s.ny1 = p.kny1;
+  s.stats = want_stats ? at<unsigned long long>(base, o_stats) : nullptr;
   float *wfd_dev = wfd ? (host ? at<float>(base, o_wfd) : wfd) : nullptr;
   void *fn = p.fn;
   const int threads = p.threads;
@@ -1783,6 +1802,14 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   }
   PW_CUDA(cudaStreamSynchronize(st));
   timer.finish(step_launches, step_launches + aux_launches + img_launches);
+  if (want_stats) {
+    unsigned long long c[6];
+    PW_CUDA(cudaMemcpy(c, s.stats, sizeof c, cudaMemcpyDeviceToHost));
+    fprintf(stderr,
+            "afd tile paths (warp-planes): tri_fast=%llu tri_full=%llu fwd_path0=%llu "
+            "fwd_path1=%llu fwd_path2=%llu fwd_path3=%llu\n",
+            c[0], c[1], c[2], c[3], c[4], c[5]);
+  }
   return PW_OK;
 }
 
@@ -2235,6 +2262,17 @@ static int run_noalloc(const pw_afd_args *a, const float *vel, const float *src,
   // stream has drained, so calls never overlap on the array
   static std::mutex locks[NOALLOC_MAXDEV];
   std::lock_guard<std::mutex> lock(locks[dev]);
+  // Declared after the lock, so it runs first on every return: once work on
+  // the array is queued, the lock is released only after `st` has drained,
+  // on the error returns too (its status is ignored there; the error that
+  // caused the return is the one reported).
+  struct DrainOnExit {
+    cudaStream_t st;
+    bool armed = false;
+    ~DrainOnExit() {
+      if (armed) cudaStreamSynchronize(st);
+    }
+  } drain{st};
   char *base = nullptr;
   PW_TRY(noalloc_scratch(&base));
   float *vv = at<float>(base, o_vv);
@@ -2245,6 +2283,7 @@ static int run_noalloc(const pw_afd_args *a, const float *vel, const float *src,
   unsigned int *mx = at<unsigned int>(base, o_mx);
 
   // wavefields, the padded velocity's halo and the trace buffer start at zero
+  drain.armed = true;
   PW_CUDA(cudaMemsetAsync(base, 0, need, st));
   PW_TRY(check_velocity(a, vel, nvel, mx, st));
 

@@ -10,21 +10,42 @@
 namespace pw {
 namespace lb {
 
-// sum(a[i]*b[i]) in FP64: grid-stride partial sums, one atomic per warp.
-__global__ void dot_kernel(const float *a, const float *b, long long n, double *out) {
+// sum(a[i]*b[i]) in FP64, deterministic: a fixed grid of DOT_BLOCKS blocks
+// of DOT_THREADS threads, each thread a grid-stride partial sum, each block a
+// fixed shared-memory tree into part[block]; dot_final_kernel then adds the
+// block sums in block order.  The same inputs give the same bits on every run
+// (no atomics), so the line search takes the same decisions every time.
+constexpr int DOT_BLOCKS = 296, DOT_THREADS = 256;
+
+__global__ void __launch_bounds__(DOT_THREADS) dot_kernel(const float *a, const float *b,
+                                                          long long n, double *part) {
+  __shared__ double sh[DOT_THREADS];
   double s = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    s += (double)a[i] * (double)b[i];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+  for (long long i = blockIdx.x * (long long)DOT_THREADS + threadIdx.x; i < n;
+       i += (long long)DOT_BLOCKS * DOT_THREADS)
+    s = __dadd_rn(s, __dmul_rn((double)a[i], (double)b[i]));
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = DOT_THREADS / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) sh[threadIdx.x] = __dadd_rn(sh[threadIdx.x], sh[threadIdx.x + h]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
-// y = a*x + b*y (FP64 coefficients, float32 storage)
+__global__ void dot_final_kernel(const double *part, double *out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < DOT_BLOCKS; k++) s = __dadd_rn(s, part[k]);
+    *out = s;
+  }
+}
+
+// y = a*x + b*y (FP64 coefficients and arithmetic, no contraction; float32 storage)
 __global__ void axpby_kernel(double a, const float *x, double b, float *y, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
-    y[i] = (float)(a * (double)x[i] + b * (double)y[i]);
+    y[i] = (float)__dadd_rn(__dmul_rn(a, (double)x[i]), __dmul_rn(b, (double)y[i]));
 }
 
 // x = clip(xk + alpha*d, lo, hi) (line_search, wave_fwilbfgs.c:125-128)
@@ -32,7 +53,8 @@ __global__ void trial_kernel(const float *xk, const float *d, float alpha, float
                              float *x, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    float v = xk[i] + alpha * d[i];
+    // the product rounded on its own, as the reference's C evaluates it
+    float v = __fadd_rn(xk[i], __fmul_rn(alpha, d[i]));
     if (v < lo) v = lo;
     if (v > hi) v = hi;
     x[i] = v;
@@ -48,12 +70,12 @@ __global__ void sub_kernel(const float *a, float *b, long long n) {  // b = a - 
 struct Dev {
   cudaStream_t st;
   long long n;
-  double *acc;  // device scalar
+  double *acc;  // device scalars: DOT_BLOCKS block sums, then the total
   int dot(const float *a, const float *b, double *out) {
-    PW_CUDA(cudaMemsetAsync(acc, 0, 8, st));
-    dot_kernel<<<296, 256, 0, st>>>(a, b, n, acc);
+    dot_kernel<<<DOT_BLOCKS, DOT_THREADS, 0, st>>>(a, b, n, acc);
+    dot_final_kernel<<<1, 32, 0, st>>>(acc, acc + DOT_BLOCKS);
     PW_CUDA(cudaGetLastError());
-    PW_CUDA(cudaMemcpyAsync(out, acc, 8, cudaMemcpyDeviceToHost, st));
+    PW_CUDA(cudaMemcpyAsync(out, acc + DOT_BLOCKS, 8, cudaMemcpyDeviceToHost, st));
     PW_CUDA(cudaStreamSynchronize(st));
     return PW_OK;
   }
@@ -113,7 +135,7 @@ extern "C" int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav,
   PW_TRY(B.alloc(&q, n));
   PW_TRY(B.alloc(&sk, n * npair));
   PW_TRY(B.alloc(&yk, n * npair));
-  PW_TRY(B.alloc(&acc, 1));
+  PW_TRY(B.alloc(&acc, DOT_BLOCKS + 1));
   const long long nd = (long long)a->ns * a->nx * a->nt;
   if (host) {
     PW_TRY(B.alloc(&wav_d, a->nt));

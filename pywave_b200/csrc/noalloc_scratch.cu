@@ -1,7 +1,10 @@
 // The fixed device scratch of pw_afd_noalloc.  It lives in its own
-// translation unit, so its module (and the array with it) is loaded only by
-// the first call that asks for its address, not by the library's other entry
-// points.  Every device gets its own copy of the array in its context.
+// translation unit, so under lazy module loading (CUDA_MODULE_LOADING=LAZY,
+// the default since CUDA 12.2) its module, and the array with it, is loaded
+// only by the first call that asks for its address, not by the library's
+// other entry points; under EAGER loading every context that loads the
+// library reserves it.  Every device gets its own copy of the array in its
+// context.
 #include "pw_common.cuh"
 
 namespace pw {

@@ -841,6 +841,8 @@ static int setup(const pw_fwi_args *a, Setup &S) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   S.ztiles = ztiles;
   S.nsm = nsm;
+  if (getenv("PW_PFWI_VERBOSE"))
+    fprintf(stderr, "pfwi plan: padded %d x %d, ZW=%d ztiles=%d\n", S.pnz, S.pnx, S.zw, S.ztiles);
   return PW_OK;
 }
 

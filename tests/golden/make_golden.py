@@ -1,25 +1,35 @@
 """Generates the golden vectors under tests/golden/ by running the REFERENCE
 itself (chenyk1990/pywave compiled from its own sources into oracle/_ref by
 `make -C oracle ref`, with zero-initialised malloc).  Needs the reference
-sources (read in place) and is run by hand in the build container:
+sources, found through the PYWAVE_REF variable (the root of a pywave checkout;
+read in place), and is run by hand in the build container:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    export PYWAVE_REF=<pywave checkout>
+    make -C oracle ref && python tests/golden/make_golden.py [fixture ...]
 
-The fixtures are small .npz files; the tests compare both the oracle
-restatement (CPU) and the CUDA path (GPU) against them.
+With no fixture names every fixture is regenerated.  The fixtures are small
+.npz files; where a reference output is too large to keep (the 3-D and
+config-geometry runs), the fixture holds its SHA-256 digest, which a
+bit-exact result reproduces, plus a decimated copy for diagnostics.  The
+tests compare both the oracle restatement (CPU) and the CUDA path (GPU)
+against them.
 """
 from __future__ import annotations
 
 import ctypes as C
+import hashlib
 import importlib.util
 import os
 import sys
 
 import numpy as np
 
+from models import (BIG3D, BIG3D_BAND, BIG3D_TRI_JSNAP, MID, big3d_velocity, digest, mid_models,
+                    mid_wavelet, pfwi_scale_case)
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF_PY = "/root/reference/pywave"
+REF_PY = os.path.join(os.environ.get("PYWAVE_REF", ""), "pywave")
 REF_BUILD = os.path.join(ROOT, "oracle", "_ref")
 sys.path.insert(0, REF_BUILD)
 
@@ -61,9 +71,188 @@ def layered(nz, nx, vals, ifaces):
     return v
 
 
-def main():
+def make_afd3d_big(a3, R):
+    """afd3d forward and time reversal on an 80 x 72 x 64 interior with a
+    10-cell taper: the expanded grid (100 x 92 x 84) has 32-cell z runs and
+    4-column x runs free of taper and masks, so the untapered fast paths of
+    a warp-tiled 3-D step run, over several y chunks.  The reference's
+    outputs are kept as digests plus decimated copies."""
+    vel = big3d_velocity()
+    kw = dict(BIG3D, verb=0)
+    d, w = quiet(a3.afd3d, vel, **kw)
+    rick = []
+    for fq, t0, A in zip(kw["f"], kw["t"], kw["A"]):
+        r = np.zeros(kw["nt"], np.float32)
+        R.refdrv_ricker(kw["nt"], kw["dt"], fq, t0, A, r)
+        rick.append(r)
+    # one receiver group's traces (x-band 18..36) reversed, snapshots every 4 steps
+    dg = np.zeros_like(d)
+    b0, b1 = BIG3D_BAND
+    dg[:, b0:b1, :] = d[:, b0:b1, :]
+    _, wt = quiet(a3.afd3d, vel, nt=kw["nt"], dt=0.001, ax=kw["ax"], ay=kw["ay"], az=kw["az"],
+                  jsnap=BIG3D_TRI_JSNAP, dat=dg, tri=True, verb=0, nbt=10, ct=0.02)
+    np.savez_compressed(os.path.join(HERE, "afd3d_big.npz"), vel_digest=digest(vel),
+                        rick=np.stack(rick), traces_digest=digest(d), snaps_digest=digest(w),
+                        tri_snaps_digest=digest(wt), traces_dec=d[::3, ::4, ::4],
+                        snaps_last_dec=w[::4, ::4, ::4, -1], tri_last_dec=wt[::4, ::4, ::4, 0],
+                        snaps_shape=np.array(w.shape), tri_shape=np.array(wt.shape))
+
+
+def _fwi_parr(par):
+    # the driver's parameter layout (oracle/ref_driver.c fill_acpar)
+    return np.array([par[k] for k in ("nz", "nx", "dz", "dx", "oz", "ox", "nt", "dt", "ot", "ns",
+                                      "ds", "os", "nb", "coef", "f0", "acqui_type", "interval")],
+                    np.float32)
+
+
+def _fwi_case(R, vt, vs, par, wav):
+    """Reference forward data of vt and gradient_av at vs (rect 1 and 3)."""
+    nz, nx, nt, ns = par["nz"], par["nx"], par["nt"], par["ns"]
+    parr = _fwi_parr(par)
+    q = np.full(nz * nx, 1e4, np.float32)
+    data = np.zeros(ns * nx * nt, np.float32)
+    quiet(R.refdrv_forward, parr, np.ascontiguousarray(vt.flatten(order="F")), q, wav.copy(), data)
+    out = {}
+    for rect in (1, 3):
+        g = np.zeros(nz * nx, np.float32)
+        fc = np.zeros(1, np.float32)
+        quiet(R.refdrv_gradient, parr, np.ascontiguousarray(vs.flatten(order="F")), q.copy(),
+              wav.copy(), data.copy(), rect, g, fc)
+        out[rect] = (g.reshape(nz, nx, order="F"), float(fc[0]))
+    # data [ns][nr][nt] -> (nt, nr, ns) as pfwi returns it
+    return data.reshape(nt, nx, ns, order="F"), out
+
+
+def make_pfwi_scale(R):
+    """pfwi forward and gradient_av at the geometry of the 300 x 600 FWI
+    benchmark (nb 60: a 420 x 720 padded grid) and on a 460 x 200 model
+    (580 x 320 padded, deeper than one z tile of a step kernel), 2 shots and
+    a reduced nt (models: models.pfwi_scale_case).  Outputs are kept as
+    digests plus decimated copies."""
+    for name in ("c4geo", "deep"):
+        vt, vs, par, wav = pfwi_scale_case(name)
+        data, g = _fwi_case(R, vt, vs, par, wav)
+        np.savez_compressed(os.path.join(HERE, f"pfwi_{name}.npz"),
+                            vtrue_digest=digest(vt), vstart_digest=digest(vs),
+                            data_digest=digest(data), data_dec=data[::5, ::10, :],
+                            grad1_digest=digest(g[1][0]), grad3_digest=digest(g[3][0]),
+                            grad1_dec=g[1][0][::5, ::5], fcost=g[1][1],
+                            **{"par_" + k: np.asarray(v) for k, v in par.items()})
+
+
+def make_pfwi_mid(pf, R):
+    """60 x 120, 4 shots, nt 800: the reference's raw gradient_av (rect 1,
+    with its first-call scaling) at the start model, for the cosine of the
+    exact adjoint against it, and 20 iterations of the reference's fwic
+    (pfwi mode 2) from the start model."""
+    vt, vs = mid_models()
+    wav = mid_wavelet(MID["nt"])
+    data, g = _fwi_case(R, vt, vs, MID, wav)
+    q = np.full(vt.shape, 1e4, np.float32)
+    vinv = quiet(pf.pfwi, vs, q, wav, None, data=data, mode=2, par=dict(MID))[1]
+    np.savez_compressed(os.path.join(HERE, "pfwi_mid.npz"), vtrue=vt, vstart=vs, wav=wav,
+                        data_digest=digest(data), grad_rect1=g[1][0], fcost=g[1][1], vinv=vinv,
+                        **{"par_" + k: np.asarray(v) for k, v in MID.items()})
+
+
+class _Recorder:
+    """Stands in for an extension module: records each call's arguments and
+    returns the real module's result."""
+
+    def __init__(self, real, names):
+        self.calls = []
+        self.real = real
+        for n in names:
+            setattr(self, n, self._wrap(n))
+        self.__all__ = list(names)
+
+    def _wrap(self, name):
+        def f(*args):
+            out = getattr(self.real, name)(*args)
+            self.calls.append((name, args, out))
+            return out
+        return f
+
+
+def make_dropin():
+    """The exact positional arguments the reference's own, unmodified Python
+    wrappers (pywave/afd2d.py:73, afd3d.py:77, pfwi.py:70,111) pass to their
+    extension modules, with digests of what the reference's modules return:
+    a replay through pywave_b200.afdcfun / pfwicfun tests the drop-in."""
+    import types
+    real_afd = importlib.import_module("afdcfun")
+    real_pf = importlib.import_module("pfwicfun")
+    rec_afd = _Recorder(real_afd, ["afd2dc", "afd3dc"])
+    rec_pf = _Recorder(real_pf, ["forward_modeling_ac", "fwic"])
+    saved = {k: sys.modules.get(k) for k in ("afdcfun", "pfwicfun")}
+    for name, rec in (("afdcfun", rec_afd), ("pfwicfun", rec_pf)):
+        m = types.ModuleType(name)
+        for n in rec.__all__:
+            setattr(m, n, getattr(rec, n))
+        m.__all__ = rec.__all__
+        sys.modules[name] = m
+    try:
+        a2, a3, pf = load("afd2d"), load("afd3d"), load("pfwi")
+        vel = layered(41, 51, [2000, 2500, 3100], [15, 28])
+        d, _ = quiet(a2.afd2d, vel, nt=300, dt=0.001, ax=[0, 20, 51], az=[0, 20, 41], ns=2,
+                     sx=[20, 31], sz=[10, 17], f=[10, 12], t=[0.1, 0.12], A=[1, 2], nbt=30,
+                     ct=0.01, jsnap=3, verb=0)
+        dg = np.zeros_like(d)
+        dg[:, 10:30] = d[:, 10:30]
+        quiet(a2.afd2d, vel, nt=300, dt=0.001, ax=[0, 20, 51], az=[0, 20, 41], jsnap=4, dat=dg,
+              tri=True, verb=0, nbt=30, ct=0.01)
+        rng = np.random.default_rng(0)
+        vel3 = (2000 + 300 * rng.random((24, 20, 22))).astype(np.float32)
+        d3, _ = quiet(a3.afd3d, vel3, nt=120, dt=0.001, ax=[0, 20, 20], ay=[0, 20, 22],
+                      az=[0, 20, 24], ns=2, sx=[8, 12], sy=[9, 11], sz=[10, 6], f=[12, 15],
+                      t=[0.03, 0.05], A=[1, 1.5], nbt=8, ct=0.02, jsnap=5, verb=0)
+        dg3 = np.zeros_like(d3)
+        dg3[:, 5:15, :] = d3[:, 5:15, :]
+        quiet(a3.afd3d, vel3, nt=120, dt=0.001, ax=[0, 20, 20], ay=[0, 20, 22], az=[0, 20, 24],
+              jsnap=4, dat=dg3, tri=True, verb=0, nbt=8, ct=0.02)
+        nz, nx, nt = 30, 50, 400
+        vt = layered(nz, nx, [2.0, 2.5, 3.0], [12, 22])
+        q = np.full((nz, nx), 1e4, np.float32)
+        tt = np.arange(nt) * 0.001
+        arg = (np.pi * 10 * (tt - 0.1)) ** 2
+        wav = ((1 - 2 * arg) * np.exp(-arg)).astype(np.float32)
+        par = dict(nz=nz, nx=nx, dz=0.01, dx=0.01, oz=0, ox=0, nt=nt, dt=0.001, ot=0, ns=3,
+                   ds=0.15, os=0.05, nb=20, coef=0.005, f0=10, acqui_type=1, interval=1, niter=2)
+        data = quiet(pf.pfwi, vt, q, wav, None, mode=1, par=dict(par))[0]
+        vs = np.full((nz, nx), 2.4, np.float32)
+        quiet(pf.pfwi, vs, q, wav, None, data=data, mode=2, par=dict(par))
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                sys.modules.pop(k, None)
+            else:
+                sys.modules[k] = v
+    out = {}
+    calls = rec_afd.calls + rec_pf.calls
+    for i, (name, args, res) in enumerate(calls):
+        out[f"c{i}_name"] = np.asarray(name)
+        out[f"c{i}_nargs"] = np.asarray(len(args))
+        for j, x in enumerate(args):
+            out[f"c{i}_a{j}"] = np.asarray(x)
+        out[f"c{i}_out_digest"] = np.asarray(digest(np.asarray(res)))
+        out[f"c{i}_out_shape"] = np.asarray(np.asarray(res).shape)
+        out[f"c{i}_out_dec"] = np.asarray(res).reshape(-1)[::97]
+    out["ncalls"] = np.asarray(len(calls))
+    np.savez_compressed(os.path.join(HERE, "dropin_calls.npz"), **out)
+
+
+def main(names=()):
     a2, a3, pf = load("afd2d"), load("afd3d"), load("pfwi")
     R = refdrv()
+    R.refdrv_forward.argtypes = [np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")] * 5
+    extra = {"afd3d_big": lambda: make_afd3d_big(a3, R), "pfwi_scale": lambda: make_pfwi_scale(R),
+             "pfwi_mid": lambda: make_pfwi_mid(pf, R), "dropin": make_dropin}
+    if names:
+        for n in names:
+            extra[n]()
+        return
+    for fn in extra.values():
+        fn()
     out = {}
 
     # ---- afd2d forward, 2 sources, snapshots ---------------------------
@@ -149,4 +338,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -1,0 +1,103 @@
+"""Seeded inputs shared by the golden-vector generator (make_golden.py, run
+against the reference) and the tests that replay them on the GPU.  Only
+numpy / scipy and the benchmark's own model generators: nothing here reads
+the reference.  Where a fixture keeps only a digest of a large reference
+output, the test rebuilds the inputs here and checks their digests first."""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+
+def digest(a) -> str:
+    """SHA-256 of an array's bytes in C order (dtype and shape as given)."""
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+# ---- afd3d on an 80 x 72 x 64 interior (untapered warp patches exist) ----
+BIG3D = dict(nt=60, dt=0.001, ax=[0, 20, 72], ay=[0, 20, 64], az=[0, 20, 80], ns=2, sx=[30, 41],
+             sy=[25, 38], sz=[40, 22], f=[25, 20], t=[0.012, 0.02], A=[1, 1.5], nbt=10, ct=0.02,
+             jsnap=20)
+BIG3D_BAND = (18, 36)   # x columns of the time-reversed receiver group
+BIG3D_TRI_JSNAP = 4
+
+
+def big3d_velocity():
+    """80 x 72 x 64 (z, x, y) velocity: a 2000 -> 2600 m/s depth gradient plus
+    seeded uniform noise of 200 m/s."""
+    rng = np.random.default_rng(11)
+    z = np.arange(80, dtype=np.float32)[:, None, None]
+    return (2000 + 600 * z / 79 + 200 * rng.random((80, 72, 64))).astype(np.float32)
+
+
+# ---- pfwi at the 300 x 600 FWI benchmark geometry and deeper ------------
+def shallow_anomaly(v, cz, cx, r, amp):
+    """v times (1 + amp * a Gaussian bump of radius r cells at (cz, cx)),
+    clipped to [1.5, 4.5] km/s: a perturbation that short records see."""
+    nz, nx = v.shape
+    z = np.arange(nz)[:, None]
+    x = np.arange(nx)[None, :]
+    bump = np.exp(-((z - cz) ** 2 + (x - cx) ** 2) / (2.0 * r * r))
+    return np.clip(v * (1.0 + amp * bump), 1.5, 4.5).astype(np.float32)
+
+
+def pfwi_scale_case(name):
+    """(vtrue, vstart, par, wavelet) of the pfwi scale fixtures.
+    c4geo: the 300 x 600 benchmark models (bench.fwi2d_models(7)), nb 60
+    (420 x 720 padded), 2 shots, nt 600.  deep: their left 200 columns
+    extended by repeating the last 160 rows to 460 x 200 (580 x 320 padded,
+    more than one z tile of the step kernel), 2 shots, nt 600.  The true
+    model gets a +10% anomaly 30 cells deep, which 0.6 s of data sees (the
+    benchmark's own anomalies lie deeper than such a record reaches)."""
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    import bench
+    vt, vs = bench.fwi2d_models(7)
+    if name == "c4geo":
+        nz, nx, nt = 300, 600, 600
+    elif name == "deep":
+        nz, nx, nt = 460, 200, 600
+        vt = np.ascontiguousarray(np.concatenate([vt[:, :200], vt[-160:, :200]], axis=0))
+        vs = np.ascontiguousarray(np.concatenate([vs[:, :200], vs[-160:, :200]], axis=0))
+    else:
+        raise KeyError(name)
+    vt = shallow_anomaly(vt, 30, nx // 2, 12, 0.1)
+    par = dict(nz=nz, nx=nx, dz=0.01, dx=0.01, oz=0.0, ox=0.0, nt=nt, dt=0.001, ot=0.0, ns=2,
+               ds=nx * 0.01 / 2, os=nx * 0.01 / 4, nb=60, coef=0.005, f0=10.0, acqui_type=1,
+               interval=1)
+    return vt, vs, par, bench.fwi2d_wavelet(nt)
+
+
+# ---- pfwi 60 x 120, 4 shots, nt 800: gradient cosine and 20 L-BFGS steps -
+MID = dict(nz=60, nx=120, dz=0.01, dx=0.01, oz=0.0, ox=0.0, nt=800, dt=0.001, ot=0.0, ns=4,
+           ds=0.3, os=0.15, nb=30, coef=0.005, f0=10.0, acqui_type=1, interval=1, niter=20)
+
+
+def mid_models():
+    """60 x 120 models at 10 m (km units): 4 seeded layers in [1.8, 3.2] km/s
+    with a +8% Gaussian anomaly (true) and the true model smoothed with
+    sigma 6 points (start)."""
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(5)
+    nz, nx = 60, 120
+    z = np.arange(nz)[:, None] + np.zeros((1, nx))
+    x = np.zeros((nz, 1)) + np.arange(nx)[None, :]
+    ifaces = np.sort(rng.choice(np.arange(10, nz - 5), 3, replace=False))
+    vals = np.sort(rng.uniform(1.8, 3.2, 4))
+    v = np.full((nz, nx), vals[0])
+    for val, zi in zip(vals[1:], ifaces):
+        v[z >= zi] = val
+    v *= 1.0 + 0.08 * np.exp(-((z - 35) ** 2 + (x - 60) ** 2) / (2 * 8.0 ** 2))
+    v = v.astype(np.float32)
+    return v, gaussian_filter(v.astype(np.float64), 6.0).astype(np.float32)
+
+
+def mid_wavelet(nt):
+    t = np.arange(nt) * 0.001 - 0.12
+    a = (np.pi * 10.0 * t) ** 2
+    return ((1 - 2 * a) * np.exp(-a)).astype(np.float32)

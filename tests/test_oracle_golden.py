@@ -124,3 +124,57 @@ def test_exact_adjoint_matches_finite_differences(golden, oracle):
         fd = (oracle.pfwi_misfit(vp, g["wav"], g["data"], weight=W, **kw) -
               oracle.pfwi_misfit(vm, g["wav"], g["data"], weight=W, **kw)) / (2 * h)
         assert abs(fd - ge[iz, ix]) <= 1e-5 * abs(ge).max() + 1e-4 * abs(fd)
+
+
+# ---- fixtures kept as digests of the reference's outputs (larger runs) ----
+
+def _models():
+    import os
+    import sys
+    from conftest import ROOT
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import models
+    return models
+
+
+def test_afd3d_big_bit_exact_vs_reference_digests(golden, oracle):
+    """80 x 72 x 64 interior with nbt 10 (the size whose untapered warp
+    patches the GPU tests exercise): forward traces, snapshots and the
+    time reversal of one x-band group reproduce the reference's digests."""
+    M = _models()
+    g = golden("afd3d_big")
+    vel = M.big3d_velocity()
+    assert M.digest(vel) == str(g["vel_digest"])
+    B = M.BIG3D
+    src = dict(sx=B["sx"], sy=B["sy"], sz=B["sz"], f=B["f"], t=B["t"], A=B["A"])
+    d, w = oracle.afd(vel, B["nt"], B["dt"], (20., 20., 20.), nbt=B["nbt"], ct=B["ct"], src=src,
+                      jsnap=B["jsnap"], rick=g["rick"])
+    assert M.digest(d) == str(g["traces_digest"]) and M.digest(w) == str(g["snaps_digest"])
+    dg = np.zeros_like(d)
+    b0, b1 = M.BIG3D_BAND
+    dg[:, b0:b1, :] = d[:, b0:b1, :]
+    _, wt = oracle.afd(vel, B["nt"], B["dt"], (20., 20., 20.), nbt=B["nbt"], ct=B["ct"], tri=True,
+                       dat=dg, jsnap=M.BIG3D_TRI_JSNAP)
+    assert M.digest(wt) == str(g["tri_snaps_digest"])
+
+
+@pytest.mark.parametrize("name", ["c4geo", "deep"])
+def test_pfwi_scale_bit_exact_vs_reference_digests(golden, oracle, name):
+    """pfwi forward data and gradient_av (rect 1 and 3, with the first-call
+    scale) at the 300 x 600 benchmark geometry and on the 460 x 200 model
+    reproduce the reference's digests; the misfit equals the reference's."""
+    M = _models()
+    g = golden("pfwi_" + name)
+    vt, vs, par, wav = M.pfwi_scale_case(name)
+    assert M.digest(vt) == str(g["vtrue_digest"]) and M.digest(vs) == str(g["vstart_digest"])
+    geo = oracle.pfwi_geometry(par["nz"], par["nx"], par["dz"], par["dx"], 0, 0, par["ns"],
+                               par["ds"], par["os"], par["nb"])
+    kw = dict(nb=par["nb"], coef=par["coef"], dz=par["dz"], dx=par["dx"], dt=par["dt"], geo=geo,
+              ns=par["ns"])
+    d = oracle.pfwi_forward(vt, wav, **kw)
+    assert M.digest(d) == str(g["data_digest"])
+    gr, f = oracle.pfwi_gradient_ref(vs, wav, d, **kw)
+    assert f == float(g["fcost"])
+    p1, _ = oracle.pfwi_postprocess(gr, rect=1)
+    p3, _ = oracle.pfwi_postprocess(gr, rect=3)
+    assert M.digest(p1) == str(g["grad1_digest"]) and M.digest(p3) == str(g["grad3_digest"])
