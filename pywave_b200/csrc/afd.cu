@@ -33,6 +33,9 @@
 // all groups.
 #include "pw_common.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -85,9 +88,10 @@ struct StepArgs {
   int nbz, nbx, nby, nz1, nx1, ny1;  // interior = [nb, nb+n1) per kernel axis
   float *wfd;                  // this step's snapshot [ny1][nx1][nz1] (group 0) or null
   float *img;                  // image accumulator (field layout) or null
-  // warp-plane counts of the 3-D step paths, or null (tile_kernel only):
-  // [0] TRI fast, [1] TRI full, [2..5] forward paths 0..3
+  // warp-plane counts of the 3-D step paths, or null (warp-tile kernels
+  // only): [0..3] TRI paths 0..3, [4..7] forward paths 0..3
   unsigned long long *stats;
+  int *err;  // set to nonzero by a warp-tile kernel whose bounded wait gave up
 };
 
 __device__ __forceinline__ float el(const float4 &v, int e) {
@@ -612,25 +616,238 @@ __global__ void __launch_bounds__(MARCH_MAXT) batch_kernel(const StepArgs *args,
   march_body<true, false, false>(sa, item.y % sa.nzc, item.y / sa.nzc, ring);
 }
 
-// Warp-tile kernel (3-D): each warp owns an 8-slot x 4-column patch of one
-// group's field and marches it along y.  Per plane the warp copies its patch
-// with a 1-slot z halo and 2-column x halo (10 x 8 float4) into a private
-// ring in shared memory with cp.async, so every A value is fetched from L2
-// 80/32 = 2.5 times instead of once per neighbour use; the lanes read their
-// z and x neighbours there after the warp's own cp.async wait and a
-// __syncwarp (no CTA barrier).  The ring holds planes y .. y+2 plus
-// TILE_NS - 3 in flight; the lead plane's centre (y+2) feeds the register
-// queue.  Each lane's B and vv cells ride in the same ring, copied with the
-// A patch of their plane (TILE_NS - 1 planes ahead of their use).  Groups of a TRI launch are separate warps of
-// the CTA; the TRI image of an imaging step is formed afterwards by
-// image_kernel.
+// Warp-tile kernels (3-D): each warp owns an 8-slot x 4-column patch of one
+// group's field and marches it along y.  Per plane the warp stages its patch
+// with a 1-slot z halo and 2-column x halo (10 x 8 float4) in a private ring
+// in shared memory, so every A value is fetched from L2 80/32 = 2.5 times
+// instead of once per neighbour use; the lanes read their z and x neighbours
+// there after a warp-level wait (no CTA barrier).  The ring holds planes
+// y .. y+2 plus TILE_NS - 3 in flight; the lead plane's centre (y+2) feeds
+// the register queue.  Each lane's B and vv cells ride in the same ring slot
+// as the A patch of their plane (TILE_NS - 1 planes ahead of their use).
+// Two ways to fill the ring:
+//   tile_kernel      every lane issues 16-byte cp.async copies (its share of
+//                    the patch plus its B and vv cells);
+//   tile_kernel_tma  one lane issues three TMA tile loads per plane (the
+//                    10 x 8 float4 A box, the 8 x 4 float4 B and vv boxes),
+//                    completed on the slot's mbarrier; the tensor maps cover
+//                    this GPU's own field buffers only (no multicast).
+// Groups of a TRI launch are separate warps of the CTA; the TRI image of an
+// imaging step is formed afterwards by image_kernel.
 constexpr int TILE_ZW = 8, TILE_XW = 4;                      // warp patch: z slots x x columns
 constexpr int TILE_TZ = TILE_ZW + 2, TILE_TX = TILE_XW + 4;  // with halos
 constexpr int TILE_TP = TILE_TZ * TILE_TX;                   // float4 per plane
 constexpr int TILE_NS = 5;                                   // ring planes per warp
 constexpr int TILE_MAXT = 512;
 constexpr int TILE_CPL = (TILE_TP + 31) / 32;                // copies per lane per plane
-constexpr int TILE_WS = TILE_NS * (TILE_TP + 64);            // ring float4 per warp
+constexpr int TILE_SLOT = TILE_TP + 64;                      // float4 per ring slot: A, B, vv
+constexpr int TILE_WS = TILE_NS * TILE_SLOT;                 // ring float4 per warp
+
+// Per-warp constants of the warp-tile kernels.
+struct TileLane {
+  int lane, gi, slot, ix, iz0, s0, c0;
+  bool valid, live;
+  long long base;  // this lane's float4 in plane 0 (field offset), or a safe one
+  float wz4[4], wzx[4], wx;
+  bool lzm[4], keep[4], lxm;
+  bool warp_plain, warp_taper_zx, warp_edge_zx, rec_zx, warp_rec, in_zx;
+  int erz, ci;
+};
+
+__device__ __forceinline__ void tile_lane_setup(const StepArgs &a, TileLane &L) {
+  const Geo &g = a.g;
+  const unsigned full = 0xffffffffu;
+  const int t = threadIdx.x, w = t >> 5;
+  L.lane = t & 31;
+  const int G = a.ngroups;
+  L.gi = w % G;
+  const int wt = w / G;
+  const int wzi = wt % a.WZ, wxi = wt / a.WZ;
+  const int zl = L.lane % TILE_ZW, xl = L.lane / TILE_ZW;
+  L.s0 = (blockIdx.x % a.nzc) * (a.WZ * TILE_ZW) + wzi * TILE_ZW;  // warp's first slot
+  L.c0 = (int)(blockIdx.x / a.nzc) * (a.WX * TILE_XW) + wxi * TILE_XW;
+  L.slot = L.s0 + zl;
+  L.ix = L.c0 + xl;
+  L.valid = L.slot < a.S && L.ix < g.nx;
+  L.iz0 = 4 * L.slot - HZ;
+  L.live = L.valid && L.slot >= 1 && L.iz0 < g.nz;
+  const long long safe = g.sx * g.hx + g.sy * g.hy;  // slot 0, column 0: in range for every plane
+  L.base = L.valid ? 4LL * L.slot + g.sx * (L.ix + g.hx) + g.sy * g.hy : safe;
+  bool lane_taper = false, lane_plain = true;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int iz = L.iz0 + e;
+    L.wz4[e] = (L.live && iz < g.nz) ? a.wz[iz] : 1.f;
+    L.lzm[e] = iz >= g.lz0 && iz < g.lz1;
+    L.keep[e] = iz < g.nz;
+    lane_taper |= L.wz4[e] != 1.f;
+    lane_plain &= L.lzm[e] && L.keep[e];
+  }
+  L.wx = L.live ? a.wx[L.ix] : 1.f;
+  L.lxm = L.ix >= g.lx0 && L.ix < g.lx1;
+  lane_taper |= L.wx != 1.f;
+  lane_plain &= L.lxm;
+  // warp-uniform: every live lane free of masks, no lane tapered in z or x
+  L.warp_plain = __all_sync(full, !L.live || lane_plain);
+  L.warp_taper_zx = __any_sync(full, L.live && lane_taper);
+  // z-x edge cells (tapered along both z and x) need the factors one by one;
+  // elsewhere wz * wx has at most one factor != 1 and is exact
+  bool lane_edge = false;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    lane_edge |= L.wz4[e] != 1.f && L.wx != 1.f;
+    L.wzx[e] = fmul(L.wz4[e], L.wx);
+  }
+  L.warp_edge_zx = __any_sync(full, L.live && lane_edge);
+  L.erz = a.rz - L.iz0;
+  L.rec_zx = L.live && L.erz >= 0 && L.erz < 4 && L.ix >= a.rx0 && L.ix < a.rx0 + a.nrx;
+  L.warp_rec = __any_sync(full, L.rec_zx);
+  L.in_zx = L.ix >= a.nbx && L.ix < a.nbx + a.nx1;
+  L.ci = (xl + 2) * TILE_TZ + zl + 1;  // centre in the patch
+}
+
+// One plane y of a warp-tile kernel: the 4th-order Laplacian of the float4
+// q2 (z neighbours from the patch pc, x neighbours from the patch, y
+// neighbours q0..q4), the leapfrog update against pv = u_{k-1} as stored,
+// injection, the taper and the store, in the reference's float order.
+// Warp-uniform paths, exact because every skipped factor is exactly 1:
+// 0 no taper and no mask; 1 y taper only (x wy); 2 z / x taper only, no z-x
+// edge (x wz*wx); 3 everything face by face (masks, sources, z-x edges).
+// Returns the path taken.
+template <bool TRI, bool SNAP>
+__device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane &L, int y, float wy,
+                                          const float4 &q0, const float4 &q1, const float4 &q2,
+                                          const float4 &q3, const float4 &q4, const float4 *pc,
+                                          const float4 &pv, const float4 &vv4, float *pB) {
+  const Geo &g = a.g;
+  const int ci = L.ci, erz = L.erz, ix = L.ix, gi = L.gi;
+  const float4 xm1 = pc[ci - TILE_TZ], xp1 = pc[ci + TILE_TZ];
+  const float4 xm2 = pc[ci - 2 * TILE_TZ], xp2 = pc[ci + 2 * TILE_TZ];
+  const float2 Lf = reinterpret_cast<const float2 *>(pc + ci - 1)[1];  // (z, w)
+  const float2 Rf = reinterpret_cast<const float2 *>(pc + ci + 1)[0];  // (x, y)
+  const bool lyok = y >= g.ly0 && y < g.ly1;
+  const int nrec = a.nrx * a.nry;
+  bool rec_here = false, inj = false;
+  int r_idx = 0;
+  float dval = 0.f;
+  if (L.warp_rec) {
+    rec_here = L.rec_zx && y >= a.ry0 && y < a.ry0 + a.nry;
+    r_idx = rec_here ? (y - a.ry0) * a.nrx + (ix - a.rx0) : 0;
+    if (TRI && rec_here) {
+      inj = a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi;
+      if (inj) dval = a.tri_dat[(size_t)a.it * nrec + r_idx];
+    }
+  }
+  bool src_plane = false;
+  if (!TRI)
+    for (int s = 0; s < a.ns; s++) src_plane |= (y >= a.sy[s] - 1 && y <= a.sy[s] + 1);
+  const bool clean = L.warp_plain && lyok && !src_plane;
+  const int path = !clean ? 3
+                   : (!L.warp_taper_zx ? (wy == 1.f ? 0 : 1)
+                                       : (wy == 1.f && !L.warp_edge_zx ? 2 : 3));
+  float4 lp;  // Laplacian sums in the reference's order
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const float cv = el(q2, e);
+    const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
+    const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
+    const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
+    const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
+    float tt = fmul(fmul(a.c0, cv), a.k0);
+    tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
+    tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
+    tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
+    tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
+    tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
+    tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
+    set_el(lp, e, tt);
+  }
+  float4 res;
+  if (path == 0) {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const float cv = el(q2, e);
+      float v = fadd(cv, fsub(cv, el(pv, e)));
+      set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
+    }
+    if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
+  } else if (path == 1 || path == 2) {
+    float4 f;
+#pragma unroll
+    for (int e = 0; e < 4; e++) set_el(f, e, path == 1 ? wy : L.wzx[e]);
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const float cv = el(q2, e);
+      float v = fadd(cv, fsub(cv, fmul(el(pv, e), el(f, e))));
+      set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
+    }
+    // time reversal injects after the update and before the taper
+    if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
+#pragma unroll
+    for (int e = 0; e < 4; e++) set_el(res, e, fmul(el(res, e), el(f, e)));
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const float cv = el(q2, e);
+      const float lap = (L.lzm[e] && L.lxm && lyok) ? el(lp, e) : 0.f;
+      // prev = taper(u_{k-1} as stored), face by face
+      float p = fmul(el(pv, e), L.wz4[e]);
+      p = fmul(p, L.wx);
+      p = fmul(p, wy);
+      const float vve = el(vv4, e);
+      float v = fadd(cv, fsub(cv, p));
+      v = fadd(v, fmul(lap, vve));
+      if (!TRI && src_plane) {
+        const int iz = L.iz0 + e;
+        for (int s = 0; s < a.ns; s++) {
+          const int dz = iz - a.sz[s], dxs = ix - a.sx[s], dys = y - a.sy[s];
+          if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
+            const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
+            v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
+          }
+        }
+      }
+      set_el(res, e, v);
+    }
+    if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      float v = fmul(el(res, e), L.wz4[e]);
+      v = fmul(v, L.wx);
+      v = fmul(v, wy);
+      set_el(res, e, L.keep[e] ? v : 0.f);
+    }
+  }
+  if (L.live) *reinterpret_cast<float4 *>(pB) = res;
+  if (!TRI && rec_here && a.rec && gi == 0) a.rec[(size_t)a.it * nrec + r_idx] = el(res, erz);
+  if (SNAP) {
+    const bool interior = L.live && L.in_zx && y >= a.nby && y < a.nby + a.ny1;
+    if (a.wfd && gi == 0 && interior) {
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int iz = L.iz0 + e;
+        if (iz >= a.nbz && iz < a.nbz + a.nz1)
+          a.wfd[((size_t)(y - a.nby) * a.nx1 + (ix - a.nbx)) * a.nz1 + (iz - a.nbz)] = el(res, e);
+      }
+    }
+  }
+  return path;
+}
+
+// Per-warp path counts (16 bits per path; a launch gives a warp at most
+// ych < 65536 planes), flushed to a.stats at the end when requested:
+// [0..3] TRI paths 0..3, [4..7] forward paths 0..3.
+template <bool TRI>
+__device__ __forceinline__ void flush_path_counts(const StepArgs &a, int lane,
+                                                  unsigned long long pcount) {
+  if (a.stats != nullptr && lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const unsigned long long c = (pcount >> (16 * k)) & 0xffffull;
+      if (c) atomicAdd(a.stats + (TRI ? k : 4 + k), c);
+    }
+  }
+}
 
 template <bool TRI, bool SNAP>
 __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
@@ -638,33 +855,20 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
   constexpr int NS = TILE_NS, D = NS - 3;
   static_assert(NS == 5, "the y loop is unrolled by the queue length 5");
   const Geo &g = a.g;
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  const unsigned full = 0xffffffffu;
-  const int G = a.ngroups;
-  const int gi = w % G;
-  const int wt = w / G;
-  const int wzi = wt % a.WZ, wxi = wt / a.WZ;
-  const int zl = lane % TILE_ZW, xl = lane / TILE_ZW;
-  const int s0 = (blockIdx.x % a.nzc) * (a.WZ * TILE_ZW) + wzi * TILE_ZW;  // warp's first slot
-  const int c0 = (int)(blockIdx.x / a.nzc) * (a.WX * TILE_XW) + wxi * TILE_XW;
-  const int slot = s0 + zl, ix = c0 + xl;
-  const bool valid = slot < a.S && ix < g.nx;
-  const int iz0 = 4 * slot - HZ;
-  const bool live = valid && slot >= 1 && iz0 < g.nz;
+  TileLane L;
+  tile_lane_setup(a, L);
+  const int lane = L.lane, w = threadIdx.x >> 5;
   const float *A = a.cur[0];
   float *B = a.nxt[0];
 #pragma unroll
   for (int k = 1; k < MAXG; k++)
-    if (gi == k) {
+    if (L.gi == k) {
       A = a.cur[k];
       B = a.nxt[k];
     }
   const long long sx = g.sx, sy = g.sy;
-  const long long safe = sx * g.hx + sy * g.hy;  // slot 0, column 0: in range for every plane
-  const long long base = valid ? 4LL * slot + sx * (ix + g.hx) + sy * g.hy : safe;
-  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  float4 *ring = tsm + (size_t)w * TILE_WS;  // NS A patches, then NS planes of B and vv per lane
-  float4 *rbv = ring + NS * TILE_TP;
+  const long long safe = sx * g.hx + sy * g.hy;
+  float4 *ring = tsm + (size_t)w * TILE_WS;  // NS slots of [A patch, B, vv]
   const int y0 = blockIdx.y * a.ych;
   const int y1 = min(g.ny, y0 + a.ych);
 
@@ -676,18 +880,18 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
   for (int k = 0; k < TILE_CPL; k++) {
     const int j = lane + 32 * k;
     const int tz = j % TILE_TZ, tx = j / TILE_TZ;
-    const int sl = s0 - 1 + tz, col = c0 - 2 + tx;
+    const int sl = L.s0 - 1 + tz, col = L.c0 - 2 + tx;
     c_ok[k] = j < TILE_TP && sl >= 0 && sl < a.S && col >= -g.hx && col < g.nx + g.hx;
     cpp[k] = A + (c_ok[k] ? 4LL * sl + sx * (col + g.hx) + sy * g.hy : safe) + sy * y0;
   }
   int next_plane = y0;
-  const float *cB = B + base + sy * y0, *cV = a.vv + base + sy * y0;
+  const float *cB = B + L.base + sy * y0, *cV = a.vv + L.base + sy * y0;
   // copies of plane next_plane into ring slot rs: the A patch, and this lane's
   // B and vv cells (used when next_plane is updated); planes past y1 + 1 are
   // not needed
   auto issue = [&](int rs) {
     if (next_plane <= y1 + 1) {
-      float4 *dst = ring + rs * TILE_TP;
+      float4 *dst = ring + rs * TILE_SLOT;
 #pragma unroll
       for (int k = 0; k < TILE_CPL; k++) {
         const int j = lane + 32 * k;
@@ -695,9 +899,8 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
         cpp[k] += sy;
       }
       if (next_plane < y1) {
-        const int bs = rs * 64;
-        cp16(rbv + bs + lane, cB, valid);
-        cp16(rbv + bs + 32 + lane, cV, valid);
+        cp16(dst + TILE_TP + lane, cB, L.valid);
+        cp16(dst + TILE_TP + 32 + lane, cV, L.valid);
       }
       cB += sy;
       cV += sy;
@@ -706,50 +909,12 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
     cp_commit();
   };
 
-  float wz4[4];
-  bool lzm[4], keep[4];
-  bool lane_taper = false, lane_plain = true;
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    const int iz = iz0 + e;
-    wz4[e] = (live && iz < g.nz) ? a.wz[iz] : 1.f;
-    lzm[e] = iz >= g.lz0 && iz < g.lz1;
-    keep[e] = iz < g.nz;
-    lane_taper |= wz4[e] != 1.f;
-    lane_plain &= lzm[e] && keep[e];
-  }
-  const float wx = live ? a.wx[ix] : 1.f;
-  const bool lxm = ix >= g.lx0 && ix < g.lx1;
-  lane_taper |= wx != 1.f;
-  lane_plain &= lxm;
-  // warp-uniform: every live lane free of masks, no lane tapered in z or x
-  const bool warp_plain = __all_sync(full, !live || lane_plain);
-  const bool warp_taper_zx = __any_sync(full, live && lane_taper);
-  // z-x edge cells (tapered along both z and x) need the factors one by one;
-  // elsewhere wz * wx has at most one factor != 1 and is exact
-  bool lane_edge = false;
-  float wzx[4];
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    lane_edge |= wz4[e] != 1.f && wx != 1.f;
-    wzx[e] = fmul(wz4[e], wx);
-  }
-  const bool warp_edge_zx = __any_sync(full, live && lane_edge);
-  const int erz = a.rz - iz0;
-  const bool rec_zx = live && erz >= 0 && erz < 4 && ix >= a.rx0 && ix < a.rx0 + a.nrx;
-  const bool warp_rec = __any_sync(full, rec_zx);
-  const bool in_zx = ix >= a.nbx && ix < a.nbx + a.nx1;
-  const int nrec = a.nrx * a.nry;
-  const int ci = (xl + 2) * TILE_TZ + zl + 1;  // centre in the patch
-
-  // per-warp path counts (16 bits per path; a launch gives a warp at most
-  // ych < 65536 planes), flushed to a.stats at the end when requested
   unsigned long long pcount = 0;
   // queue: plane y-2+k sits in q[(y - y0 + k) % 5]
   float4 q[5];
-  q[4] = zero4;
-  const float *pA = A + base;
-  float *pB = B + base + sy * y0;
+  q[4] = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float *pA = A + L.base;
+  float *pB = B + L.base + sy * y0;
   q[0] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 2)));
   q[1] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 1)));
   q[2] = __ldg(reinterpret_cast<const float4 *>(pA + sy * y0));
@@ -766,208 +931,189 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
         issue((u + 2 + D) % NS);  // plane y + 2 + D into the slot plane y - 1 left
         cp_wait<D>();
         __syncwarp();
-        const float4 *pc = ring + u * TILE_TP;
-        q[(u + 4) % NS] = ring[((u + 2) % NS) * TILE_TP + ci];
-        const float4 q0 = q[u], q1 = q[(u + 1) % NS], q2 = q[(u + 2) % NS],
-                     q3 = q[(u + 3) % NS], q4 = q[(u + 4) % NS];
-        const float4 pv = rbv[u * 64 + lane], vv4 = rbv[u * 64 + 32 + lane];
-        const float4 xm1 = pc[ci - TILE_TZ], xp1 = pc[ci + TILE_TZ];
-        const float4 xm2 = pc[ci - 2 * TILE_TZ], xp2 = pc[ci + 2 * TILE_TZ];
-        const float2 Lf = reinterpret_cast<const float2 *>(pc + ci - 1)[1];  // (z, w)
-        const float2 Rf = reinterpret_cast<const float2 *>(pc + ci + 1)[0];  // (x, y)
+        const float4 *slot = ring + u * TILE_SLOT;
+        q[(u + 4) % NS] = ring[((u + 2) % NS) * TILE_SLOT + L.ci];
         const float wy = wyn;
         if (y + 1 < y1) wyn = __ldg(a.wy + y + 1);
-        const bool lyok = y >= g.ly0 && y < g.ly1;
-        bool rec_here = false, inj = false;
-        int r_idx = 0;
-        float dval = 0.f;
-        if (warp_rec) {
-          rec_here = rec_zx && y >= a.ry0 && y < a.ry0 + a.nry;
-          r_idx = rec_here ? (y - a.ry0) * a.nrx + (ix - a.rx0) : 0;
-          if (TRI && rec_here) {
-            inj = a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi;
-            if (inj) dval = a.tri_dat[(size_t)a.it * nrec + r_idx];
-          }
-        }
-        bool src_plane = false;
-        if (!TRI)
-          for (int s = 0; s < a.ns; s++) src_plane |= (y >= a.sy[s] - 1 && y <= a.sy[s] + 1);
-        float4 res;
-        if constexpr (TRI) {
-          // time reversal: one fast path (no taper, no mask) and the full one
-          const bool fast = warp_plain && lyok && !warp_taper_zx && wy == 1.f && !inj && !src_plane;
-          pcount += fast ? 1ull : (1ull << 16);
-          if (fast) {
-  #pragma unroll
-            for (int e = 0; e < 4; e++) {
-              const float cv = el(q2, e);
-              const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
-              const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
-              const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
-              const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
-              float tt = fmul(fmul(a.c0, cv), a.k0);
-              tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
-              tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
-              tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
-              tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
-              tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-              tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-              float v = fadd(cv, fsub(cv, el(pv, e)));
-              v = fadd(v, fmul(tt, el(vv4, e)));
-              set_el(res, e, v);
-            }
-          } else {
-  #pragma unroll
-            for (int e = 0; e < 4; e++) {
-              const float cv = el(q2, e);
-              const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
-              const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
-              const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
-              const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
-              float tt = fmul(fmul(a.c0, cv), a.k0);
-              tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
-              tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
-              tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
-              tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
-              tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-              tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-              const float lap = (lzm[e] && lxm && lyok) ? tt : 0.f;
-              // prev = taper(u_{k-1} as stored); x1.0 outside the faces is exact
-              float p = fmul(el(pv, e), wz4[e]);
-              p = fmul(p, wx);
-              p = fmul(p, wy);
-              const float vve = el(vv4, e);
-              float v = fadd(cv, fsub(cv, p));
-              v = fadd(v, fmul(lap, vve));
-              if (TRI) {
-                if (inj && e == erz) v = fadd(v, fmul(vve, dval));
-              } else if (src_plane) {
-                const int iz = iz0 + e;
-                for (int s = 0; s < a.ns; s++) {
-                  const int dz = iz - a.sz[s], dxs = ix - a.sx[s], dys = y - a.sy[s];
-                  if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
-                    const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
-                    v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
-                  }
-                }
-              }
-              v = fmul(v, wz4[e]);
-              v = fmul(v, wx);
-              v = fmul(v, wy);
-              set_el(res, e, keep[e] ? v : 0.f);
-            }
-          }
-        } else {
-          // forward modelling: two more exact taper paths (measured faster here)
-          // warp-uniform path: no masks and at most one taper family -> FAST
-          // (none), YT (y only: x wy), ZXT (z / x only, no z-x edge: x wz*wx);
-          // FULL otherwise.  The multiplications equal the reference's
-          // face-by-face products because the skipped factors are exactly 1.
-          constexpr bool MULTI = true;
-          const bool clean = warp_plain && lyok && !src_plane;
-          const int path = !clean ? 3
-                           : (!warp_taper_zx ? (wy == 1.f ? 0 : (MULTI ? 1 : 3))
-                                             : (MULTI && wy == 1.f && !warp_edge_zx ? 2 : 3));
-          pcount += 1ull << (16 * path);
-          float4 lp;  // Laplacian sums in the reference's order
-  #pragma unroll
-          for (int e = 0; e < 4; e++) {
-            const float cv = el(q2, e);
-            const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
-            const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
-            const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
-            const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
-            float tt = fmul(fmul(a.c0, cv), a.k0);
-            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
-            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
-            tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
-            tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
-            tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-            tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-            set_el(lp, e, tt);
-          }
-          if (path == 0) {
-  #pragma unroll
-            for (int e = 0; e < 4; e++) {
-              const float cv = el(q2, e);
-              float v = fadd(cv, fsub(cv, el(pv, e)));
-              set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
-            }
-            if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
-          } else if (MULTI && (path == 1 || path == 2)) {
-            float4 f;
-  #pragma unroll
-            for (int e = 0; e < 4; e++) set_el(f, e, path == 1 ? wy : wzx[e]);
-  #pragma unroll
-            for (int e = 0; e < 4; e++) {
-              const float cv = el(q2, e);
-              float v = fadd(cv, fsub(cv, fmul(el(pv, e), el(f, e))));
-              set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
-            }
-            if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
-  #pragma unroll
-            for (int e = 0; e < 4; e++) set_el(res, e, fmul(el(res, e), el(f, e)));
-          } else {
-  #pragma unroll
-            for (int e = 0; e < 4; e++) {
-              const float cv = el(q2, e);
-              const float lap = (lzm[e] && lxm && lyok) ? el(lp, e) : 0.f;
-              // prev = taper(u_{k-1} as stored), face by face
-              float p = fmul(el(pv, e), wz4[e]);
-              p = fmul(p, wx);
-              p = fmul(p, wy);
-              const float vve = el(vv4, e);
-              float v = fadd(cv, fsub(cv, p));
-              v = fadd(v, fmul(lap, vve));
-              if (!TRI && src_plane) {
-                const int iz = iz0 + e;
-                for (int s = 0; s < a.ns; s++) {
-                  const int dz = iz - a.sz[s], dxs = ix - a.sx[s], dys = y - a.sy[s];
-                  if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
-                    const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
-                    v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
-                  }
-                }
-              }
-              set_el(res, e, v);
-            }
-            if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
-  #pragma unroll
-            for (int e = 0; e < 4; e++) {
-              float v = fmul(el(res, e), wz4[e]);
-              v = fmul(v, wx);
-              v = fmul(v, wy);
-              set_el(res, e, keep[e] ? v : 0.f);
-            }
-          }
-        }
-        if (live) *reinterpret_cast<float4 *>(pB) = res;
-        if (!TRI && rec_here && a.rec && gi == 0) a.rec[(size_t)a.it * nrec + r_idx] = el(res, erz);
-        if (SNAP) {
-          const bool interior = live && in_zx && y >= a.nby && y < a.nby + a.ny1;
-          if (a.wfd && gi == 0 && interior) {
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-              const int iz = iz0 + e;
-              if (iz >= a.nbz && iz < a.nbz + a.nz1)
-                a.wfd[((size_t)(y - a.nby) * a.nx1 + (ix - a.nbx)) * a.nz1 + (iz - a.nbz)] =
-                    el(res, e);
-            }
-          }
-        }
+        const int path = tile_plane<TRI, SNAP>(a, L, y, wy, q[u], q[(u + 1) % NS],
+                                               q[(u + 2) % NS], q[(u + 3) % NS],
+                                               q[(u + 4) % NS], slot, slot[TILE_TP + lane],
+                                               slot[TILE_TP + 32 + lane], pB);
+        pcount += 1ull << (16 * path);
         pB += sy;
         __syncwarp();  // the ring slot refilled next iteration was read above
       }
     }
   }
   cp_wait_all();
-  if (a.stats != nullptr && lane == 0) {
+  flush_path_counts<TRI>(a, lane, pcount);
+}
+
+// ---- TMA ring -----------------------------------------------------------
+// Tensor maps of one step launch (3-D field layout, float32, zero fill out of
+// bounds): the A box (40 z floats x 8 columns x 1 plane) of each group's
+// current field, the B box (32 x 4 x 1) of each group's previous field and
+// of vv.  Dimensions {lz, nx + 2 hx, ny + 2 hy} in array coordinates.
+struct TileMaps {
+  CUtensorMap a[MAXG];
+  CUtensorMap b[MAXG];
+  CUtensorMap v;
+};
+constexpr unsigned TILE_A_BYTES = TILE_TP * 16, TILE_BV_BYTES = 32 * 16;
+constexpr int TILE_WAIT_LIMIT = 1 << 20;  // try_wait rounds before a wait gives up
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(b)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(b)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *b, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(b)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the given phase of an mbarrier: false when it gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned phase) {
+  for (int n = 0; n < TILE_WAIT_LIMIT; n++)
+    if (mbar_try_wait(b, phase)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *m, int c0, int c1, int c2,
+                                          unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_addr(dst)),
+      "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+      : "memory");
+}
+
+template <bool TRI, bool SNAP>
+__global__ void __launch_bounds__(TILE_MAXT)
+    tile_kernel_tma(const StepArgs a, const __grid_constant__ TileMaps maps) {
+  extern __shared__ __align__(128) float4 tsm_tma[];
+  float4 *const tsm = tsm_tma;
+  constexpr int NS = TILE_NS, D = NS - 3;
+  static_assert(NS == 5, "the y loop is unrolled by the queue length 5");
+  const Geo &g = a.g;
+  TileLane L;
+  tile_lane_setup(a, L);
+  const int lane = L.lane, w = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const float *A = a.cur[0];
+  float *B = a.nxt[0];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const unsigned long long c = (pcount >> (16 * k)) & 0xffffull;
-      if (c) atomicAdd(a.stats + (TRI ? k : 2 + k), c);
+  for (int k = 1; k < MAXG; k++)
+    if (L.gi == k) {
+      A = a.cur[k];
+      B = a.nxt[k];
+    }
+  const long long sy = g.sy;
+  float4 *ring = tsm + (size_t)w * TILE_WS;  // NS slots of [A patch, B, vv]
+  unsigned long long *bars =
+      reinterpret_cast<unsigned long long *>(tsm + (size_t)nwarps * TILE_WS) + w * NS;
+  const int y0 = blockIdx.y * a.ych;
+  const int y1 = min(g.ny, y0 + a.ych);
+  const CUtensorMap *mA = &maps.a[L.gi], *mB = &maps.b[L.gi], *mV = &maps.v;
+  // box origins in array coordinates (z floats, x columns, y planes)
+  const int az = 4 * (L.s0 - 1), ax = L.c0 - 2 + g.hx, bz = 4 * L.s0, bx = L.c0 + g.hx;
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < NS; s++) mbar_init(bars + s, 1);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  __syncwarp();
+  int next_plane = y0;
+  // lane 0 loads plane next_plane into ring slot rs: the A box, and the B and
+  // vv boxes when next_plane is updated; planes past y1 + 1 are not needed
+  auto issue = [&](int rs) {
+    if (lane == 0 && next_plane <= y1 + 1) {
+      float4 *dst = ring + rs * TILE_SLOT;
+      const bool upd = next_plane < y1;
+      // the slot was last read by the whole warp (ordered by the __syncwarp
+      // that precedes this call); order those reads before the async writes
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      mbar_expect_tx(bars + rs, TILE_A_BYTES + (upd ? 2 * TILE_BV_BYTES : 0));
+      const int py = next_plane + g.hy;
+      tma_load3(dst, mA, az, ax, py, bars + rs);
+      if (upd) {
+        tma_load3(dst + TILE_TP, mB, bz, bx, py, bars + rs);
+        tma_load3(dst + TILE_TP + 32, mV, bz, bx, py, bars + rs);
+      }
+    }
+    next_plane++;
+  };
+  int waited = y0 - 1;  // last plane whose slot this warp has waited for
+  bool ok = true;
+  // wait for plane p (ring slot (p - y0) % NS, phase ((p - y0) / NS) & 1)
+  auto wait_plane = [&](int p) {
+    if (ok) {
+      const int k = p - y0;
+      ok = mbar_wait(bars + k % NS, (unsigned)((k / NS) & 1));
+      if (ok) waited = p;
+    }
+  };
+
+  unsigned long long pcount = 0;
+  float4 q[5];
+  q[4] = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float *pA = A + L.base;
+  float *pB = B + L.base + sy * y0;
+  q[0] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 2)));
+  q[1] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 1)));
+  q[2] = __ldg(reinterpret_cast<const float4 *>(pA + sy * y0));
+  q[3] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 + 1)));
+  float wyn = y0 < y1 ? __ldg(a.wy + y0) : 1.f;
+#pragma unroll
+  for (int j = 0; j < 2 + D; j++) issue(j);
+  wait_plane(y0);
+  wait_plane(y0 + 1);
+  ok = __all_sync(0xffffffffu, ok);
+
+  for (int yb = y0; yb < y1 && ok; yb += NS) {
+#pragma unroll
+    for (int u = 0; u < NS; u++) {
+      const int y = yb + u;
+      if (y < y1 && ok) {
+        issue((u + 2 + D) % NS);  // plane y + 2 + D into the slot plane y - 1 left
+        wait_plane(y + 2);
+        if (!__all_sync(0xffffffffu, ok)) {
+          ok = false;
+          break;
+        }
+        const float4 *slot = ring + u * TILE_SLOT;
+        q[(u + 4) % NS] = ring[((u + 2) % NS) * TILE_SLOT + L.ci];
+        const float wy = wyn;
+        if (y + 1 < y1) wyn = __ldg(a.wy + y + 1);
+        const int path = tile_plane<TRI, SNAP>(a, L, y, wy, q[u], q[(u + 1) % NS],
+                                               q[(u + 2) % NS], q[(u + 3) % NS],
+                                               q[(u + 4) % NS], slot, slot[TILE_TP + lane],
+                                               slot[TILE_TP + 32 + lane], pB);
+        pcount += 1ull << (16 * path);
+        pB += sy;
+        __syncwarp();  // the ring slot refilled next iteration was read above
+      }
     }
   }
+  if (!ok) {
+    // a wait gave up: report it, then let the loads still in flight land in
+    // this CTA's shared memory (bounded again) before the warp exits
+    if (lane == 0 && a.err) atomicOr(a.err, 1);
+    ok = true;
+    for (int p = waited + 1; p < next_plane && p <= y1 + 1 && ok; p++) wait_plane(p);
+  }
+  flush_path_counts<TRI>(a, lane, pcount);
 }
 
 // TRI image of one imaging step: img += prod_g u_g^2 over the interior cells
@@ -1109,6 +1255,7 @@ struct Plan {
   size_t smem;
   void *fn, *fn_snap;  // plain steps / snapshot and imaging steps
   bool tile;           // warp-tile kernel: TRI images by image_kernel
+  bool tma;            // warp-tile kernel with the TMA ring (takes TileMaps)
   int threads;
   int S, ZS, KX, nzc, WPC, WZ, WX;
 };
@@ -1214,28 +1361,45 @@ static int plan_march(bool tri, int G, int nsm, Plan &p) {
   return PW_OK;
 }
 
-template <bool TRI, bool SNAP>
+static size_t tile_smem(int threads, bool tma) {
+  const size_t nw = (size_t)threads / 32;
+  return nw * TILE_WS * sizeof(float4) + (tma ? nw * TILE_NS * sizeof(unsigned long long) : 0);
+}
+
+template <bool TRI, bool SNAP, bool TMA>
 static void *tile_ptr() {
-  void *f = (void *)tile_kernel<TRI, SNAP>;
+  void *f = TMA ? (void *)tile_kernel_tma<TRI, SNAP> : (void *)tile_kernel<TRI, SNAP>;
   static bool once = [f] {
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (TILE_MAXT / 32) * TILE_WS * (int)sizeof(float4));
+                         (int)tile_smem(TILE_MAXT, TMA));
     return true;
   }();
   (void)once;
   return f;
 }
 
-static size_t tile_smem(int threads) {
-  return (size_t)(threads / 32) * TILE_WS * sizeof(float4);
+static void *tile_fn(bool tri, bool snap, bool tma) {
+  if (tma) {
+    if (tri) return snap ? tile_ptr<true, true, true>() : tile_ptr<true, false, true>();
+    return snap ? tile_ptr<false, true, true>() : tile_ptr<false, false, true>();
+  }
+  if (tri) return snap ? tile_ptr<true, true, false>() : tile_ptr<true, false, false>();
+  return snap ? tile_ptr<false, true, false>() : tile_ptr<false, false, false>();
+}
+
+// Ring filling of the 3-D warp-tile kernels: TMA tile loads (default) or
+// per-lane cp.async copies (PW_AFD_TMA=0); both give identical results.
+static bool tile_use_tma() {
+  const char *e = getenv("PW_AFD_TMA");
+  return !(e && e[0] == '0');
 }
 
 // Tile of the 3-D warp-tile kernel: CTA = G groups x WZ x WX warps of 8 slots
 // x 4 columns, ych planes.  Same score as plan_march without the x-halo term
 // (every warp fetches its own halo).
-static int plan_tile(bool tri, int G, int nsm, Plan &p) {
+static int plan_tile(bool tri, int G, int nsm, bool tma, Plan &p) {
   const Geo &g = p.g;
-  void *fn = tri ? tile_ptr<true, false>() : tile_ptr<false, false>();
+  void *fn = tile_fn(tri, false, tma);
   const int S = g.lz / 4;
   const int live_slots = ceil_div(g.nz, 4);
   const double useful = (double)G * live_slots * g.nx * g.ny;
@@ -1250,7 +1414,7 @@ static int plan_tile(bool tri, int G, int nsm, Plan &p) {
     for (int WX = 1; G * WZ * WX * 32 <= TILE_MAXT; WX++) {
       if (fk && WX != fk) continue;
       const int threads = G * WZ * WX * 32;
-      const size_t smem = tile_smem(threads);
+      const size_t smem = tile_smem(threads, tma);
       int occ = 0;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) {
         cudaGetLastError();
@@ -1282,24 +1446,26 @@ static int plan_tile(bool tri, int G, int nsm, Plan &p) {
   }
   PW_CHECK(best > 0, PW_ERR_SHAPE, "no launchable tile for the step kernel");
   p.fn = fn;
-  p.fn_snap = tri ? tile_ptr<true, true>() : tile_ptr<false, true>();
+  p.fn_snap = tile_fn(tri, true, tma);
   p.tile = true;
+  p.tma = tma;
   p.S = S;
   p.WZ = bz;
   p.WX = bx;
   p.nzc = ceil_div(S, bz * TILE_ZW);
   p.ych = by;
   p.threads = G * bz * bx * 32;
-  p.smem = tile_smem(p.threads);
+  p.smem = tile_smem(p.threads, tma);
   p.grid = dim3((unsigned)(p.nzc * ceil_div(g.nx, bx * TILE_XW)), (unsigned)ceil_div(g.ny, by), 1);
   if (getenv("PW_AFD_VERBOSE"))
     fprintf(stderr,
-            "afd tile plan: G=%d S=%d nzc=%d WZ=%d WX=%d ych=%d threads=%d grid=%ux%u score=%.3f\n",
-            G, S, p.nzc, bz, bx, by, p.threads, p.grid.x, p.grid.y, best);
+            "afd tile plan: G=%d S=%d nzc=%d WZ=%d WX=%d ych=%d threads=%d grid=%ux%u score=%.3f "
+            "ring=%s\n",
+            G, S, p.nzc, bz, bx, by, p.threads, p.grid.x, p.grid.y, best, tma ? "tma" : "cp.async");
   return PW_OK;
 }
 
-static int make_plan(const pw_afd_args *a, bool tri, int G, Plan &p) {
+static int make_plan(const pw_afd_args *a, bool tri, int G, Plan &p, bool allow_tma = true) {
   PW_CHECK(a->dim == 2 || a->dim == 3, PW_ERR_SHAPE, "dim must be 2 or 3 (got %d)", a->dim);
   PW_CHECK(a->nz >= 1 && a->nx >= 1 && a->ny >= 1 && a->nt >= 1 && a->nbt >= 0, PW_ERR_SHAPE,
            "sizes must be positive (nz=%d nx=%d ny=%d nt=%d nbt=%d)", a->nz, a->nx, a->ny, a->nt,
@@ -1344,8 +1510,9 @@ static int make_plan(const pw_afd_args *a, bool tri, int G, Plan &p) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   p.S = p.ZS = p.KX = p.nzc = p.WPC = p.WZ = p.WX = 0;
+  p.tile = p.tma = false;
   if (two_d) PW_TRY(plan_march(tri, G, nsm, p));  // 2-D: no x neighbours to stage
-  else PW_TRY(plan_tile(tri, G, nsm, p));
+  else PW_TRY(plan_tile(tri, G, nsm, allow_tma && tile_use_tma(), p));
   return PW_OK;
 }
 
@@ -1482,6 +1649,54 @@ static bool plan_resident(const Geo &g, int G, bool tri, ResPlan &rp) {
   return false;
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once.
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      f = nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// Tensor map of one field-layout array of this GPU (z floats x columns incl.
+// halo x planes incl. halo) with a box of bz floats x bx columns x 1 plane.
+static int field_map(const Geo &g, const float *base, int bz, int bx, CUtensorMap *m) {
+  auto enc = encode_fn();
+  PW_CHECK(enc != nullptr, PW_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  const cuuint64_t dim[3] = {(cuuint64_t)g.lz, (cuuint64_t)(g.nx + 2 * g.hx), (cuuint64_t)g.py};
+  const cuuint64_t stride[2] = {(cuuint64_t)g.sx * 4, (cuuint64_t)g.sy * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)bx, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dim,
+                         stride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  PW_CHECK(r == CUDA_SUCCESS, PW_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return PW_OK;
+}
+
+// The two step launches' tensor maps: parity 0 reads buf0 as the current
+// field and buf1 as the previous one, parity 1 the other way round.
+static int tile_maps(const Geo &g, int G, float *const *buf0, float *const *buf1, const float *vv,
+                     TileMaps m[2]) {
+  for (int par = 0; par < 2; par++) {
+    memset(&m[par], 0, sizeof(TileMaps));
+    for (int i = 0; i < G; i++) {
+      PW_TRY(field_map(g, par ? buf1[i] : buf0[i], 4 * TILE_TZ, TILE_TX, &m[par].a[i]));
+      PW_TRY(field_map(g, par ? buf0[i] : buf1[i], 4 * TILE_ZW, TILE_XW, &m[par].b[i]));
+    }
+    PW_TRY(field_map(g, vv, 4 * TILE_ZW, TILE_XW, &m[par].v));
+  }
+  return PW_OK;
+}
+
 static int run(const pw_afd_args *a, int G, const int *group, const float *vel, const float *src,
                const float *wavelet, float *dat, float *wfd, float *img_out, int normalize,
                cudaStream_t st) {
@@ -1591,6 +1806,7 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   // PW_AFD_VERBOSE: also count which paths the 3-D step kernels took
   const bool want_stats = p.tile && getenv("PW_AFD_VERBOSE") != nullptr;
   const size_t o_stats = cv.add(want_stats ? 8 * sizeof(unsigned long long) : 0);
+  const size_t o_err = cv.add(p.tma ? 16 : 0);
 
   Workspace &ws = Workspace::for_current_device();
   std::lock_guard<std::mutex> lock(ws.mutex());
@@ -1709,6 +1925,9 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   s.nbz = p.kbz; s.nbx = p.kbx; s.nby = p.kby;
   s.nz1 = p.knz1; s.nx1 = p.knx1; s.ny1 = p.kny1;
   s.stats = want_stats ? at<unsigned long long>(base, o_stats) : nullptr;
+  s.err = p.tma ? at<int>(base, o_err) : nullptr;
+  TileMaps maps[2];
+  if (p.tma) PW_TRY(tile_maps(g, G, A, B, vv, maps));
   float *wfd_dev = wfd ? (host ? at<float>(base, o_wfd) : wfd) : nullptr;
   void *fn = p.fn;
   const int threads = p.threads;
@@ -1765,7 +1984,7 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
     s.wfd = (snap && wfd_dev) ? wfd_dev + (size_t)(it / a->jsnap) * nvel : nullptr;
     const bool img_step = snap && img;
     s.img = (img_step && !p.tile) ? img : nullptr;
-    void *args[] = {(void *)&s};
+    void *args[] = {(void *)&s, (void *)&maps[k & 1]};
     void *f = (s.wfd || s.img) ? p.fn_snap : fn;
     PW_CUDA(cudaLaunchKernel(f, p.grid, dim3(threads), args, p.smem, st));
     if (img_step && p.tile) {
@@ -1800,15 +2019,19 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
     }
     if (host) PW_TRY(to_host(img_out, dst, nvel * 4, true, st));
   }
+  int err_flag = 0;
+  if (p.tma) PW_CUDA(cudaMemcpyAsync(&err_flag, s.err, sizeof(int), cudaMemcpyDeviceToHost, st));
   PW_CUDA(cudaStreamSynchronize(st));
   timer.finish(step_launches, step_launches + aux_launches + img_launches);
+  PW_CHECK(err_flag == 0, PW_ERR_TIMEOUT,
+           "a 3-D step kernel gave up waiting for its TMA loads (results are invalid)");
   if (want_stats) {
-    unsigned long long c[6];
+    unsigned long long c[8];
     PW_CUDA(cudaMemcpy(c, s.stats, sizeof c, cudaMemcpyDeviceToHost));
     fprintf(stderr,
-            "afd tile paths (warp-planes): tri_fast=%llu tri_full=%llu fwd_path0=%llu "
-            "fwd_path1=%llu fwd_path2=%llu fwd_path3=%llu\n",
-            c[0], c[1], c[2], c[3], c[4], c[5]);
+            "afd tile paths (warp-planes): tri_path0=%llu tri_path1=%llu tri_path2=%llu "
+            "tri_path3=%llu fwd_path0=%llu fwd_path1=%llu fwd_path2=%llu fwd_path3=%llu\n",
+            c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7]);
   }
   return PW_OK;
 }
@@ -2226,7 +2449,7 @@ static int run_noalloc(const pw_afd_args *a, const float *vel, const float *src,
   PW_CHECK(a->tri == 0, PW_ERR_VALUE, "pw_afd_noalloc runs forward modelling only (tri = 0)");
   PW_CHECK(vel != nullptr, PW_ERR_VALUE, "velocity is null");
   Plan p;
-  PW_TRY(make_plan(a, false, 1, p));
+  PW_TRY(make_plan(a, false, 1, p, false));
   const Geo &g = p.g;
   const bool two_d = p.dim == 2;
   PW_CHECK(a->jsnap >= 0, PW_ERR_VALUE, "jsnap must be >= 0");

@@ -52,8 +52,9 @@ def pfwi_scale_case(name):
     (420 x 720 padded), 2 shots, nt 600.  deep: their left 200 columns
     extended by repeating the last 160 rows to 460 x 200 (580 x 320 padded,
     more than one z tile of the step kernel), 2 shots, nt 600.  The true
-    model gets a +10% anomaly 30 cells deep, which 0.6 s of data sees (the
-    benchmark's own anomalies lie deeper than such a record reaches)."""
+    model gets a +10% anomaly 30 cells deep under the first shot, which 0.6 s
+    of data sees (the benchmark's own anomalies lie deeper than such a record
+    reaches)."""
     if ROOT not in sys.path:
         sys.path.insert(0, ROOT)
     import bench
@@ -66,7 +67,7 @@ def pfwi_scale_case(name):
         vs = np.ascontiguousarray(np.concatenate([vs[:, :200], vs[-160:, :200]], axis=0))
     else:
         raise KeyError(name)
-    vt = shallow_anomaly(vt, 30, nx // 2, 12, 0.1)
+    vt = shallow_anomaly(vt, 30, nx // 4, 12, 0.1)
     par = dict(nz=nz, nx=nx, dz=0.01, dx=0.01, oz=0.0, ox=0.0, nt=nt, dt=0.001, ot=0.0, ns=2,
                ds=nx * 0.01 / 2, os=nx * 0.01 / 4, nb=60, coef=0.005, f0=10.0, acqui_type=1,
                interval=1)
