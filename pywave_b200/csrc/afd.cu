@@ -616,128 +616,134 @@ __global__ void __launch_bounds__(MARCH_MAXT) batch_kernel(const StepArgs *args,
   march_body<true, false, false>(sa, item.y % sa.nzc, item.y / sa.nzc, ring);
 }
 
-// Warp-tile kernels (3-D): each warp owns an 8-slot x 4-column patch of one
-// group's field and marches it along y.  Per plane the warp stages its patch
-// with a 1-slot z halo and 2-column x halo (10 x 8 float4) in a private ring
-// in shared memory, so every A value is fetched from L2 80/32 = 2.5 times
-// instead of once per neighbour use; the lanes read their z and x neighbours
-// there after a warp-level wait (no CTA barrier).  The ring holds planes
-// y .. y+2 plus TILE_NS - 3 in flight; the lead plane's centre (y+2) feeds
-// the register queue.  Each lane's B and vv cells ride in the same ring slot
-// as the A patch of their plane (TILE_NS - 1 planes ahead of their use).
-// Two ways to fill the ring:
-//   tile_kernel      every lane issues 16-byte cp.async copies (its share of
-//                    the patch plus its B and vv cells);
-//   tile_kernel_tma  one lane issues three TMA tile loads per plane (the
-//                    10 x 8 float4 A box, the 8 x 4 float4 B and vv boxes),
-//                    completed on the slot's mbarrier; the tensor maps cover
-//                    this GPU's own field buffers only (no multicast).
+// Warp-tile kernels (3-D): each warp owns an 8-slot x 4*NC-column patch of
+// one group's field and marches it along y; a lane owns one float4 of z
+// cells in NC columns (xl, xl + 4, ...).  Per plane the warp stages its
+// patch with a 1-slot z halo and 2-column x halo (10 x (4 NC + 4) float4) in
+// a private ring in shared memory, so an A value is fetched from L2
+// (4 NC + 4) * 10 / (32 NC) times instead of once per neighbour use; the
+// lanes read their z and x neighbours there after a warp-level wait (no CTA
+// barrier).  The ring holds planes y .. y+2 plus TILE_NS - 3 in flight; the
+// lead plane's centre (y+2) feeds a register queue of y neighbours.  Each
+// lane's B and vv cells ride in the same ring slot as the A patch of their
+// plane (TILE_NS - 1 planes ahead of their use).  Two ways to fill the ring:
+//   tile_kernel      (NC = 1) every lane issues 16-byte cp.async copies (its
+//                    share of the patch plus its B and vv cells);
+//   tile_kernel_tma  one lane issues three TMA tile loads per plane (the A
+//                    box, the 8 x 4 NC float4 B and vv boxes), completed on
+//                    the slot's mbarrier; the tensor maps cover this GPU's
+//                    own field buffers only (no multicast).
 // Groups of a TRI launch are separate warps of the CTA; the TRI image of an
 // imaging step is formed afterwards by image_kernel.
-constexpr int TILE_ZW = 8, TILE_XW = 4;                      // warp patch: z slots x x columns
-constexpr int TILE_TZ = TILE_ZW + 2, TILE_TX = TILE_XW + 4;  // with halos
-constexpr int TILE_TP = TILE_TZ * TILE_TX;                   // float4 per plane
-constexpr int TILE_NS = 5;                                   // ring planes per warp
+constexpr int TILE_ZW = 8, TILE_XW = 4;  // warp patch per column set: z slots x x columns
+constexpr int TILE_TZ = TILE_ZW + 2;     // z slots with halo
+constexpr int TILE_NS = 5;               // ring planes per warp
 constexpr int TILE_MAXT = 512;
-constexpr int TILE_CPL = (TILE_TP + 31) / 32;                // copies per lane per plane
-constexpr int TILE_SLOT = TILE_TP + 64;                      // float4 per ring slot: A, B, vv
-constexpr int TILE_WS = TILE_NS * TILE_SLOT;                 // ring float4 per warp
+constexpr int TILE_MAXNC = 2;            // columns per lane
+__host__ __device__ constexpr int tile_tx(int nc) { return TILE_XW * nc + 4; }  // A-box columns
+__host__ __device__ constexpr int tile_tp(int nc) { return TILE_TZ * tile_tx(nc); }  // A-box float4
+__host__ __device__ constexpr int tile_slot(int nc) { return tile_tp(nc) + 64 * nc; }  // + B, vv
+__host__ __device__ constexpr int tile_ws(int nc) { return TILE_NS * tile_slot(nc); }  // per warp
 
-// Per-warp constants of the warp-tile kernels.
+// Per-lane constants of the warp-tile kernels.
+template <int NC>
 struct TileLane {
-  int lane, gi, slot, ix, iz0, s0, c0;
-  bool valid, live;
-  long long base;  // this lane's float4 in plane 0 (field offset), or a safe one
-  float wz4[4], wzx[4], wx;
-  bool lzm[4], keep[4], lxm;
-  bool warp_plain, warp_taper_zx, warp_edge_zx, rec_zx, warp_rec, in_zx;
-  int erz, ci;
+  int lane, gi, zl, xl, slot, iz0, s0, c0, erz;
+  int ix[NC];
+  bool valid[NC], live[NC], lxm[NC], rec_zx[NC], in_zx[NC];
+  long long base[NC];  // field offset of each column's float4 in plane 0 (or a safe one)
+  float wz4[4], wx[NC], wzx[NC][4];
+  bool lzm[4], keep[4];
+  bool warp_plain, warp_taper_zx, warp_edge_zx, warp_rec;
 };
 
-__device__ __forceinline__ void tile_lane_setup(const StepArgs &a, TileLane &L) {
+// GROUP_GRID: the CTA holds one group's warps and blockIdx.x = group + G *
+// tile; otherwise the CTA holds the G group warps of one tile (warp = group
+// + G * warp-in-group).
+template <int NC, bool GROUP_GRID>
+__device__ __forceinline__ void tile_lane_setup(const StepArgs &a, TileLane<NC> &L) {
   const Geo &g = a.g;
   const unsigned full = 0xffffffffu;
   const int t = threadIdx.x, w = t >> 5;
   L.lane = t & 31;
   const int G = a.ngroups;
-  L.gi = w % G;
-  const int wt = w / G;
+  L.gi = GROUP_GRID ? (int)(blockIdx.x % G) : w % G;
+  const int wt = GROUP_GRID ? w : w / G;
+  const int tile = GROUP_GRID ? (int)(blockIdx.x / G) : (int)blockIdx.x;
   const int wzi = wt % a.WZ, wxi = wt / a.WZ;
-  const int zl = L.lane % TILE_ZW, xl = L.lane / TILE_ZW;
-  L.s0 = (blockIdx.x % a.nzc) * (a.WZ * TILE_ZW) + wzi * TILE_ZW;  // warp's first slot
-  L.c0 = (int)(blockIdx.x / a.nzc) * (a.WX * TILE_XW) + wxi * TILE_XW;
-  L.slot = L.s0 + zl;
-  L.ix = L.c0 + xl;
-  L.valid = L.slot < a.S && L.ix < g.nx;
+  L.zl = L.lane % TILE_ZW;
+  L.xl = L.lane / TILE_ZW;
+  L.s0 = (tile % a.nzc) * (a.WZ * TILE_ZW) + wzi * TILE_ZW;  // warp's first slot
+  L.c0 = (tile / a.nzc) * (a.WX * TILE_XW * NC) + wxi * TILE_XW * NC;
+  L.slot = L.s0 + L.zl;
   L.iz0 = 4 * L.slot - HZ;
-  L.live = L.valid && L.slot >= 1 && L.iz0 < g.nz;
   const long long safe = g.sx * g.hx + g.sy * g.hy;  // slot 0, column 0: in range for every plane
-  L.base = L.valid ? 4LL * L.slot + g.sx * (L.ix + g.hx) + g.sy * g.hy : safe;
-  bool lane_taper = false, lane_plain = true;
+  bool lane_taper = false, lane_plain = true, lane_edge = false, any_rec = false;
 #pragma unroll
   for (int e = 0; e < 4; e++) {
     const int iz = L.iz0 + e;
-    L.wz4[e] = (L.live && iz < g.nz) ? a.wz[iz] : 1.f;
     L.lzm[e] = iz >= g.lz0 && iz < g.lz1;
     L.keep[e] = iz < g.nz;
-    lane_taper |= L.wz4[e] != 1.f;
-    lane_plain &= L.lzm[e] && L.keep[e];
   }
-  L.wx = L.live ? a.wx[L.ix] : 1.f;
-  L.lxm = L.ix >= g.lx0 && L.ix < g.lx1;
-  lane_taper |= L.wx != 1.f;
-  lane_plain &= L.lxm;
-  // warp-uniform: every live lane free of masks, no lane tapered in z or x
-  L.warp_plain = __all_sync(full, !L.live || lane_plain);
-  L.warp_taper_zx = __any_sync(full, L.live && lane_taper);
-  // z-x edge cells (tapered along both z and x) need the factors one by one;
-  // elsewhere wz * wx has at most one factor != 1 and is exact
-  bool lane_edge = false;
+  const bool zlive = L.slot < a.S && L.slot >= 1 && L.iz0 < g.nz;
 #pragma unroll
   for (int e = 0; e < 4; e++) {
-    lane_edge |= L.wz4[e] != 1.f && L.wx != 1.f;
-    L.wzx[e] = fmul(L.wz4[e], L.wx);
+    const int iz = L.iz0 + e;
+    L.wz4[e] = (zlive && iz < g.nz) ? a.wz[iz] : 1.f;
   }
-  L.warp_edge_zx = __any_sync(full, L.live && lane_edge);
   L.erz = a.rz - L.iz0;
-  L.rec_zx = L.live && L.erz >= 0 && L.erz < 4 && L.ix >= a.rx0 && L.ix < a.rx0 + a.nrx;
-  L.warp_rec = __any_sync(full, L.rec_zx);
-  L.in_zx = L.ix >= a.nbx && L.ix < a.nbx + a.nx1;
-  L.ci = (xl + 2) * TILE_TZ + zl + 1;  // centre in the patch
+#pragma unroll
+  for (int j = 0; j < NC; j++) {
+    const int ix = L.c0 + L.xl + TILE_XW * j;
+    L.ix[j] = ix;
+    L.valid[j] = L.slot < a.S && ix < g.nx;
+    L.live[j] = L.valid[j] && zlive;
+    L.base[j] = L.valid[j] ? 4LL * L.slot + g.sx * (ix + g.hx) + g.sy * g.hy : safe;
+    L.wx[j] = L.live[j] ? a.wx[ix] : 1.f;
+    L.lxm[j] = ix >= g.lx0 && ix < g.lx1;
+    bool plain = L.lxm[j], taper = L.wx[j] != 1.f, edge = false;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      plain &= L.lzm[e] && L.keep[e];
+      taper |= L.wz4[e] != 1.f;
+      edge |= L.wz4[e] != 1.f && L.wx[j] != 1.f;
+      L.wzx[j][e] = fmul(L.wz4[e], L.wx[j]);
+    }
+    lane_plain &= !L.live[j] || plain;
+    lane_taper |= L.live[j] && taper;
+    lane_edge |= L.live[j] && edge;
+    L.rec_zx[j] = L.live[j] && L.erz >= 0 && L.erz < 4 && ix >= a.rx0 && ix < a.rx0 + a.nrx;
+    any_rec |= L.rec_zx[j];
+    L.in_zx[j] = ix >= a.nbx && ix < a.nbx + a.nx1;
+  }
+  // warp-uniform: every live cell free of masks; any cell tapered in z or x;
+  // any z-x edge cell (tapered along both z and x: the factors one by one;
+  // elsewhere wz * wx has at most one factor != 1 and is exact)
+  L.warp_plain = __all_sync(full, lane_plain);
+  L.warp_taper_zx = __any_sync(full, lane_taper);
+  L.warp_edge_zx = __any_sync(full, lane_edge);
+  L.warp_rec = __any_sync(full, any_rec);
 }
 
-// One plane y of a warp-tile kernel: the 4th-order Laplacian of the float4
-// q2 (z neighbours from the patch pc, x neighbours from the patch, y
-// neighbours q0..q4), the leapfrog update against pv = u_{k-1} as stored,
-// injection, the taper and the store, in the reference's float order.
+// One plane y of a warp-tile kernel for the lane's NC float4: the 4th-order
+// Laplacian (z neighbours and x neighbours from the staged A patch pc, y
+// neighbours from the queue q), the leapfrog update against pv = u_{k-1} as
+// stored, injection, the taper and the store, in the reference's float order.
 // Warp-uniform paths, exact because every skipped factor is exactly 1:
 // 0 no taper and no mask; 1 y taper only (x wy); 2 z / x taper only, no z-x
 // edge (x wz*wx); 3 everything face by face (masks, sources, z-x edges).
 // Returns the path taken.
-template <bool TRI, bool SNAP>
-__device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane &L, int y, float wy,
-                                          const float4 &q0, const float4 &q1, const float4 &q2,
-                                          const float4 &q3, const float4 &q4, const float4 *pc,
-                                          const float4 &pv, const float4 &vv4, float *pB) {
+template <bool TRI, bool SNAP, int NC>
+__device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> &L, int y,
+                                          float wy, const float4 (&q0)[NC],
+                                          const float4 (&q1)[NC], const float4 (&q2)[NC],
+                                          const float4 (&q3)[NC], const float4 (&q4)[NC],
+                                          const float4 *pc, const float4 *pbv, float *const (&pB)[NC]) {
   const Geo &g = a.g;
-  const int ci = L.ci, erz = L.erz, ix = L.ix, gi = L.gi;
-  const float4 xm1 = pc[ci - TILE_TZ], xp1 = pc[ci + TILE_TZ];
-  const float4 xm2 = pc[ci - 2 * TILE_TZ], xp2 = pc[ci + 2 * TILE_TZ];
-  const float2 Lf = reinterpret_cast<const float2 *>(pc + ci - 1)[1];  // (z, w)
-  const float2 Rf = reinterpret_cast<const float2 *>(pc + ci + 1)[0];  // (x, y)
+  constexpr int TZ = TILE_TZ;
+  const int erz = L.erz, gi = L.gi;
   const bool lyok = y >= g.ly0 && y < g.ly1;
   const int nrec = a.nrx * a.nry;
-  bool rec_here = false, inj = false;
-  int r_idx = 0;
-  float dval = 0.f;
-  if (L.warp_rec) {
-    rec_here = L.rec_zx && y >= a.ry0 && y < a.ry0 + a.nry;
-    r_idx = rec_here ? (y - a.ry0) * a.nrx + (ix - a.rx0) : 0;
-    if (TRI && rec_here) {
-      inj = a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi;
-      if (inj) dval = a.tri_dat[(size_t)a.it * nrec + r_idx];
-    }
-  }
   bool src_plane = false;
   if (!TRI)
     for (int s = 0; s < a.ns; s++) src_plane |= (y >= a.sy[s] - 1 && y <= a.sy[s] + 1);
@@ -745,89 +751,112 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane &L, 
   const int path = !clean ? 3
                    : (!L.warp_taper_zx ? (wy == 1.f ? 0 : 1)
                                        : (wy == 1.f && !L.warp_edge_zx ? 2 : 3));
-  float4 lp;  // Laplacian sums in the reference's order
 #pragma unroll
-  for (int e = 0; e < 4; e++) {
-    const float cv = el(q2, e);
-    const float zm1 = e == 0 ? Lf.y : el(q2, e - 1);
-    const float zp1 = e == 3 ? Rf.x : el(q2, e + 1);
-    const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2, e - 2));
-    const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2, e + 2));
-    float tt = fmul(fmul(a.c0, cv), a.k0);
-    tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
-    tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
-    tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
-    tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
-    tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-    tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-    set_el(lp, e, tt);
-  }
-  float4 res;
-  if (path == 0) {
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const float cv = el(q2, e);
-      float v = fadd(cv, fsub(cv, el(pv, e)));
-      set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
-    }
-    if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
-  } else if (path == 1 || path == 2) {
-    float4 f;
-#pragma unroll
-    for (int e = 0; e < 4; e++) set_el(f, e, path == 1 ? wy : L.wzx[e]);
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const float cv = el(q2, e);
-      float v = fadd(cv, fsub(cv, fmul(el(pv, e), el(f, e))));
-      set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
-    }
-    // time reversal injects after the update and before the taper
-    if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
-#pragma unroll
-    for (int e = 0; e < 4; e++) set_el(res, e, fmul(el(res, e), el(f, e)));
-  } else {
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const float cv = el(q2, e);
-      const float lap = (L.lzm[e] && L.lxm && lyok) ? el(lp, e) : 0.f;
-      // prev = taper(u_{k-1} as stored), face by face
-      float p = fmul(el(pv, e), L.wz4[e]);
-      p = fmul(p, L.wx);
-      p = fmul(p, wy);
-      const float vve = el(vv4, e);
-      float v = fadd(cv, fsub(cv, p));
-      v = fadd(v, fmul(lap, vve));
-      if (!TRI && src_plane) {
-        const int iz = L.iz0 + e;
-        for (int s = 0; s < a.ns; s++) {
-          const int dz = iz - a.sz[s], dxs = ix - a.sx[s], dys = y - a.sy[s];
-          if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
-            const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
-            v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
-          }
-        }
+  for (int j = 0; j < NC; j++) {
+    const int ix = L.ix[j];
+    const int ci = (L.xl + TILE_XW * j + 2) * TZ + L.zl + 1;  // centre in the A patch
+    const float4 xm1 = pc[ci - TZ], xp1 = pc[ci + TZ];
+    const float4 xm2 = pc[ci - 2 * TZ], xp2 = pc[ci + 2 * TZ];
+    const float2 Lf = reinterpret_cast<const float2 *>(pc + ci - 1)[1];  // (z, w)
+    const float2 Rf = reinterpret_cast<const float2 *>(pc + ci + 1)[0];  // (x, y)
+    const float4 pv = pbv[L.lane + 32 * j];
+    const float4 vv4 = pbv[32 * NC + L.lane + 32 * j];
+    bool rec_here = false, inj = false;
+    int r_idx = 0;
+    float dval = 0.f;
+    if (L.warp_rec) {
+      rec_here = L.rec_zx[j] && y >= a.ry0 && y < a.ry0 + a.nry;
+      r_idx = rec_here ? (y - a.ry0) * a.nrx + (ix - a.rx0) : 0;
+      if (TRI && rec_here) {
+        inj = a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi;
+        if (inj) dval = a.tri_dat[(size_t)a.it * nrec + r_idx];
       }
-      set_el(res, e, v);
     }
-    if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
+    float4 lp;  // Laplacian sums in the reference's order
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      float v = fmul(el(res, e), L.wz4[e]);
-      v = fmul(v, L.wx);
-      v = fmul(v, wy);
-      set_el(res, e, L.keep[e] ? v : 0.f);
+      const float cv = el(q2[j], e);
+      const float zm1 = e == 0 ? Lf.y : el(q2[j], e - 1);
+      const float zp1 = e == 3 ? Rf.x : el(q2[j], e + 1);
+      const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2[j], e - 2));
+      const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2[j], e + 2));
+      float tt = fmul(fmul(a.c0, cv), a.k0);
+      tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1[j], e), el(q3[j], e))), a.idy));
+      tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0[j], e), el(q4[j], e))), a.idy));
+      tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
+      tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
+      tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
+      tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
+      set_el(lp, e, tt);
     }
-  }
-  if (L.live) *reinterpret_cast<float4 *>(pB) = res;
-  if (!TRI && rec_here && a.rec && gi == 0) a.rec[(size_t)a.it * nrec + r_idx] = el(res, erz);
-  if (SNAP) {
-    const bool interior = L.live && L.in_zx && y >= a.nby && y < a.nby + a.ny1;
-    if (a.wfd && gi == 0 && interior) {
+    float4 res;
+    if (path == 0) {
 #pragma unroll
       for (int e = 0; e < 4; e++) {
-        const int iz = L.iz0 + e;
-        if (iz >= a.nbz && iz < a.nbz + a.nz1)
-          a.wfd[((size_t)(y - a.nby) * a.nx1 + (ix - a.nbx)) * a.nz1 + (iz - a.nbz)] = el(res, e);
+        const float cv = el(q2[j], e);
+        float v = fadd(cv, fsub(cv, el(pv, e)));
+        set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
+      }
+      if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
+    } else if (path == 1 || path == 2) {
+      float4 f;
+#pragma unroll
+      for (int e = 0; e < 4; e++) set_el(f, e, path == 1 ? wy : L.wzx[j][e]);
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const float cv = el(q2[j], e);
+        float v = fadd(cv, fsub(cv, fmul(el(pv, e), el(f, e))));
+        set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
+      }
+      // time reversal injects after the update and before the taper
+      if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
+#pragma unroll
+      for (int e = 0; e < 4; e++) set_el(res, e, fmul(el(res, e), el(f, e)));
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const float cv = el(q2[j], e);
+        const float lap = (L.lzm[e] && L.lxm[j] && lyok) ? el(lp, e) : 0.f;
+        // prev = taper(u_{k-1} as stored), face by face
+        float p = fmul(el(pv, e), L.wz4[e]);
+        p = fmul(p, L.wx[j]);
+        p = fmul(p, wy);
+        const float vve = el(vv4, e);
+        float v = fadd(cv, fsub(cv, p));
+        v = fadd(v, fmul(lap, vve));
+        if (!TRI && src_plane) {
+          const int iz = L.iz0 + e;
+          for (int s = 0; s < a.ns; s++) {
+            const int dz = iz - a.sz[s], dxs = ix - a.sx[s], dys = y - a.sy[s];
+            if (dz >= -1 && dz <= 1 && dxs >= -1 && dxs <= 1 && dys >= -1 && dys <= 1) {
+              const float den = (float)(abs(dxs) + abs(dys) + abs(dz) + 1);
+              v = fadd(v, fdiv(fmul(vve, a.rick[(size_t)s * a.nt + a.it]), den));
+            }
+          }
+        }
+        set_el(res, e, v);
+      }
+      if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        float v = fmul(el(res, e), L.wz4[e]);
+        v = fmul(v, L.wx[j]);
+        v = fmul(v, wy);
+        set_el(res, e, L.keep[e] ? v : 0.f);
+      }
+    }
+    if (L.live[j]) *reinterpret_cast<float4 *>(pB[j]) = res;
+    if (!TRI && rec_here && a.rec && gi == 0) a.rec[(size_t)a.it * nrec + r_idx] = el(res, erz);
+    if (SNAP) {
+      const bool interior = L.live[j] && L.in_zx[j] && y >= a.nby && y < a.nby + a.ny1;
+      if (a.wfd && gi == 0 && interior) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int iz = L.iz0 + e;
+          if (iz >= a.nbz && iz < a.nbz + a.nz1)
+            a.wfd[((size_t)(y - a.nby) * a.nx1 + (ix - a.nbx)) * a.nz1 + (iz - a.nbz)] =
+                el(res, e);
+        }
       }
     }
   }
@@ -835,7 +864,7 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane &L, 
 }
 
 // Per-warp path counts (16 bits per path; a launch gives a warp at most
-// ych < 65536 planes), flushed to a.stats at the end when requested:
+// ych < 65536 planes), kept only when a.stats is set and flushed at the end:
 // [0..3] TRI paths 0..3, [4..7] forward paths 0..3.
 template <bool TRI>
 __device__ __forceinline__ void flush_path_counts(const StepArgs &a, int lane,
@@ -849,14 +878,25 @@ __device__ __forceinline__ void flush_path_counts(const StepArgs &a, int lane,
   }
 }
 
-template <bool TRI, bool SNAP>
+// cp.async ring of the warp-tile kernel.  The CTA holds WZ x WX warps of one
+// group (the group index runs fastest over the CTAs, so the G CTAs of a patch
+// run side by side and share vv through L2).  Per warp: an A ring of TILE_NS
+// patches and a B / vv ring of TILE_BV_NS planes of this warp's cells, which
+// are copied two planes before their use.
+constexpr int TILE_BV_NS = 3;
+__host__ __device__ constexpr int tile_cp_ws(int nc) {  // float4 per warp
+  return TILE_NS * tile_tp(nc) + TILE_BV_NS * 64 * nc;
+}
+
+template <bool TRI, bool SNAP, int NC>
 __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
   extern __shared__ float4 tsm[];
-  constexpr int NS = TILE_NS, D = NS - 3;
+  constexpr int NS = TILE_NS, D = NS - 3, TP = tile_tp(NC), BVS = 64 * NC;
+  constexpr int CPL = (TP + 31) / 32;  // A-patch copies per lane per plane
   static_assert(NS == 5, "the y loop is unrolled by the queue length 5");
   const Geo &g = a.g;
-  TileLane L;
-  tile_lane_setup(a, L);
+  TileLane<NC> L;
+  tile_lane_setup<NC, true>(a, L);
   const int lane = L.lane, w = threadIdx.x >> 5;
   const float *A = a.cur[0];
   float *B = a.nxt[0];
@@ -868,80 +908,111 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
     }
   const long long sx = g.sx, sy = g.sy;
   const long long safe = sx * g.hx + sy * g.hy;
-  float4 *ring = tsm + (size_t)w * TILE_WS;  // NS slots of [A patch, B, vv]
+  float4 *ring = tsm + (size_t)w * tile_cp_ws(NC);  // NS A patches
+  float4 *bvring = ring + NS * TP;                  // TILE_BV_NS planes of [B, vv]
   const int y0 = blockIdx.y * a.ych;
   const int y1 = min(g.ny, y0 + a.ych);
 
-  // this lane's share of the patch copy: element j = lane + 32k of the
-  // (TILE_TZ x TILE_TX) patch, tz fastest; pointers at the next plane to copy
-  const float *cpp[TILE_CPL];
-  bool c_ok[TILE_CPL];
+  // this lane's share of the A-patch copy: element j = lane + 32k of the
+  // (TILE_TZ x tile_tx(NC)) patch, tz fastest; pointers at the next plane
+  const float *cpp[CPL];
+  bool c_ok[CPL];
 #pragma unroll
-  for (int k = 0; k < TILE_CPL; k++) {
+  for (int k = 0; k < CPL; k++) {
     const int j = lane + 32 * k;
     const int tz = j % TILE_TZ, tx = j / TILE_TZ;
     const int sl = L.s0 - 1 + tz, col = L.c0 - 2 + tx;
-    c_ok[k] = j < TILE_TP && sl >= 0 && sl < a.S && col >= -g.hx && col < g.nx + g.hx;
+    c_ok[k] = j < TP && sl >= 0 && sl < a.S && col >= -g.hx && col < g.nx + g.hx;
     cpp[k] = A + (c_ok[k] ? 4LL * sl + sx * (col + g.hx) + sy * g.hy : safe) + sy * y0;
   }
-  int next_plane = y0;
-  const float *cB = B + L.base + sy * y0, *cV = a.vv + L.base + sy * y0;
-  // copies of plane next_plane into ring slot rs: the A patch, and this lane's
-  // B and vv cells (used when next_plane is updated); planes past y1 + 1 are
-  // not needed
-  auto issue = [&](int rs) {
-    if (next_plane <= y1 + 1) {
-      float4 *dst = ring + rs * TILE_SLOT;
+  // this lane's B and vv cells, pointers at the next plane
+  const float *cB[NC], *cV[NC];
 #pragma unroll
-      for (int k = 0; k < TILE_CPL; k++) {
+  for (int j = 0; j < NC; j++) {
+    cB[j] = B + L.base[j] + sy * y0;
+    cV[j] = a.vv + L.base[j] + sy * y0;
+  }
+  int next_a = y0, next_bv = y0;
+  auto issue_a = [&](int rs) {  // A patch of plane next_a into A slot rs
+    if (next_a <= y1 + 1) {
+      float4 *dst = ring + rs * TP;
+#pragma unroll
+      for (int k = 0; k < CPL; k++) {
         const int j = lane + 32 * k;
-        if (j < TILE_TP) cp16(dst + j, cpp[k], c_ok[k]);
+        if (j < TP) cp16(dst + j, cpp[k], c_ok[k]);
         cpp[k] += sy;
       }
-      if (next_plane < y1) {
-        cp16(dst + TILE_TP + lane, cB, L.valid);
-        cp16(dst + TILE_TP + 32 + lane, cV, L.valid);
-      }
-      cB += sy;
-      cV += sy;
     }
-    next_plane++;
-    cp_commit();
+    next_a++;
+  };
+  auto issue_bv = [&](int bs) {  // B and vv of plane next_bv into B/vv slot bs
+    if (next_bv < y1) {
+      float4 *dst = bvring + bs * BVS;
+#pragma unroll
+      for (int j = 0; j < NC; j++) {
+        cp16(dst + lane + 32 * j, cB[j], L.valid[j]);
+        cp16(dst + 32 * NC + lane + 32 * j, cV[j], L.valid[j]);
+        cB[j] += sy;
+        cV[j] += sy;
+      }
+    }
+    next_bv++;
   };
 
+  const bool counting = a.stats != nullptr;
   unsigned long long pcount = 0;
   // queue: plane y-2+k sits in q[(y - y0 + k) % 5]
-  float4 q[5];
-  q[4] = make_float4(0.f, 0.f, 0.f, 0.f);
-  const float *pA = A + L.base;
-  float *pB = B + L.base + sy * y0;
-  q[0] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 2)));
-  q[1] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 1)));
-  q[2] = __ldg(reinterpret_cast<const float4 *>(pA + sy * y0));
-  q[3] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 + 1)));
-  float wyn = y0 < y1 ? __ldg(a.wy + y0) : 1.f;
+  float4 q[5][NC];
+  float *pB[NC];
 #pragma unroll
-  for (int j = 0; j < 2 + D; j++) issue(j);
+  for (int j = 0; j < NC; j++) {
+    q[4][j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float *pA = A + L.base[j];
+    pB[j] = B + L.base[j] + sy * y0;
+    q[0][j] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 2)));
+    q[1][j] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 1)));
+    q[2][j] = __ldg(reinterpret_cast<const float4 *>(pA + sy * y0));
+    q[3][j] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 + 1)));
+  }
+  float wyn = y0 < y1 ? __ldg(a.wy + y0) : 1.f;
+  // commit groups: {A y0..y0+2, B/vv y0..y0+1}, {A y0+3}, then per plane y
+  // {A y+4, B/vv y+2}; at plane y the group of plane y-2 (or the first two)
+  // holds A y+2 and B/vv y, so D = 2 groups may stay in flight
+  issue_a(0);
+  issue_a(1);
+  issue_a(2);
+  issue_bv(0);
+  issue_bv(1);
+  cp_commit();
+  issue_a(3);
+  cp_commit();
+  int bvs = 0;  // B/vv slot of plane y
 
   for (int yb = y0; yb < y1; yb += NS) {
 #pragma unroll
     for (int u = 0; u < NS; u++) {
       const int y = yb + u;
       if (y < y1) {
-        issue((u + 2 + D) % NS);  // plane y + 2 + D into the slot plane y - 1 left
+        issue_a((u + 4) % NS);                               // into the slot plane y - 1 left
+        issue_bv(bvs == 0 ? 2 : bvs - 1);                    // (bvs + 2) % 3: plane y - 1's
+        cp_commit();
         cp_wait<D>();
         __syncwarp();
-        const float4 *slot = ring + u * TILE_SLOT;
-        q[(u + 4) % NS] = ring[((u + 2) % NS) * TILE_SLOT + L.ci];
+        const float4 *slot = ring + u * TP;
+        const float4 *lead = ring + ((u + 2) % NS) * TP;
+#pragma unroll
+        for (int j = 0; j < NC; j++)
+          q[(u + 4) % NS][j] = lead[(L.xl + TILE_XW * j + 2) * TILE_TZ + L.zl + 1];
         const float wy = wyn;
         if (y + 1 < y1) wyn = __ldg(a.wy + y + 1);
-        const int path = tile_plane<TRI, SNAP>(a, L, y, wy, q[u], q[(u + 1) % NS],
-                                               q[(u + 2) % NS], q[(u + 3) % NS],
-                                               q[(u + 4) % NS], slot, slot[TILE_TP + lane],
-                                               slot[TILE_TP + 32 + lane], pB);
-        pcount += 1ull << (16 * path);
-        pB += sy;
-        __syncwarp();  // the ring slot refilled next iteration was read above
+        const int path = tile_plane<TRI, SNAP, NC>(a, L, y, wy, q[u], q[(u + 1) % NS],
+                                                   q[(u + 2) % NS], q[(u + 3) % NS],
+                                                   q[(u + 4) % NS], slot, bvring + bvs * BVS, pB);
+        if (counting) pcount += 1ull << (16 * path);
+#pragma unroll
+        for (int j = 0; j < NC; j++) pB[j] += sy;
+        bvs = bvs == 2 ? 0 : bvs + 1;
+        __syncwarp();  // the ring slots refilled next iteration were read above
       }
     }
   }
@@ -951,16 +1022,16 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
 
 // ---- TMA ring -----------------------------------------------------------
 // Tensor maps of one step launch (3-D field layout, float32, zero fill out of
-// bounds): the A box (40 z floats x 8 columns x 1 plane) of each group's
-// current field, the B box (32 x 4 x 1) of each group's previous field and
-// of vv.  Dimensions {lz, nx + 2 hx, ny + 2 hy} in array coordinates.
+// bounds): the A box (40 z floats x (4 NC + 4) columns x 1 plane) of each
+// group's current field, the B box (32 x 4 NC x 1) of each group's previous
+// field and of vv.  Dimensions {lz, nx + 2 hx, ny + 2 hy} in array
+// coordinates.
 struct TileMaps {
   CUtensorMap a[MAXG];
   CUtensorMap b[MAXG];
   CUtensorMap v;
 };
-constexpr unsigned TILE_A_BYTES = TILE_TP * 16, TILE_BV_BYTES = 32 * 16;
-constexpr int TILE_WAIT_LIMIT = 1 << 20;  // try_wait rounds before a wait gives up
+constexpr unsigned long long TILE_WAIT_NS = 2000000000ull;  // a wait gives up after 2 s
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -974,21 +1045,31 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long *b, unsigned b
                "r"(bytes)
                : "memory");
 }
+// One try_wait on the given phase parity; the thread may be suspended in the
+// hardware for up to about a millisecond while the phase is incomplete.
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long *b, unsigned phase) {
   unsigned ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
       " selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(smem_addr(b)), "r"(phase)
+      : "r"(smem_addr(b)), "r"(phase), "r"(1000000u)
       : "memory");
   return ok != 0;
 }
-// Bounded wait for the given phase of an mbarrier: false when it gave up.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// Wait for the given phase of an mbarrier, bounded in time: false when it
+// gave up (TILE_WAIT_NS).
 __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned phase) {
-  for (int n = 0; n < TILE_WAIT_LIMIT; n++)
-    if (mbar_try_wait(b, phase)) return true;
-  return false;
+  if (mbar_try_wait(b, phase)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(b, phase))
+    if (global_ns() - t0 > TILE_WAIT_NS) return false;
+  return true;
 }
 __device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *m, int c0, int c1, int c2,
                                           unsigned long long *bar) {
@@ -999,30 +1080,32 @@ __device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *m, int c
       : "memory");
 }
 
-template <bool TRI, bool SNAP>
+template <bool TRI, bool SNAP, int NC>
 __global__ void __launch_bounds__(TILE_MAXT)
     tile_kernel_tma(const StepArgs a, const __grid_constant__ TileMaps maps) {
   extern __shared__ __align__(128) float4 tsm_tma[];
-  float4 *const tsm = tsm_tma;
-  constexpr int NS = TILE_NS, D = NS - 3;
+  constexpr int NS = TILE_NS, D = NS - 3, TP = tile_tp(NC), SLOT = tile_slot(NC);
+  constexpr unsigned A_BYTES = TP * 16, BV_BYTES = 32 * NC * 16;
   static_assert(NS == 5, "the y loop is unrolled by the queue length 5");
+  static_assert((SLOT * 16) % 128 == 0 && (TP * 16) % 128 == 0 && (32 * NC * 16) % 128 == 0,
+                "TMA destinations stay 128-byte aligned");
   const Geo &g = a.g;
-  TileLane L;
-  tile_lane_setup(a, L);
+  TileLane<NC> L;
+  tile_lane_setup<NC, false>(a, L);
   const int lane = L.lane, w = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
-  const float *A = a.cur[0];
   float *B = a.nxt[0];
 #pragma unroll
   for (int k = 1; k < MAXG; k++)
-    if (L.gi == k) {
-      A = a.cur[k];
-      B = a.nxt[k];
-    }
+    if (L.gi == k) B = a.nxt[k];
+  const float *A = a.cur[0];
+#pragma unroll
+  for (int k = 1; k < MAXG; k++)
+    if (L.gi == k) A = a.cur[k];
   const long long sy = g.sy;
-  float4 *ring = tsm + (size_t)w * TILE_WS;  // NS slots of [A patch, B, vv]
+  float4 *ring = tsm_tma + (size_t)w * tile_ws(NC);  // NS slots of [A patch, B, vv]
   unsigned long long *bars =
-      reinterpret_cast<unsigned long long *>(tsm + (size_t)nwarps * TILE_WS) + w * NS;
+      reinterpret_cast<unsigned long long *>(tsm_tma + (size_t)nwarps * tile_ws(NC)) + w * NS;
   const int y0 = blockIdx.y * a.ych;
   const int y1 = min(g.ny, y0 + a.ych);
   const CUtensorMap *mA = &maps.a[L.gi], *mB = &maps.b[L.gi], *mV = &maps.v;
@@ -1039,22 +1122,22 @@ __global__ void __launch_bounds__(TILE_MAXT)
   // vv boxes when next_plane is updated; planes past y1 + 1 are not needed
   auto issue = [&](int rs) {
     if (lane == 0 && next_plane <= y1 + 1) {
-      float4 *dst = ring + rs * TILE_SLOT;
+      float4 *dst = ring + rs * SLOT;
       const bool upd = next_plane < y1;
       // the slot was last read by the whole warp (ordered by the __syncwarp
       // that precedes this call); order those reads before the async writes
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      mbar_expect_tx(bars + rs, TILE_A_BYTES + (upd ? 2 * TILE_BV_BYTES : 0));
+      mbar_expect_tx(bars + rs, A_BYTES + (upd ? 2 * BV_BYTES : 0));
       const int py = next_plane + g.hy;
       tma_load3(dst, mA, az, ax, py, bars + rs);
       if (upd) {
-        tma_load3(dst + TILE_TP, mB, bz, bx, py, bars + rs);
-        tma_load3(dst + TILE_TP + 32, mV, bz, bx, py, bars + rs);
+        tma_load3(dst + TP, mB, bz, bx, py, bars + rs);
+        tma_load3(dst + TP + 32 * NC, mV, bz, bx, py, bars + rs);
       }
     }
     next_plane++;
   };
-  int waited = y0 - 1;  // last plane whose slot this warp has waited for
+  int waited = y0 - 1;  // last plane whose slot this lane has waited for
   bool ok = true;
   // wait for plane p (ring slot (p - y0) % NS, phase ((p - y0) / NS) & 1)
   auto wait_plane = [&](int p) {
@@ -1065,15 +1148,21 @@ __global__ void __launch_bounds__(TILE_MAXT)
     }
   };
 
+  const bool counting = a.stats != nullptr;
   unsigned long long pcount = 0;
-  float4 q[5];
-  q[4] = make_float4(0.f, 0.f, 0.f, 0.f);
-  const float *pA = A + L.base;
-  float *pB = B + L.base + sy * y0;
-  q[0] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 2)));
-  q[1] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 1)));
-  q[2] = __ldg(reinterpret_cast<const float4 *>(pA + sy * y0));
-  q[3] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 + 1)));
+  // queue: plane y-2+k sits in q[(y - y0 + k) % 5]
+  float4 q[5][NC];
+  float *pB[NC];
+#pragma unroll
+  for (int j = 0; j < NC; j++) {
+    q[4][j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float *pA = A + L.base[j];
+    pB[j] = B + L.base[j] + sy * y0;
+    q[0][j] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 2)));
+    q[1][j] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 - 1)));
+    q[2][j] = __ldg(reinterpret_cast<const float4 *>(pA + sy * y0));
+    q[3][j] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 + 1)));
+  }
   float wyn = y0 < y1 ? __ldg(a.wy + y0) : 1.f;
 #pragma unroll
   for (int j = 0; j < 2 + D; j++) issue(j);
@@ -1092,16 +1181,19 @@ __global__ void __launch_bounds__(TILE_MAXT)
           ok = false;
           break;
         }
-        const float4 *slot = ring + u * TILE_SLOT;
-        q[(u + 4) % NS] = ring[((u + 2) % NS) * TILE_SLOT + L.ci];
+        const float4 *slot = ring + u * SLOT;
+        const float4 *lead = ring + ((u + 2) % NS) * SLOT;
+#pragma unroll
+        for (int j = 0; j < NC; j++)
+          q[(u + 4) % NS][j] = lead[(L.xl + TILE_XW * j + 2) * TILE_TZ + L.zl + 1];
         const float wy = wyn;
         if (y + 1 < y1) wyn = __ldg(a.wy + y + 1);
-        const int path = tile_plane<TRI, SNAP>(a, L, y, wy, q[u], q[(u + 1) % NS],
-                                               q[(u + 2) % NS], q[(u + 3) % NS],
-                                               q[(u + 4) % NS], slot, slot[TILE_TP + lane],
-                                               slot[TILE_TP + 32 + lane], pB);
-        pcount += 1ull << (16 * path);
-        pB += sy;
+        const int path = tile_plane<TRI, SNAP, NC>(a, L, y, wy, q[u], q[(u + 1) % NS],
+                                                   q[(u + 2) % NS], q[(u + 3) % NS],
+                                                   q[(u + 4) % NS], slot, slot + TP, pB);
+        if (counting) pcount += 1ull << (16 * path);
+#pragma unroll
+        for (int j = 0; j < NC; j++) pB[j] += sy;
         __syncwarp();  // the ring slot refilled next iteration was read above
       }
     }
@@ -1256,6 +1348,7 @@ struct Plan {
   void *fn, *fn_snap;  // plain steps / snapshot and imaging steps
   bool tile;           // warp-tile kernel: TRI images by image_kernel
   bool tma;            // warp-tile kernel with the TMA ring (takes TileMaps)
+  int nc;              // warp-tile kernel: columns per lane
   int threads;
   int S, ZS, KX, nzc, WPC, WZ, WX;
 };
@@ -1361,107 +1454,134 @@ static int plan_march(bool tri, int G, int nsm, Plan &p) {
   return PW_OK;
 }
 
-static size_t tile_smem(int threads, bool tma) {
+static size_t tile_smem(int threads, bool tma, int nc) {
   const size_t nw = (size_t)threads / 32;
-  return nw * TILE_WS * sizeof(float4) + (tma ? nw * TILE_NS * sizeof(unsigned long long) : 0);
+  if (!tma) return nw * tile_cp_ws(nc) * sizeof(float4);
+  return nw * tile_ws(nc) * sizeof(float4) + nw * TILE_NS * sizeof(unsigned long long);
 }
 
-template <bool TRI, bool SNAP, bool TMA>
+template <bool TRI, bool SNAP, bool TMA, int NC>
 static void *tile_ptr() {
-  void *f = TMA ? (void *)tile_kernel_tma<TRI, SNAP> : (void *)tile_kernel<TRI, SNAP>;
+  void *f = TMA ? (void *)tile_kernel_tma<TRI, SNAP, NC> : (void *)tile_kernel<TRI, SNAP, NC>;
   static bool once = [f] {
+    // as much as a block may opt into (the planner only picks launchable tiles)
+    int dev = 0, maxsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)tile_smem(TILE_MAXT, TMA));
+                         std::min((int)tile_smem(TILE_MAXT, TMA, NC), maxsm));
+    cudaGetLastError();
     return true;
   }();
   (void)once;
   return f;
 }
 
-static void *tile_fn(bool tri, bool snap, bool tma) {
-  if (tma) {
-    if (tri) return snap ? tile_ptr<true, true, true>() : tile_ptr<true, false, true>();
-    return snap ? tile_ptr<false, true, true>() : tile_ptr<false, false, true>();
-  }
-  if (tri) return snap ? tile_ptr<true, true, false>() : tile_ptr<true, false, false>();
-  return snap ? tile_ptr<false, true, false>() : tile_ptr<false, false, false>();
+template <bool TRI, bool SNAP>
+static void *tile_fn_t(bool tma, int nc) {
+  if (!tma) return nc == 2 ? tile_ptr<TRI, SNAP, false, 2>() : tile_ptr<TRI, SNAP, false, 1>();
+  return nc == 2 ? tile_ptr<TRI, SNAP, true, 2>() : tile_ptr<TRI, SNAP, true, 1>();
+}
+static void *tile_fn(bool tri, bool snap, bool tma, int nc) {
+  if (tri) return snap ? tile_fn_t<true, true>(tma, nc) : tile_fn_t<true, false>(tma, nc);
+  return snap ? tile_fn_t<false, true>(tma, nc) : tile_fn_t<false, false>(tma, nc);
 }
 
-// Ring filling of the 3-D warp-tile kernels: TMA tile loads (default) or
-// per-lane cp.async copies (PW_AFD_TMA=0); both give identical results.
+// Ring filling of the 3-D warp-tile kernels: per-lane cp.async copies
+// (default) or TMA tile loads (PW_AFD_TMA=1); both give identical results.
 static bool tile_use_tma() {
   const char *e = getenv("PW_AFD_TMA");
-  return !(e && e[0] == '0');
+  return e && e[0] == '1';
 }
 
-// Tile of the 3-D warp-tile kernel: CTA = G groups x WZ x WX warps of 8 slots
-// x 4 columns, ych planes.  Same score as plan_march without the x-halo term
-// (every warp fetches its own halo).
+// Tile of the 3-D warp-tile kernel: warps of 8 slots x 4 NC columns (NC
+// columns per lane: 1 or 2), ych planes; a CTA holds WZ x WX warps of one
+// group (cp.async ring: the group is the fastest CTA index) or of each of
+// the G groups (TMA ring).
+// Score = useful thread-planes / capacity spent (idle lanes, dead slots,
+// partial waves, the 2-plane prologue of each y chunk) times a latency
+// factor below 24 resident warps per SM, a warp with NC columns counting NC
+// times (its columns are independent instruction streams).  PW_AFD_NC fixes
+// NC, PW_AFD_TILE_G<G>="WZ,WX" the warp layout.
 static int plan_tile(bool tri, int G, int nsm, bool tma, Plan &p) {
   const Geo &g = p.g;
-  void *fn = tile_fn(tri, false, tma);
   const int S = g.lz / 4;
   const int live_slots = ceil_div(g.nz, 4);
-  const double useful = (double)G * live_slots * g.nx * g.ny;
   int fw, fk;
   tile_override(G, fw, fk);
+  int fnc = 0;
+  if (const char *e = getenv("PW_AFD_NC")) fnc = atoi(e);
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   double best = -1;
-  int bz = 0, bx = 0, by = 0;
-  for (int WZ = 1; WZ <= ceil_div(S, TILE_ZW); WZ++) {
-    if (fw && WZ != fw) continue;
-    const int nzc = ceil_div(S, WZ * TILE_ZW);
-    if (WZ > 1 && ceil_div(S, (WZ - 1) * TILE_ZW) == nzc) continue;
-    for (int WX = 1; G * WZ * WX * 32 <= TILE_MAXT; WX++) {
-      if (fk && WX != fk) continue;
-      const int threads = G * WZ * WX * 32;
-      const size_t smem = tile_smem(threads, tma);
-      int occ = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) {
-        cudaGetLastError();
-        occ = 0;
-      }
-      if (occ <= 0) continue;
-      const long long slots = (long long)nsm * occ;
-      const long long tiles = (long long)nzc * ceil_div(g.nx, WX * TILE_XW);
-      const double warps = (double)occ * threads / 32;
-      const double lat = std::min(1.0, warps / 24.0);
-      for (int ych = std::max(4, ceil_div(g.ny, 65535)); ych <= g.ny + 3; ych++) {
-        const int yc = std::min(ych, g.ny);
-        const long long ctas = tiles * ceil_div(g.ny, yc);
-        const long long waves = (ctas + slots - 1) / slots;
-        const double cap = (double)waves * slots * threads * (yc + 2);
-        const double score = useful / cap * lat;
-        // forward runs (one group): among equal scores the larger CTA, which
-        // measured faster (201^3: 4 warps 112.8 us per step, 1 warp 121.8)
-        const bool wider = G == 1 && score > best - 1e-9 && threads > 32 * bz * bx;
-        if (score > best + 1e-9 || wider) {
-          best = std::max(best, score);
-          bz = WZ;
-          bx = WX;
-          by = yc;
+  int bz = 0, bx = 0, by = 0, bnc = 1;
+  const int gpc = tma ? G : 1;  // groups per CTA
+  for (int nc = 1; nc <= TILE_MAXNC; nc++) {
+    if (fnc && nc != fnc) continue;
+    void *fn = tile_fn(tri, false, tma, nc);
+    const double useful = (double)G * live_slots * g.nx * g.ny / nc;  // lane-planes
+    for (int WZ = 1; WZ <= ceil_div(S, TILE_ZW); WZ++) {
+      if (fw && WZ != fw) continue;
+      const int nzc = ceil_div(S, WZ * TILE_ZW);
+      if (WZ > 1 && ceil_div(S, (WZ - 1) * TILE_ZW) == nzc) continue;
+      for (int WX = 1; gpc * WZ * WX * 32 <= TILE_MAXT; WX++) {
+        if (fk && WX != fk) continue;
+        const int threads = gpc * WZ * WX * 32;
+        const size_t smem = tile_smem(threads, tma, nc);
+        if (smem > (size_t)maxsm) continue;
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) {
+          cudaGetLastError();
+          occ = 0;
         }
-        if (yc == g.ny) break;
+        if (occ <= 0) continue;
+        const long long slots = (long long)nsm * occ;
+        const long long tiles = (long long)nzc * ceil_div(g.nx, WX * TILE_XW * nc) * (G / gpc);
+        const double warps = (double)occ * threads / 32;
+        const double lat = std::min(1.0, warps * nc / 24.0);
+        for (int ych = std::max(4, ceil_div(g.ny, 65535)); ych <= g.ny + 3; ych++) {
+          const int yc = std::min(ych, g.ny);
+          const long long ctas = tiles * ceil_div(g.ny, yc);
+          const long long waves = (ctas + slots - 1) / slots;
+          const double cap = (double)waves * slots * threads * (yc + 2);
+          const double score = useful / cap * lat;
+          // forward runs (one group): among equal scores the larger CTA, which
+          // measured faster (201^3: 4 warps 112.8 us per step, 1 warp 121.8)
+          const bool wider = G == 1 && nc == bnc && score > best - 1e-9 && threads > 32 * bz * bx;
+          if (score > best + 1e-9 || wider) {
+            best = std::max(best, score);
+            bz = WZ;
+            bx = WX;
+            by = yc;
+            bnc = nc;
+          }
+          if (yc == g.ny) break;
+        }
       }
     }
   }
   PW_CHECK(best > 0, PW_ERR_SHAPE, "no launchable tile for the step kernel");
-  p.fn = fn;
-  p.fn_snap = tile_fn(tri, true, tma);
+  p.fn = tile_fn(tri, false, tma, bnc);
+  p.fn_snap = tile_fn(tri, true, tma, bnc);
   p.tile = true;
   p.tma = tma;
+  p.nc = bnc;
   p.S = S;
   p.WZ = bz;
   p.WX = bx;
   p.nzc = ceil_div(S, bz * TILE_ZW);
   p.ych = by;
-  p.threads = G * bz * bx * 32;
-  p.smem = tile_smem(p.threads, tma);
-  p.grid = dim3((unsigned)(p.nzc * ceil_div(g.nx, bx * TILE_XW)), (unsigned)ceil_div(g.ny, by), 1);
+  p.threads = gpc * bz * bx * 32;
+  p.smem = tile_smem(p.threads, tma, bnc);
+  p.grid = dim3((unsigned)(p.nzc * ceil_div(g.nx, bx * TILE_XW * bnc) * (G / gpc)),
+                (unsigned)ceil_div(g.ny, by), 1);
   if (getenv("PW_AFD_VERBOSE"))
     fprintf(stderr,
-            "afd tile plan: G=%d S=%d nzc=%d WZ=%d WX=%d ych=%d threads=%d grid=%ux%u score=%.3f "
-            "ring=%s\n",
-            G, S, p.nzc, bz, bx, by, p.threads, p.grid.x, p.grid.y, best, tma ? "tma" : "cp.async");
+            "afd tile plan: G=%d S=%d nzc=%d WZ=%d WX=%d NC=%d ych=%d threads=%d grid=%ux%u "
+            "score=%.3f ring=%s\n",
+            G, S, p.nzc, bz, bx, bnc, by, p.threads, p.grid.x, p.grid.y, best,
+            tma ? "tma" : "cp.async");
   return PW_OK;
 }
 
@@ -1511,6 +1631,7 @@ static int make_plan(const pw_afd_args *a, bool tri, int G, Plan &p, bool allow_
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   p.S = p.ZS = p.KX = p.nzc = p.WPC = p.WZ = p.WX = 0;
   p.tile = p.tma = false;
+  p.nc = 1;
   if (two_d) PW_TRY(plan_march(tri, G, nsm, p));  // 2-D: no x neighbours to stage
   else PW_TRY(plan_tile(tri, G, nsm, allow_tma && tile_use_tma(), p));
   return PW_OK;
@@ -1684,15 +1805,15 @@ static int field_map(const Geo &g, const float *base, int bz, int bx, CUtensorMa
 
 // The two step launches' tensor maps: parity 0 reads buf0 as the current
 // field and buf1 as the previous one, parity 1 the other way round.
-static int tile_maps(const Geo &g, int G, float *const *buf0, float *const *buf1, const float *vv,
-                     TileMaps m[2]) {
+static int tile_maps(const Geo &g, int G, int nc, float *const *buf0, float *const *buf1,
+                     const float *vv, TileMaps m[2]) {
   for (int par = 0; par < 2; par++) {
     memset(&m[par], 0, sizeof(TileMaps));
     for (int i = 0; i < G; i++) {
-      PW_TRY(field_map(g, par ? buf1[i] : buf0[i], 4 * TILE_TZ, TILE_TX, &m[par].a[i]));
-      PW_TRY(field_map(g, par ? buf0[i] : buf1[i], 4 * TILE_ZW, TILE_XW, &m[par].b[i]));
+      PW_TRY(field_map(g, par ? buf1[i] : buf0[i], 4 * TILE_TZ, tile_tx(nc), &m[par].a[i]));
+      PW_TRY(field_map(g, par ? buf0[i] : buf1[i], 4 * TILE_ZW, TILE_XW * nc, &m[par].b[i]));
     }
-    PW_TRY(field_map(g, vv, 4 * TILE_ZW, TILE_XW, &m[par].v));
+    PW_TRY(field_map(g, vv, 4 * TILE_ZW, TILE_XW * nc, &m[par].v));
   }
   return PW_OK;
 }
@@ -1927,7 +2048,7 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
   s.stats = want_stats ? at<unsigned long long>(base, o_stats) : nullptr;
   s.err = p.tma ? at<int>(base, o_err) : nullptr;
   TileMaps maps[2];
-  if (p.tma) PW_TRY(tile_maps(g, G, A, B, vv, maps));
+  if (p.tma) PW_TRY(tile_maps(g, G, p.nc, A, B, vv, maps));
   float *wfd_dev = wfd ? (host ? at<float>(base, o_wfd) : wfd) : nullptr;
   void *fn = p.fn;
   const int threads = p.threads;

@@ -99,6 +99,10 @@ def mid_models():
 
 
 def mid_wavelet(nt):
+    """10 Hz Ricker peaking at 0.12 s, scaled by 1e6 as the reference's FWI
+    demos scale theirs (demos/test_fwi_vel2d.py): fwic's line search compares
+    the misfit with a gradient rescaled to 0.1 / max|g|, so it only makes
+    progress when the data carry the demos' amplitude."""
     t = np.arange(nt) * 0.001 - 0.12
     a = (np.pi * 10.0 * t) ** 2
-    return ((1 - 2 * a) * np.exp(-a)).astype(np.float32)
+    return (1e6 * (1 - 2 * a) * np.exp(-a)).astype(np.float32)
