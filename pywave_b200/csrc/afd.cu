@@ -747,7 +747,35 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> 
   bool src_plane = false;
   if (!TRI)
     for (int s = 0; s < a.ns; s++) src_plane |= (y >= a.sy[s] - 1 && y <= a.sy[s] + 1);
-  const bool clean = L.warp_plain && lyok && !src_plane;
+  // receivers of this plane: forward recording, time-reversal injection
+  bool rec_here[NC], inj[NC];
+  int r_idx[NC];
+  float dval[NC];
+  bool inj_warp = false;
+#pragma unroll
+  for (int j = 0; j < NC; j++) {
+    rec_here[j] = inj[j] = false;
+    r_idx[j] = 0;
+    dval[j] = 0.f;
+  }
+  if (L.warp_rec) {  // warp-uniform: only warps holding the receiver row
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < NC; j++) {
+      const int ix = L.ix[j];
+      rec_here[j] = L.rec_zx[j] && y >= a.ry0 && y < a.ry0 + a.nry;
+      r_idx[j] = rec_here[j] ? (y - a.ry0) * a.nrx + (ix - a.rx0) : 0;
+      if (TRI && rec_here[j]) {
+        inj[j] = a.gid == nullptr ? gi == 0 : a.gid[r_idx[j]] == gi;
+        if (inj[j]) dval[j] = a.tri_dat[(size_t)a.it * nrec + r_idx[j]];
+      }
+      any |= inj[j];
+    }
+    if (TRI) inj_warp = __any_sync(0xffffffffu, any);
+  }
+  // injecting warps take the face-by-face path, which adds the trace after
+  // the update and before the taper
+  const bool clean = L.warp_plain && lyok && !src_plane && !inj_warp;
   const int path = !clean ? 3
                    : (!L.warp_taper_zx ? (wy == 1.f ? 0 : 1)
                                        : (wy == 1.f && !L.warp_edge_zx ? 2 : 3));
@@ -761,17 +789,6 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> 
     const float2 Rf = reinterpret_cast<const float2 *>(pc + ci + 1)[0];  // (x, y)
     const float4 pv = pbv[L.lane + 32 * j];
     const float4 vv4 = pbv[32 * NC + L.lane + 32 * j];
-    bool rec_here = false, inj = false;
-    int r_idx = 0;
-    float dval = 0.f;
-    if (L.warp_rec) {
-      rec_here = L.rec_zx[j] && y >= a.ry0 && y < a.ry0 + a.nry;
-      r_idx = rec_here ? (y - a.ry0) * a.nrx + (ix - a.rx0) : 0;
-      if (TRI && rec_here) {
-        inj = a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi;
-        if (inj) dval = a.tri_dat[(size_t)a.it * nrec + r_idx];
-      }
-    }
     float4 lp;  // Laplacian sums in the reference's order
 #pragma unroll
     for (int e = 0; e < 4; e++) {
@@ -797,7 +814,6 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> 
         float v = fadd(cv, fsub(cv, el(pv, e)));
         set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
       }
-      if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
     } else if (path == 1 || path == 2) {
       float4 f;
 #pragma unroll
@@ -806,12 +822,9 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> 
       for (int e = 0; e < 4; e++) {
         const float cv = el(q2[j], e);
         float v = fadd(cv, fsub(cv, fmul(el(pv, e), el(f, e))));
-        set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
+        v = fadd(v, fmul(el(lp, e), el(vv4, e)));
+        set_el(res, e, fmul(v, el(f, e)));
       }
-      // time reversal injects after the update and before the taper
-      if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
-#pragma unroll
-      for (int e = 0; e < 4; e++) set_el(res, e, fmul(el(res, e), el(f, e)));
     } else {
 #pragma unroll
       for (int e = 0; e < 4; e++) {
@@ -824,6 +837,8 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> 
         const float vve = el(vv4, e);
         float v = fadd(cv, fsub(cv, p));
         v = fadd(v, fmul(lap, vve));
+        // time reversal injects after the update and before the taper
+        if (TRI && inj_warp && inj[j] && e == erz) v = fadd(v, fmul(vve, dval[j]));
         if (!TRI && src_plane) {
           const int iz = L.iz0 + e;
           for (int s = 0; s < a.ns; s++) {
@@ -836,7 +851,6 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> 
         }
         set_el(res, e, v);
       }
-      if (inj) set_el(res, erz, fadd(el(res, erz), fmul(el(vv4, erz), dval)));
 #pragma unroll
       for (int e = 0; e < 4; e++) {
         float v = fmul(el(res, e), L.wz4[e]);
@@ -846,7 +860,8 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> 
       }
     }
     if (L.live[j]) *reinterpret_cast<float4 *>(pB[j]) = res;
-    if (!TRI && rec_here && a.rec && gi == 0) a.rec[(size_t)a.it * nrec + r_idx] = el(res, erz);
+    if (!TRI && L.warp_rec && rec_here[j] && a.rec && gi == 0)
+      a.rec[(size_t)a.it * nrec + r_idx[j]] = el(res, erz);
     if (SNAP) {
       const bool interior = L.live[j] && L.in_zx[j] && y >= a.nby && y < a.nby + a.ny1;
       if (a.wfd && gi == 0 && interior) {
@@ -878,25 +893,29 @@ __device__ __forceinline__ void flush_path_counts(const StepArgs &a, int lane,
   }
 }
 
-// cp.async ring of the warp-tile kernel.  The CTA holds WZ x WX warps of one
-// group (the group index runs fastest over the CTAs, so the G CTAs of a patch
-// run side by side and share vv through L2).  Per warp: an A ring of TILE_NS
-// patches and a B / vv ring of TILE_BV_NS planes of this warp's cells, which
-// are copied two planes before their use.
+// cp.async ring of the warp-tile kernel (CTA = the G group warps of WZ x WX
+// tiles, as with the TMA ring).  NC = 1: one ring of TILE_NS slots, each the
+// A patch of a plane with this warp's B and vv cells of that plane (copied
+// four planes before their use).  NC = 2: an A ring of TILE_NS patches and a
+// separate ring of TILE_BV_NS planes of B and vv, copied two planes before
+// their use, which keeps the larger patches within the shared memory of
+// three resident CTAs.
 constexpr int TILE_BV_NS = 3;
 __host__ __device__ constexpr int tile_cp_ws(int nc) {  // float4 per warp
-  return TILE_NS * tile_tp(nc) + TILE_BV_NS * 64 * nc;
+  return nc == 1 ? TILE_NS * tile_slot(1) : TILE_NS * tile_tp(nc) + TILE_BV_NS * 64 * nc;
 }
 
 template <bool TRI, bool SNAP, int NC>
 __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
   extern __shared__ float4 tsm[];
   constexpr int NS = TILE_NS, D = NS - 3, TP = tile_tp(NC), BVS = 64 * NC;
-  constexpr int CPL = (TP + 31) / 32;  // A-patch copies per lane per plane
+  constexpr bool SPLIT = NC > 1;
+  constexpr int ASTEP = SPLIT ? TP : tile_slot(NC);  // float4 between A slots
+  constexpr int CPL = (TP + 31) / 32;                // A-patch copies per lane per plane
   static_assert(NS == 5, "the y loop is unrolled by the queue length 5");
   const Geo &g = a.g;
   TileLane<NC> L;
-  tile_lane_setup<NC, true>(a, L);
+  tile_lane_setup<NC, false>(a, L);
   const int lane = L.lane, w = threadIdx.x >> 5;
   const float *A = a.cur[0];
   float *B = a.nxt[0];
@@ -908,8 +927,8 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
     }
   const long long sx = g.sx, sy = g.sy;
   const long long safe = sx * g.hx + sy * g.hy;
-  float4 *ring = tsm + (size_t)w * tile_cp_ws(NC);  // NS A patches
-  float4 *bvring = ring + NS * TP;                  // TILE_BV_NS planes of [B, vv]
+  float4 *ring = tsm + (size_t)w * tile_cp_ws(NC);  // A slots (with B / vv when !SPLIT)
+  float4 *bvring = ring + NS * TP;                  // SPLIT: TILE_BV_NS planes of [B, vv]
   const int y0 = blockIdx.y * a.ych;
   const int y1 = min(g.ny, y0 + a.ych);
 
@@ -935,7 +954,7 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
   int next_a = y0, next_bv = y0;
   auto issue_a = [&](int rs) {  // A patch of plane next_a into A slot rs
     if (next_a <= y1 + 1) {
-      float4 *dst = ring + rs * TP;
+      float4 *dst = ring + rs * ASTEP;
 #pragma unroll
       for (int k = 0; k < CPL; k++) {
         const int j = lane + 32 * k;
@@ -945,16 +964,18 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
     }
     next_a++;
   };
-  auto issue_bv = [&](int bs) {  // B and vv of plane next_bv into B/vv slot bs
+  auto issue_bv = [&](float4 *dst) {  // B and vv of plane next_bv into dst
     if (next_bv < y1) {
-      float4 *dst = bvring + bs * BVS;
 #pragma unroll
       for (int j = 0; j < NC; j++) {
         cp16(dst + lane + 32 * j, cB[j], L.valid[j]);
         cp16(dst + 32 * NC + lane + 32 * j, cV[j], L.valid[j]);
-        cB[j] += sy;
-        cV[j] += sy;
       }
+    }
+#pragma unroll
+    for (int j = 0; j < NC; j++) {
+      cB[j] += sy;
+      cV[j] += sy;
     }
     next_bv++;
   };
@@ -975,31 +996,49 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
     q[3][j] = __ldg(reinterpret_cast<const float4 *>(pA + sy * (y0 + 1)));
   }
   float wyn = y0 < y1 ? __ldg(a.wy + y0) : 1.f;
-  // commit groups: {A y0..y0+2, B/vv y0..y0+1}, {A y0+3}, then per plane y
-  // {A y+4, B/vv y+2}; at plane y the group of plane y-2 (or the first two)
-  // holds A y+2 and B/vv y, so D = 2 groups may stay in flight
-  issue_a(0);
-  issue_a(1);
-  issue_a(2);
-  issue_bv(0);
-  issue_bv(1);
-  cp_commit();
-  issue_a(3);
-  cp_commit();
-  int bvs = 0;  // B/vv slot of plane y
+  int bvs = 0;  // SPLIT: B/vv slot of plane y
+  if constexpr (!SPLIT) {
+    // one commit group per plane (A patch and B / vv of that plane); at plane
+    // y the group of plane y + 2 must be complete, so D = 2 may stay in flight
+#pragma unroll
+    for (int j = 0; j < 2 + D; j++) {
+      issue_a(j);
+      issue_bv(ring + j * ASTEP + TP);
+      cp_commit();
+    }
+  } else {
+    // commit groups: {A y0..y0+2, B/vv y0..y0+1}, {A y0+3}, then per plane y
+    // {A y+4, B/vv y+2}; at plane y the group of plane y-2 (or the first two)
+    // holds A y+2 and B/vv y, so D = 2 groups may stay in flight
+    issue_a(0);
+    issue_a(1);
+    issue_a(2);
+    issue_bv(bvring);
+    issue_bv(bvring + BVS);
+    cp_commit();
+    issue_a(3);
+    cp_commit();
+  }
 
   for (int yb = y0; yb < y1; yb += NS) {
 #pragma unroll
     for (int u = 0; u < NS; u++) {
       const int y = yb + u;
       if (y < y1) {
-        issue_a((u + 4) % NS);                               // into the slot plane y - 1 left
-        issue_bv(bvs == 0 ? 2 : bvs - 1);                    // (bvs + 2) % 3: plane y - 1's
+        const float4 *pbv;
+        issue_a((u + 4) % NS);  // into the slot plane y - 1 left
+        if constexpr (!SPLIT) {
+          issue_bv(ring + ((u + 4) % NS) * ASTEP + TP);
+          pbv = ring + u * ASTEP + TP;
+        } else {
+          issue_bv(bvring + (bvs == 0 ? 2 : bvs - 1) * BVS);  // (bvs + 2) % 3: plane y - 1's
+          pbv = bvring + bvs * BVS;
+        }
         cp_commit();
         cp_wait<D>();
         __syncwarp();
-        const float4 *slot = ring + u * TP;
-        const float4 *lead = ring + ((u + 2) % NS) * TP;
+        const float4 *slot = ring + u * ASTEP;
+        const float4 *lead = ring + ((u + 2) % NS) * ASTEP;
 #pragma unroll
         for (int j = 0; j < NC; j++)
           q[(u + 4) % NS][j] = lead[(L.xl + TILE_XW * j + 2) * TILE_TZ + L.zl + 1];
@@ -1007,11 +1046,11 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
         if (y + 1 < y1) wyn = __ldg(a.wy + y + 1);
         const int path = tile_plane<TRI, SNAP, NC>(a, L, y, wy, q[u], q[(u + 1) % NS],
                                                    q[(u + 2) % NS], q[(u + 3) % NS],
-                                                   q[(u + 4) % NS], slot, bvring + bvs * BVS, pB);
+                                                   q[(u + 4) % NS], slot, pbv, pB);
         if (counting) pcount += 1ull << (16 * path);
 #pragma unroll
         for (int j = 0; j < NC; j++) pB[j] += sy;
-        bvs = bvs == 2 ? 0 : bvs + 1;
+        if constexpr (SPLIT) bvs = bvs == 2 ? 0 : bvs + 1;
         __syncwarp();  // the ring slots refilled next iteration were read above
       }
     }
@@ -1495,9 +1534,8 @@ static bool tile_use_tma() {
 }
 
 // Tile of the 3-D warp-tile kernel: warps of 8 slots x 4 NC columns (NC
-// columns per lane: 1 or 2), ych planes; a CTA holds WZ x WX warps of one
-// group (cp.async ring: the group is the fastest CTA index) or of each of
-// the G groups (TMA ring).
+// columns per lane: 1 or 2), ych planes; a CTA holds the G group warps of
+// WZ x WX tiles.
 // Score = useful thread-planes / capacity spent (idle lanes, dead slots,
 // partial waves, the 2-plane prologue of each y chunk) times a latency
 // factor below 24 resident warps per SM, a warp with NC columns counting NC
@@ -1516,7 +1554,7 @@ static int plan_tile(bool tri, int G, int nsm, bool tma, Plan &p) {
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   double best = -1;
   int bz = 0, bx = 0, by = 0, bnc = 1;
-  const int gpc = tma ? G : 1;  // groups per CTA
+  const int gpc = G;  // groups per CTA
   for (int nc = 1; nc <= TILE_MAXNC; nc++) {
     if (fnc && nc != fnc) continue;
     void *fn = tile_fn(tri, false, tma, nc);
