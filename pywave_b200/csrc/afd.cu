@@ -1538,17 +1538,18 @@ static bool tile_use_tma() {
 // WZ x WX tiles.
 // Score = useful thread-planes / capacity spent (idle lanes, dead slots,
 // partial waves, the 2-plane prologue of each y chunk) times a latency
-// factor below 24 resident warps per SM, a warp with NC columns counting NC
-// times (its columns are independent instruction streams).  PW_AFD_NC fixes
-// NC, PW_AFD_TILE_G<G>="WZ,WX" the warp layout.
+// factor below 24 resident warps per SM.  One column per lane unless
+// PW_AFD_NC=2: on the 261^3 TRI step two columns issued 6% fewer
+// instructions but ran 12% slower (12 instead of 16 resident warps);
+// PW_AFD_TILE_G<G>="WZ,WX" fixes the warp layout.
 static int plan_tile(bool tri, int G, int nsm, bool tma, Plan &p) {
   const Geo &g = p.g;
   const int S = g.lz / 4;
   const int live_slots = ceil_div(g.nz, 4);
   int fw, fk;
   tile_override(G, fw, fk);
-  int fnc = 0;
-  if (const char *e = getenv("PW_AFD_NC")) fnc = atoi(e);
+  int fnc = 1;
+  if (const char *e = getenv("PW_AFD_NC")) fnc = std::max(1, std::min(TILE_MAXNC, atoi(e)));
   int dev = 0, maxsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -1577,7 +1578,7 @@ static int plan_tile(bool tri, int G, int nsm, bool tma, Plan &p) {
         const long long slots = (long long)nsm * occ;
         const long long tiles = (long long)nzc * ceil_div(g.nx, WX * TILE_XW * nc) * (G / gpc);
         const double warps = (double)occ * threads / 32;
-        const double lat = std::min(1.0, warps * nc / 24.0);
+        const double lat = std::min(1.0, warps / 24.0);
         for (int ych = std::max(4, ceil_div(g.ny, 65535)); ych <= g.ny + 3; ych++) {
           const int yc = std::min(ych, g.ny);
           const long long ctas = tiles * ceil_div(g.ny, yc);
