@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--groups", type=int, default=4)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-fwi2d", action="store_true",
+                   help="tri3d: skip the secondary 2-D FWI gradients/s field")
     p.add_argument("--workload", default="tri3d", choices=["tri3d", "fwi2d", "batch2d", "c1"],
                    help="tri3d: the 3-D TRI image (default); fwi2d: 2-D FWI gradients/s; "
                         "batch2d: uneven 2-D forward shots in one batch; c1: one 2-D shot")
@@ -161,41 +163,75 @@ def pool_map(fn, arglist, timeout_s=600):
         pool.join()
 
 
-def reference_sample(n, nt_s, seed, workers):
-    """The reference's own afd3dc (compiled from its sources into oracle/_ref;
-    the oracle port when that is absent), time-reversing one receiver group
-    for nt_s steps on the full grid, in `workers` independent processes."""
-    res = pool_map(_ref_worker, [(n, nt_s, seed + w) for w in range(workers)])
-    wall = max(r[0] for r in res)
-    kind = res[0][1]
-    pts = (n + 2 * NBT) ** 3 * nt_s * workers
-    return pts / wall / 1e9, kind, wall
+REF_STEPS = (4, 12)  # two step counts per reference call: their difference excludes set-up
 
 
-def _ref_worker(n, nt_s, seed):
+def ref_inputs(n, seed):
+    """The benchmark's own velocity model (c2_model, the GPU arm's rank-0
+    seed) and time-reversal traces of the first receiver group's x-band
+    (seeded band-limited noise at the amplitude of the recorded traces) for
+    the reference's time reversal; written to a temporary .npz that the
+    spawned workers read."""
+    from scipy.ndimage import gaussian_filter1d
+    vel, _, _, _ = c2_model(n, seed)
+    rng = np.random.default_rng(seed)
+    nt_s = max(REF_STEPS)
+    dat = np.zeros((nt_s, n, n), np.float32)
+    band = n // 4
+    dat[:, :band, :] = 1e-2 * gaussian_filter1d(rng.standard_normal((nt_s, band, n)), 2.0,
+                                                axis=0)
+    fd, path = tempfile.mkstemp(suffix=".npz")
+    os.close(fd)
+    np.savez(path, vel=vel, dat=dat)
+    return path
+
+
+def reference_sample(n, path, workers):
+    """Per-step rate of the reference's own afd3dc (compiled from its sources
+    into oracle/_ref; the oracle port when that is absent) time-reversing one
+    receiver group on the full grid, in `workers` independent processes.
+    Each process times a call of REF_STEPS[0] and one of REF_STEPS[1] steps;
+    the difference of the two walls is the time of the extra steps alone
+    (the reference's per-call set-up -- allocation, vel_expand and the
+    unused pseudo-spectral Laplacian of wave_fdm.c:28-200 -- cancels).
+    Returns (Gpt/s over all workers, kind, per-step seconds, set-up seconds)."""
+    res = pool_map(_ref_worker, [(n, path)] * workers)
+    d = max(r[1] - r[0] for r in res)  # slowest worker's extra-steps time
+    kind = res[0][2]
+    extra = REF_STEPS[1] - REF_STEPS[0]
+    pts = (n + 2 * NBT) ** 3 * extra * workers
+    per_step = d / extra
+    setup = max(r[0] for r in res) - REF_STEPS[0] * per_step
+    return pts / d / 1e9, kind, per_step, setup
+
+
+def _ref_worker(n, path):
     sys.path.insert(0, ROOT)
     devnull = os.open(os.devnull, os.O_WRONLY)
     os.dup2(devnull, 1)
-    rng = np.random.default_rng(seed)
-    vel = (2000 + 500 * rng.random((n, n, n))).astype(np.float32)
-    dat = np.zeros((nt_s, n, n), np.float32)
-    dat[:, : n // 4, :] = rng.standard_normal((nt_s, n // 4, n)).astype(np.float32) * 1e-3
+    with np.load(path) as z:
+        vel, dat = z["vel"], z["dat"]
+    vflat = vel.flatten(order="F")
     refdir = os.path.join(ROOT, "oracle", "_ref")
+    walls = []
     try:
         sys.path.insert(0, refdir)
         import afdcfun  # the reference's own extension module
         kind = "reference"
-        t0 = time.perf_counter()
-        afdcfun.afd3dc(vel.flatten(order="F"), dat.flatten(order="F"), 1, nt_s, n, n, n, -1, 0, 4,
-                       0, 1, NBT, CT, DT, 0.0, H, 0.0, H, 0.0, H)
-        wall = time.perf_counter() - t0
+        for nt_s in REF_STEPS:
+            d = dat[-nt_s:].flatten(order="F")
+            t0 = time.perf_counter()
+            afdcfun.afd3dc(vflat, d, 1, nt_s, n, n, n, -1, 0, 4, 0, 1, NBT, CT, DT, 0.0, H, 0.0, H,
+                           0.0, H)
+            walls.append(time.perf_counter() - t0)
     except ImportError:
         from oracle import oracle as O
         kind = "port"
-        t0 = time.perf_counter()
-        O.afd(vel, nt_s, DT, (H, H, H), nbt=NBT, ct=CT, tri=True, dat=dat, jsnap=4)
-        wall = time.perf_counter() - t0
-    return wall, kind
+        for nt_s in REF_STEPS:
+            t0 = time.perf_counter()
+            O.afd(vel, nt_s, DT, (H, H, H), nbt=NBT, ct=CT, tri=True, dat=dat[-nt_s:], jsnap=4)
+            walls.append(time.perf_counter() - t0)
+    return walls[0], walls[1], kind
 
 
 def max_over_ranks(x, world, device="cuda"):
@@ -219,25 +255,34 @@ def run_reference(args, rank):
     if rank != 0:
         return
     n = args.n
-    nt_s = 4
     workers = max(1, min(os.cpu_count() or 1, 16))
-    vals = []
-    for i in range(args.warmup + args.steps):
-        v, kind, wall = reference_sample(n, nt_s, 100 + i, workers)
-        if i >= args.warmup:
-            vals.append(v)
+    path = ref_inputs(n, 1234)
+    vals, steps_s, setups = [], [], []
+    try:
+        for i in range(args.warmup + args.steps):
+            v, kind, per_step, setup = reference_sample(n, path, workers)
+            if i >= args.warmup:
+                vals.append(v)
+                steps_s.append(per_step)
+                setups.append(setup)
+    finally:
+        os.unlink(path)
     value = statistics.median(vals)
+    sample = (f"afd3dc time reversal of the first receiver group on the {n + 2 * NBT}^3 expanded "
+              f"grid of the benchmark's velocity model, {workers} independent single-threaded "
+              f"processes; per-step rate from calls of {REF_STEPS[0]} and {REF_STEPS[1]} steps "
+              f"(difference of walls: {statistics.median(steps_s):.3f} s per step, the "
+              f"{statistics.median(setups):.2f} s per-call set-up excluded)")
     line = {
         "impl": "reference", "metric": "Gpt-updates/s (3-D TRI, 4 lockstep groups)",
         "value": value, "unit": "Gpt/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic",
+        "dtype": "f32", "data": "synthetic (the benchmark's seeded velocity model; seeded traces)",
         "config": {"workload": f"3-D TRI image {n}^3 h=10m nt={args.nt} nbt={NBT} "
-                               f"groups={args.groups}", "sample": f"{nt_s} steps x {workers} procs"},
+                               f"groups={args.groups} jsnap=4", "same_model": True,
+                   "sample": f"{REF_STEPS[0]} and {REF_STEPS[1]} steps x {workers} procs"},
         "cpu_baseline": {"value": value, "unit": "Gpt/s", "cores": workers, "kind": kind,
-                         "sample": f"afd3dc time reversal of one group, {nt_s} of {args.nt} steps "
-                                   f"on the {n + 2 * NBT}^3 expanded grid, {workers} independent "
-                                   f"single-threaded processes"},
+                         "sample": sample},
         "e2e": {"value": value, "unit": "Gpt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -312,6 +357,78 @@ def _fwi_ref_worker_spawned(nt_s):
     return pool_map(_fwi_ref_worker, [(nt_s, 7)])[0]
 
 
+class FwiBench:
+    """Device state of the 2-D FWI gradient measurement: the seeded models,
+    observed data modelled on the GPU from the true model, and a timer of
+    pw_pfwi_gradient calls from the start model."""
+
+    def __init__(self, ns, nt, seed, stream):
+        import ctypes
+        import torch
+        from pywave_b200 import _lib as L
+        from pywave_b200 import fwi
+        self.L, self.lib, self.st = L, L.lib(), stream
+        self.vt, self.vs = fwi2d_models(seed)
+        self.par = fwi2d_par(ns, nt)
+        self.wav = fwi2d_wavelet(nt)
+        self.a = fwi.fwi_args(self.par, 0)
+        dev = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).cuda()
+        self.vt_d = dev(self.vt.flatten(order="F"))
+        self.vs_d = dev(self.vs.flatten(order="F"))
+        self.wav_d = dev(self.wav)
+        self.dobs_d = torch.empty(ns * FWI_NX * nt, device="cuda")
+        L.check(self.lib.pw_pfwi_forward(self.a, self.vt_d.data_ptr(), self.wav_d.data_ptr(),
+                                         self.dobs_d.data_ptr(), stream))
+        self.g_d = torch.empty(FWI_NZ * FWI_NX, device="cuda")
+        self.J = ctypes.c_double(0.0)
+
+    def grad(self, flags, mode):
+        import ctypes
+        self.a.flags = flags
+        self.L.check(self.lib.pw_pfwi_gradient(self.a, mode, self.vs_d.data_ptr(),
+                                               self.wav_d.data_ptr(), self.dobs_d.data_ptr(), None,
+                                               self.g_d.data_ptr(), ctypes.byref(self.J), 0,
+                                               self.st))
+        return self.L.last_timing()
+
+    def timed(self, flags, steps, warmup, world, mode):
+        """(max-over-ranks ms of `steps` gradients, median loop ms, launches)."""
+        import torch
+        import torch.distributed as dist
+        for _ in range(warmup):
+            self.grad(flags, mode)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        loops, launches = [], 0
+        e0.record()
+        for _ in range(steps):
+            ms, nst, tot = self.grad(flags, mode)
+            loops.append(ms)
+            launches += tot
+        e1.record()
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), world), statistics.median(loops), launches
+
+
+def fwi2d_secondary(world, rank, stream, steps=2):
+    """The 2-D FWI benchmark's headline pair, for the default line: exact
+    gradients/s with the 32 shots batched, and with one shot at a time
+    (PW_PER_SHOT, the plain per-shot path), same models and data."""
+    from pywave_b200 import _lib as L
+    ns, nt = 32, 2000
+    fb = FwiBench(ns, nt, 11 + rank, stream)
+    ms_b, _, lb = fb.timed(0, steps, 1, world, L.PW_GRAD_EXACT)
+    ms_p, _, lp = fb.timed(L.PW_PER_SHOT, 1, 1, world, L.PW_GRAD_EXACT)
+    batched = job_rate(1, steps, world, ms_b)
+    plain = job_rate(1, 1, world, ms_p)
+    return {"workload": f"2-D FWI exact gradient {FWI_NZ}x{FWI_NX} h=10m nt={nt} shots={ns} "
+                        f"nb={FWI_NB}", "batched": batched, "plain_per_shot": plain,
+            "unit": "gradients/s", "batched_over_plain": batched / plain,
+            "steps": {"batched": steps, "plain_per_shot": 1}, "gpu_launches": lb + lp}
+
+
 def run_fwi2d(args, world, rank, local):
     ns, nt = args.shots, args.fwi_nt
     pad = (FWI_NZ + 2 * FWI_NB) * (FWI_NX + 2 * FWI_NB)
@@ -352,41 +469,11 @@ def run_fwi2d(args, world, rank, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     st = torch.cuda.current_stream().cuda_stream
     lib = L.lib()
-    vt, vs = fwi2d_models(11 + rank)
-    par = fwi2d_par(ns, nt)
-    wav = fwi2d_wavelet(nt)
-    a = fwi.fwi_args(par, 0)
-    dev = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).cuda()
-    vt_d = dev(vt.flatten(order="F"))
-    vs_d = dev(vs.flatten(order="F"))
-    wav_d = dev(wav)
-    dobs_d = torch.empty(ns * FWI_NX * nt, device="cuda")
-    L.check(lib.pw_pfwi_forward(a, vt_d.data_ptr(), wav_d.data_ptr(), dobs_d.data_ptr(), st))
-    g_d = torch.empty(FWI_NZ * FWI_NX, device="cuda")
-    J = ctypes.c_double(0.0)
-
-    def grad(flags, mode):
-        a.flags = flags
-        L.check(lib.pw_pfwi_gradient(a, mode, vs_d.data_ptr(), wav_d.data_ptr(), dobs_d.data_ptr(),
-                                     None, g_d.data_ptr(), ctypes.byref(J), 0, st))
-        return L.last_timing()
+    fb = FwiBench(ns, nt, 11 + rank, st)
+    vs, wav, par, dobs_d, J = fb.vs, fb.wav, fb.par, fb.dobs_d, fb.J
 
     def timed(flags, steps, mode=L.PW_GRAD_EXACT):
-        for _ in range(args.warmup):
-            grad(flags, mode)
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        loops, launches = [], 0
-        e0.record()
-        for _ in range(steps):
-            ms, nst, tot = grad(flags, mode)
-            loops.append(ms)
-            launches += tot
-        e1.record()
-        torch.cuda.synchronize()
-        return max_over_ranks(e0.elapsed_time(e1), world), statistics.median(loops), launches
+        return fb.timed(flags, steps, args.warmup, world, mode)
 
     clk = Clocks(local)
     clk.start()
@@ -463,6 +550,8 @@ def run_fwi2d(args, world, rank, local):
                          "frac": achieved / peak, "traffic": traffic,
                          "traffic_unit": "bytes per gradient (ncu, one FWD + one ADJ_EXACT "
                                          "launch per step)",
+                         "traffic_source": "stored ncu figure (profiles/traffic.json), "
+                                           "not measured in this run",
                          "kernel": "pf_step_kernel FWD + ADJ_EXACT (whole gradient loop)",
                          "alg_bytes_per_gradient": alg, "loop_ms": loop_b,
                          "peak_source": peak_kind},
@@ -960,6 +1049,8 @@ def main():
     alg_bytes = cells * (12 * G + 4) + cells * 8 / 4  # fields + vv per step, image RMW every 4th
     peak, peak_kind = peaks()
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+    # DRAM bytes of one step launch from an ncu capture of this workload
+    # (profiles/traffic.json, a stored figure: not measured in this run)
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
@@ -967,17 +1058,27 @@ def main():
     except (OSError, ValueError):
         pass
 
+    # secondary field: the 2-D FWI gradient benchmark's batched / per-shot pair
+    fwi2d = None
+    if not args.no_fwi2d and n == 201 and nt == 1501:
+        fwi2d = fwi2d_secondary(world, rank, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        path = ref_inputs(n, 1234)
         try:
-            workers = 1
-            v, kind, wall = reference_sample(n, 16, 7, workers)
-            cpu = {"value": v, "unit": "Gpt/s", "cores": workers, "kind": kind,
-                   "sample": f"afd3dc time reversal of one group, 16 of {nt} steps on the "
-                             f"{n + 2 * NBT}^3 expanded grid, 1 core ({wall:.1f} s)"}
+            v, kind, per_step, setup = reference_sample(n, path, 1)
+            cpu = {"value": v, "unit": "Gpt/s", "cores": 1, "kind": kind,
+                   "sample": f"afd3dc time reversal of the first receiver group on the "
+                             f"{n + 2 * NBT}^3 expanded grid of the same velocity model, 1 core; "
+                             f"calls of {REF_STEPS[0]} and {REF_STEPS[1]} steps, per-step time "
+                             f"{per_step:.3f} s from their difference ({setup:.2f} s per-call "
+                             f"set-up excluded)"}
         except Exception as ex:  # noqa: BLE001
             cpu = {"value": None, "unit": "Gpt/s", "cores": 1, "kind": "reference",
                    "sample": f"failed: {ex!r}"[:200]}
+        finally:
+            os.unlink(path)
 
     if rank == 0:
         line = {
@@ -995,10 +1096,14 @@ def main():
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": f"tile_kernel<TRI> x{G} groups + image_kernel every 4th step", "kernel_ms": kern_ms,
-                         "alg_bytes_per_launch": alg_bytes, "peak_source": peak_kind},
+                         "traffic_source": "stored ncu figure (profiles/traffic.json), "
+                                           "not measured in this run",
+                         "kernel": f"tile_kernel<TRI> x{G} groups + image_kernel every 4th step",
+                         "kernel_ms": kern_ms, "alg_bytes_per_launch": alg_bytes,
+                         "peak_source": peak_kind},
             "cpu_baseline": cpu,
             "clocks": clocks,
+            "fwi2d": fwi2d,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
