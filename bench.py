@@ -292,6 +292,7 @@ def run_reference(args, rank):
 # fwi2d: FWI gradients/s on a 300 x 600 model at 10 m (km units as pfwi uses)
 # --------------------------------------------------------------------------
 FWI_NZ, FWI_NX, FWI_H, FWI_DT, FWI_NB, FWI_COEF, FWI_F0 = 300, 600, 0.01, 0.001, 60, 0.005, 10.0
+FWI_BUDGET = 40 << 30  # device bytes the exact gradient's checkpoints may hold
 
 
 def fwi2d_models(seed):
@@ -371,7 +372,7 @@ class FwiBench:
         self.vt, self.vs = fwi2d_models(seed)
         self.par = fwi2d_par(ns, nt)
         self.wav = fwi2d_wavelet(nt)
-        self.a = fwi.fwi_args(self.par, 0)
+        self.a = fwi.fwi_args(self.par, 0, FWI_BUDGET)
         dev = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).cuda()
         self.vt_d = dev(self.vt.flatten(order="F"))
         self.vs_d = dev(self.vs.flatten(order="F"))
@@ -411,6 +412,12 @@ class FwiBench:
         torch.cuda.synchronize()
         return max_over_ranks(e0.elapsed_time(e1), world), statistics.median(loops), launches
 
+    def plan(self):
+        """The last exact gradient's checkpoint plan, as a JSON field."""
+        k, nsb, nbytes, rc = self.L.last_fwi_plan()
+        return {"budget_bytes": FWI_BUDGET, "interval_k": k, "shots_per_batch": nsb,
+                "device_bytes": nbytes, "recompute_factor": rc}
+
 
 def fwi2d_secondary(world, rank, stream, steps=2):
     """The 2-D FWI benchmark's headline pair, for the default line: exact
@@ -420,13 +427,15 @@ def fwi2d_secondary(world, rank, stream, steps=2):
     ns, nt = 32, 2000
     fb = FwiBench(ns, nt, 11 + rank, stream)
     ms_b, _, lb = fb.timed(0, steps, 1, world, L.PW_GRAD_EXACT)
+    plan = fb.plan()
     ms_p, _, lp = fb.timed(L.PW_PER_SHOT, 1, 1, world, L.PW_GRAD_EXACT)
     batched = job_rate(1, steps, world, ms_b)
     plain = job_rate(1, 1, world, ms_p)
     return {"workload": f"2-D FWI exact gradient {FWI_NZ}x{FWI_NX} h=10m nt={nt} shots={ns} "
                         f"nb={FWI_NB}", "batched": batched, "plain_per_shot": plain,
             "unit": "gradients/s", "batched_over_plain": batched / plain,
-            "steps": {"batched": steps, "plain_per_shot": 1}, "gpu_launches": lb + lp}
+            "steps": {"batched": steps, "plain_per_shot": 1}, "gpu_launches": lb + lp,
+            "checkpoint": plan}
 
 
 def run_fwi2d(args, world, rank, local):
@@ -479,6 +488,7 @@ def run_fwi2d(args, world, rank, local):
     clk.start()
     ms_b, loop_b, launches = timed(0, args.steps)
     clocks = clk.stop()
+    plan = fb.plan()
     value = job_rate(1, args.steps, world, ms_b)
     nplain = max(1, args.steps // 2)
     ms_p, _, _ = timed(L.PW_PER_SHOT, nplain)
@@ -491,7 +501,7 @@ def run_fwi2d(args, world, rank, local):
         vs_h = torch.from_numpy(np.ascontiguousarray(vs.flatten(order="F"))).pin_memory()
         dobs_h = dobs_d.cpu().pin_memory()
         g_h = torch.empty(FWI_NZ * FWI_NX).pin_memory()
-        ah = fwi.fwi_args(par, L.PW_HOST_PTRS)
+        ah = fwi.fwi_args(par, L.PW_HOST_PTRS, FWI_BUDGET)
         wav_h = torch.from_numpy(wav).pin_memory()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -506,9 +516,10 @@ def run_fwi2d(args, world, rank, local):
                "d2h_bytes_per_step": int(g_h.numel() * 4 + 8)}
 
     peak, peak_kind = peaks()
-    # forward 20 B (cur, prev, V read; next, term write) + exact adjoint 28 B
-    # (cur, prev, V, term, gradient read; next, gradient write) per
-    # point-step-shot: the planner keeps every forward term at this size
+    # algorithmic bytes per padded point-step-shot: forward 20 B (cur, prev,
+    # V read; next, term write) + exact adjoint 28 B (cur, prev, V, term,
+    # gradient read; next, gradient write) = 48 B; recomputed forward steps
+    # (plan["recompute_factor"] - 1 of them per step) are not counted
     alg = 48.0 * pad * nt * ns
     traffic = None
     try:
@@ -545,6 +556,7 @@ def run_fwi2d(args, world, rank, local):
             "batched_over_plain": value / plain,
             "reference_mode_gradient": {"value": ref_mode, "unit": "gradients/s",
                                         "note": "gradient_av imaging, batched"},
+            "checkpoint": plan,
             "e2e": e2e, "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

@@ -147,6 +147,8 @@ typedef struct pw_fwi_args {
   int niter;       /* L-BFGS iterations (pw_fwi) */
   int sz, rz;      /* source / receiver depth below the top (pfwi.c: 5 and 1) */
   int flags;       /* PW_HOST_PTRS | PW_NO_CFL_CHECK | PW_PER_SHOT */
+  long long hbm_budget; /* bytes of device memory the exact gradient's checkpoints, segment
+                           buffer and wavefields may hold; 0 = a quarter of the device */
 } pw_fwi_args;
 
 /* Fills a pw_fwi_args from pfwi's float parameter array (pfwi.c:691-713
@@ -170,10 +172,19 @@ int pw_pfwi_forward(const pw_fwi_args *a, const float *vel, const float *wav, fl
  *   grad    [nx][nz] dJ/dv (EXACT) or the reference's raw gradient (REFERENCE)
  *   misfit  0.5*sum(r^2) in FP64 (REFERENCE: unweighted residual as the
  *           reference; EXACT: 0.5*sum(w r^2), consistent with grad)
- *   ckpt_k  checkpoint interval of the EXACT mode (0 = autotuned) */
+ *   ckpt_k  checkpoint interval of the EXACT mode (0 = planned under a->hbm_budget,
+ *           see pw_last_fwi_plan) */
 int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const float *wav,
                      const float *dobs, const float *weight, float *grad, double *misfit,
                      int ckpt_k, void *stream);
+
+/* Checkpoint plan of the calling thread's last PW_GRAD_EXACT gradient: the
+ * interval k, the shots per batch, the device bytes the call held and the
+ * recompute factor (forward steps run / nt; 1 = nothing recomputed).  The
+ * planner fits pw_fwi_args.hbm_budget and minimises recompute.  No
+ * counterpart in the reference, which stores every snapshot
+ * (wave_fwigradient.c:116). */
+int pw_last_fwi_plan(int *ckpt_k, int *shots_per_batch, long long *bytes, double *recompute);
 
 /* gradient_av's tail (wave_fwigradient.c:244-255): triangle smoothing
  * rect x rect (wave_fwiutil.c:298-335) and the scale factor; *scaling <= 0 on

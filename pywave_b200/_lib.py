@@ -62,7 +62,8 @@ class FwiArgs(C.Structure):
                 ("ot", C.c_float), ("ns", C.c_int), ("ds", C.c_float), ("os", C.c_float),
                 ("nb", C.c_int), ("coef", C.c_float), ("f0", C.c_float),
                 ("acqui_type", C.c_int), ("interval", C.c_int), ("niter", C.c_int),
-                ("sz", C.c_int), ("rz", C.c_int), ("flags", C.c_int)]
+                ("sz", C.c_int), ("rz", C.c_int), ("flags", C.c_int),
+                ("hbm_budget", C.c_longlong)]
 
 
 _lib = None
@@ -82,6 +83,8 @@ _SIGS = {
     "pw_gradient_postprocess": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int,
                                           _vp]),
     "pw_fwi": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp, C.POINTER(C.c_int), _vp]),
+    "pw_last_fwi_plan": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
     "pw_last_error": (C.c_char_p, []),
     "pw_version": (C.c_char_p, []),
     "pw_release_cache": (C.c_int, []),
@@ -139,6 +142,14 @@ def last_timing():
     ms, n, t = C.c_double(), C.c_longlong(), C.c_longlong()
     lib().pw_last_timing(C.byref(ms), C.byref(n), C.byref(t))
     return ms.value, n.value, t.value
+
+
+def last_fwi_plan():
+    """(checkpoint interval, shots per batch, device bytes, recompute factor)
+    of this thread's last exact gradient."""
+    k, nsb, b, rc = C.c_int(), C.c_int(), C.c_longlong(), C.c_double()
+    lib().pw_last_fwi_plan(C.byref(k), C.byref(nsb), C.byref(b), C.byref(rc))
+    return k.value, nsb.value, b.value, rc.value
 
 
 def f32(a):

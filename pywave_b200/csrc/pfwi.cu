@@ -1083,44 +1083,102 @@ extern "C" int pw_pfwi_forward(const pw_fwi_args *a, const float *vel, const flo
   return PW_OK;
 }
 
-// Checkpoint interval of the exact gradient.  The segment buffer holds k term
-// fields per shot and the checkpoints two fields every k steps.  The forward
-// pass keeps the terms of the last segment, so the backward pass recomputes
-// nt - k steps: k is the largest interval whose working set fits the HBM
-// budget (80% of the free memory plus the workspace this call reuses; k = nt
-// recomputes nothing).  When not even
-// k = sqrt(2 nt), the interval of the smallest working set, fits, the shot
-// batch shrinks first.
-static void plan_exact(const Setup &S, int ckpt_k, size_t held, int &k, int &nsb) {
+// Checkpoint plan of the exact gradient under an HBM budget.  The working
+// set of a batch of nsb shots is, in field-sized buffers per shot: the two
+// wavefield pairs, the gradient slice and traces (about 5), the checkpoints
+// (two fields every k steps) and the segment buffer of k forward terms.  The
+// forward pass keeps the terms of the last segment, so the backward pass
+// recomputes the (nck - 1) k steps before it: the recompute factor (forward
+// steps run / nt) is 1 + (nck - 1) k / nt.  Once the shots of a batch fill
+// the GPU a step costs in proportion to its shots, so the planner picks,
+// over batch sizes nsb = ns, ns/2, ... (down to 2 shots, the smallest whose
+// shot slices are summed in the same order as a full batch), the largest k
+// that fits the budget, and among those the plan with the least recompute,
+// then the largest batch.  k = nt stores every term and recomputes nothing;
+// a fixed ckpt_k > 0 keeps k and only shrinks the batch if needed.
+struct ExactPlan {
+  int k = 0, nsb = 0;
+  double recompute = 1.0;
+  size_t bytes = 0;
+};
+
+static ExactPlan plan_exact(const Setup &S, int ckpt_k, size_t held) {
   const int nt = S.a.nt;
   size_t freeb = 0, totb = 0;
   if (cudaMemGetInfo(&freeb, &totb) != cudaSuccess) {
     cudaGetLastError();
-    freeb = (size_t)32 << 30;
+    freeb = totb = (size_t)32 << 30;
   }
-  const double budget = 0.8 * (double)(freeb + held);
+  // budget: the caller's, or a quarter of the device; never more than 80% of
+  // what is free plus the workspace this call reuses
+  double budget = S.a.hbm_budget > 0 ? (double)S.a.hbm_budget : 0.25 * (double)totb;
+  budget = std::min(budget, 0.8 * (double)(freeb + held));
   const double fb = (double)S.fstride * 4;
   auto need = [&](int kk, int nb) {
     const int nck = (nt + kk - 1) / kk;
     return fb * nb * (5.0 + 2.0 * nck + kk) + fb * 2;
   };
+  auto recompute = [&](int kk) {
+    const int nck = (nt + kk - 1) / kk;
+    return 1.0 + (double)(nck - 1) * kk / nt;
+  };
   const int kmin = std::min(nt, std::max(1, (int)std::lround(std::sqrt(2.0 * nt))));
-  k = ckpt_k > 0 ? std::min(ckpt_k, nt) : kmin;
-  nsb = std::min(S.a.ns, MAXS);
-  while (nsb > 1 && need(k, nsb) > budget) nsb = (nsb + 1) / 2;
-  if (ckpt_k > 0) return;
-  if (need(nt, nsb) <= budget) {
-    k = nt;
-    return;
+  const int nsb_max = std::min(S.a.ns, MAXS);
+  ExactPlan best;
+  for (int nb = nsb_max; nb >= 1; nb = (nb + 1) / 2) {
+    int k;
+    if (ckpt_k > 0) {
+      k = std::min(ckpt_k, nt);
+      if (need(k, nb) > budget && nb > 1) {
+        if (nb <= 2) break;
+        continue;
+      }
+    } else if (need(nt, nb) <= budget) {
+      k = nt;
+    } else if (need(kmin, nb) <= budget) {
+      // need() rises with k above kmin: the largest k in [kmin, nt) that fits
+      int lo = kmin, hi = nt;
+      while (hi - lo > 1) {
+        const int mid = lo + (hi - lo) / 2;
+        if (need(mid, nb) <= budget) lo = mid;
+        else hi = mid;
+      }
+      k = lo;
+    } else {
+      k = 0;
+    }
+    if (k > 0) {
+      const double rc = recompute(k);
+      if (best.k == 0 || rc < best.recompute - 1e-12) {
+        best.k = k;
+        best.nsb = nb;
+        best.recompute = rc;
+        best.bytes = (size_t)need(k, nb);
+      }
+      if (ckpt_k > 0 || rc == 1.0) break;  // nothing better below
+    }
+    if (nb <= 2) break;
   }
-  // need() rises with k above kmin: the largest k in [kmin, nt) that fits
-  int lo = kmin, hi = nt;
-  while (hi - lo > 1) {
-    const int mid = lo + (hi - lo) / 2;
-    if (need(mid, nsb) <= budget) lo = mid;
-    else hi = mid;
+  if (best.k == 0) {
+    // nothing fits the budget: the smallest working set (one batch of two
+    // shots or one, k = sqrt(2 nt)); the allocation reports if even that fails
+    best.nsb = std::min(nsb_max, 2);
+    best.k = ckpt_k > 0 ? std::min(ckpt_k, nt) : kmin;
+    best.recompute = recompute(best.k);
+    best.bytes = (size_t)need(best.k, best.nsb);
   }
-  k = lo;
+  return best;
+}
+
+// Per-thread record of the last exact gradient's checkpoint plan.
+struct PlanRecord {
+  int k = 0, nsb = 0;
+  long long bytes = 0;
+  double recompute = 0.0;
+};
+static PlanRecord &plan_record() {
+  static thread_local PlanRecord r;
+  return r;
 }
 
 extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const float *wav,
@@ -1141,8 +1199,12 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   std::lock_guard<std::mutex> lock(ws.mutex());
   int k = 0, nsb = per_shot ? 1 : std::min(ns, MAXS);
   if (exact) {
-    plan_exact(S, ckpt_k, ws.capacity(), k, nsb);
-    if (per_shot) nsb = 1;
+    const ExactPlan ep = plan_exact(S, ckpt_k, ws.capacity());
+    k = ep.k;
+    nsb = per_shot ? 1 : ep.nsb;
+    plan_record().k = k;
+    plan_record().nsb = nsb;
+    plan_record().recompute = ep.recompute;
   }
   const int nck = exact ? (nt + k - 1) / k : 0;
   std::vector<float> wts;
@@ -1170,6 +1232,7 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   const size_t o_mis = cv.add(16);
   const size_t o_mx = cv.add(16);
   PW_TRY(ws.reserve(cv.total()));
+  if (exact) plan_record().bytes = (long long)cv.total();
   char *base = ws.base();
   // snapshots, checkpoints and segment terms are written before they are
   // read: zero the rest only (the term buffer alone is tens of GB)
@@ -1368,6 +1431,16 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   if (misfit) PW_CUDA(cudaMemcpyAsync(misfit, dmis, 8, cudaMemcpyDeviceToHost, st));
   PW_CUDA(cudaStreamSynchronize(st));
   timer.finish(launches, launches + 8);
+  return PW_OK;
+}
+
+extern "C" int pw_last_fwi_plan(int *ckpt_k, int *shots_per_batch, long long *bytes,
+                                double *recompute) {
+  const PlanRecord &r = plan_record();
+  if (ckpt_k) *ckpt_k = r.k;
+  if (shots_per_batch) *shots_per_batch = r.nsb;
+  if (bytes) *bytes = r.bytes;
+  if (recompute) *recompute = r.recompute;
   return PW_OK;
 }
 

@@ -7,7 +7,9 @@ scheme's own transpose (sponge and edge-replicated padding included) and
 images with the zero-lag condition fused into the adjoint step kernel:
     dJ/dv = pad2d^T( 2/v * sum_n phi_n * (Lap8 a_n + r w_n) ).
 Memory is capped by checkpoints of the forward state every k steps and a
-per-segment recompute (k from the planner when ``ckpt_k=0``).
+per-segment recompute; with ``ckpt_k=0`` the planner picks k and the shots
+per batch within an HBM budget (``hbm_budget`` bytes, default a quarter of
+the device), minimising the recomputed forward steps.
 
 Arrays follow pfwi: velocity (nz, nx), wavelet (nt,), data (nt, nr, ns).
 """
@@ -25,13 +27,16 @@ except ImportError:  # pragma: no cover
     torch = None
 
 
-def fwi_args(par, flags=0):
-    """pw_fwi_args from a pfwi ``par`` dictionary (after fillpar)."""
+def fwi_args(par, flags=0, hbm_budget=0):
+    """pw_fwi_args from a pfwi ``par`` dictionary (after fillpar);
+    ``hbm_budget`` bytes bound the exact gradient's working set (0: a quarter
+    of the device)."""
     from .pfwi import pararray, fillpar
     arr = pararray(fillpar(dict(par)))
     a = L.FwiArgs()
     L.check(L.lib().pw_fwi_args_from_pararray(L.ptr(arr), int(arr.size), a))
     a.flags = flags
+    a.hbm_budget = int(hbm_budget)
     return a
 
 
@@ -40,15 +45,18 @@ def _data_flat(dobs):
     return np.ascontiguousarray(np.asarray(dobs, np.float32).flatten(order="F"))
 
 
-def gradient(vel, wav, dobs, par, mode="exact", ckpt_k=0, per_shot=False, weight=None):
+def gradient(vel, wav, dobs, par, mode="exact", ckpt_k=0, per_shot=False, weight=None,
+             hbm_budget=0):
     """FWI gradient dJ/dv (nz, nx) and the FP64 misfit, host arrays in/out.
 
     mode "reference": gradient_av's imaging (wave_fwigradient.c:93-242) before
     its smoothing / scaling; misfit 0.5*sum((dobs-d)^2).
-    mode "exact": exact adjoint of the scheme; misfit 0.5*sum(w*(d-dobs)^2).
+    mode "exact": exact adjoint of the scheme; misfit 0.5*sum(w*(d-dobs)^2);
+    checkpoint interval ckpt_k, or planned within hbm_budget bytes when 0
+    (pywave_b200._lib.last_fwi_plan reports the plan).
     weight: (nr, nt) residual weights, default the reference's tapers."""
     flags = L.PW_HOST_PTRS | (L.PW_PER_SHOT if per_shot else 0)
-    a = fwi_args(par, flags)
+    a = fwi_args(par, flags, hbm_budget)
     v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F"))
     w = np.ascontiguousarray(np.asarray(wav, np.float32).reshape(-1))
     d = _data_flat(dobs)
@@ -81,8 +89,8 @@ if torch is not None:
         one pass and keeps dJ/dv for backward."""
 
         @staticmethod
-        def forward(ctx, vel, wav, dobs, par, ckpt_k=0, weight=None):
-            a = fwi_args(par, 0)
+        def forward(ctx, vel, wav, dobs, par, ckpt_k=0, weight=None, hbm_budget=0):
+            a = fwi_args(par, 0, hbm_budget)
             v = vel.detach().t().contiguous().float()          # [nx][nz]
             w = wav.detach().contiguous().float()
             d = dobs.detach().contiguous().float()              # [ns][nr][nt]
@@ -99,8 +107,9 @@ if torch is not None:
         @staticmethod
         def backward(ctx, gJ):
             (g,) = ctx.saved_tensors
-            return (g * gJ.to(g.dtype)), None, None, None, None, None
+            return (g * gJ.to(g.dtype)), None, None, None, None, None, None
 
-    def fwi_misfit(vel, wav, dobs, par, ckpt_k=0, weight=None):
-        """Differentiable misfit (see FwiMisfit)."""
-        return FwiMisfit.apply(vel, wav, dobs, par, ckpt_k, weight)
+    def fwi_misfit(vel, wav, dobs, par, ckpt_k=0, weight=None, hbm_budget=0):
+        """Differentiable misfit (see FwiMisfit); the checkpoints of the exact
+        adjoint fit hbm_budget bytes (0: a quarter of the device)."""
+        return FwiMisfit.apply(vel, wav, dobs, par, ckpt_k, weight, hbm_budget)

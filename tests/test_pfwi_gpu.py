@@ -123,6 +123,31 @@ def test_exact_gradient_independent_of_checkpoint_interval(golden, cuda_lib):
         assert np.array_equal(gk, ref), k
 
 
+def test_exact_gradient_independent_of_hbm_budget(golden, cuda_lib):
+    """The planner fits the checkpoints into the budget (a tighter budget: a
+    smaller interval and more recompute, or fewer shots per batch) and the
+    gradient stays bit-identical."""
+    from pywave_b200 import _lib as L
+    from pywave_b200 import fwi
+    g = golden("pfwi")
+    ref, Jr = fwi.gradient(g["vstart"], g["wav"], g["data"], _par(g), mode="exact", ckpt_k=1)
+    plans = []
+    for budget in (0, 40 << 20, 12 << 20, 6 << 20, 3 << 20):
+        gb, Jb = fwi.gradient(g["vstart"], g["wav"], g["data"], _par(g), mode="exact",
+                              hbm_budget=budget)
+        k, nsb, nbytes, rc = L.last_fwi_plan()
+        plans.append((budget, k, nsb, nbytes, rc))
+        print(f"budget {budget >> 20} MiB: k {k}, shots per batch {nsb}, held {nbytes / 2**20:.1f} "
+              f"MiB, recompute factor {rc:.3f}")
+        assert np.array_equal(gb, ref), budget
+        assert Jb == Jr
+    assert plans[0][1] == 400 and plans[0][4] == 1.0  # the default budget keeps every term
+    assert plans[-1][1] < plans[1][1] and plans[-1][4] > 1.0
+    for budget, k, nsb, nbytes, rc in plans[1:]:
+        # the checkpoints and segment buffer fit; the rest is data and traces
+        assert rc >= 1.0 and (nbytes < budget + (4 << 20))
+
+
 def test_autograd_function(golden, cuda_lib):
     import torch
     from pywave_b200 import fwi
