@@ -47,9 +47,13 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fwi2d", action="store_true",
                    help="tri3d: skip the secondary 2-D FWI gradients/s field")
-    p.add_argument("--workload", default="tri3d", choices=["tri3d", "fwi2d", "batch2d", "c1"],
+    p.add_argument("--workload", default="tri3d",
+                   choices=["tri3d", "fwi2d", "batch2d", "c1", "fwi3d"],
                    help="tri3d: the 3-D TRI image (default); fwi2d: 2-D FWI gradients/s; "
-                        "batch2d: uneven 2-D forward shots in one batch; c1: one 2-D shot")
+                        "batch2d: uneven 2-D forward shots in one batch; c1: one 2-D shot; "
+                        "fwi3d: 3-D FWI gradients/s")
+    p.add_argument("--fwi3d-nt", type=int, default=2500, help="fwi3d: time samples")
+    p.add_argument("--fwi3d-shots", type=int, default=16, help="fwi3d: shots per gradient")
     p.add_argument("--shots", type=int, default=32, help="fwi2d: shots per gradient")
     p.add_argument("--fwi-nt", type=int, default=2000, help="fwi2d: time samples")
     return p.parse_args()
@@ -960,6 +964,140 @@ def run_c1(args, world, rank, local):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------------------
+# fwi3d: 3-D FWI gradients/s, 400 x 400 x 200 at 12.5 m (km units)
+# --------------------------------------------------------------------------
+F3_NZ, F3_NX, F3_NY, F3_H, F3_DT, F3_NB, F3_COEF, F3_F0 = 200, 400, 400, 0.0125, 0.001, 20, 0.015, 12.0
+
+
+def fwi3d_models(seed):
+    """True model: a smooth gradient 1.8 -> 3.6 km/s over the depth with a
+    seeded 3% smooth perturbation and a salt-like body of 4.5 km/s (an
+    ellipsoid of seeded centre and radii); start model: the true model
+    Gaussian-smoothed with sigma 10 points.  (nz, nx, ny) float32."""
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    z = np.arange(F3_NZ, dtype=np.float32)[:, None, None] / (F3_NZ - 1)
+    v = 1.8 + 1.8 * z + np.zeros((F3_NZ, F3_NX, F3_NY), np.float32)
+    p = gaussian_filter(rng.standard_normal((F3_NZ // 4, F3_NX // 4, F3_NY // 4)), 2.0)
+    p = np.repeat(np.repeat(np.repeat(p / np.abs(p).max(), 4, 0), 4, 1), 4, 2)
+    v = v * (1.0 + 0.03 * p.astype(np.float32))
+    cz, cx, cy = rng.uniform(0.45, 0.65) * F3_NZ, rng.uniform(0.35, 0.65) * F3_NX, \
+        rng.uniform(0.35, 0.65) * F3_NY
+    rz, rx, ry = 0.12 * F3_NZ, rng.uniform(0.1, 0.2) * F3_NX, rng.uniform(0.1, 0.2) * F3_NY
+    iz, ix, iy = np.ogrid[:F3_NZ, :F3_NX, :F3_NY]
+    salt = ((iz - cz) / rz) ** 2 + ((ix - cx) / rx) ** 2 + ((iy - cy) / ry) ** 2 <= 1.0
+    v = np.where(salt, 4.5, v).astype(np.float32)
+    vs = gaussian_filter(v.astype(np.float64), 10.0).astype(np.float32)
+    return v, vs
+
+
+def fwi3d_geom(ns, nt):
+    """ns shots on a square grid at depth 5, 160 x 160 receivers spread over
+    the surface at depth 1, 12 Hz Ricker."""
+    side = int(round(np.sqrt(ns)))
+    sxs = [int((i + 0.5) * F3_NX / side) for i in range(side)]
+    sys_ = [int((j + 0.5) * F3_NY / side) for j in range(side)]
+    src = [(5, x, y) for y in sys_ for x in sxs][:ns]
+    rx = [int((i + 0.5) * F3_NX / 160) for i in range(160)]
+    ry = [int((j + 0.5) * F3_NY / 160) for j in range(160)]
+    return dict(nb=F3_NB, coef=F3_COEF, dz=F3_H, dx=F3_H, dy=F3_H, nt=nt, dt=F3_DT, src=src,
+                rz=1, rx=rx, ry=ry)
+
+
+def fwi3d_wavelet(nt):
+    t = np.arange(nt) * F3_DT - 1.2 / F3_F0
+    a = (np.pi * F3_F0 * t) ** 2
+    return (1e6 * (1 - 2 * a) * np.exp(-a)).astype(np.float32)
+
+
+def run_fwi3d(args, world, rank, local):
+    ns, nt = args.fwi3d_shots, args.fwi3d_nt
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference has no 3-D FWI (pywave's FWI is 2-D only)"}),
+                  flush=True)
+        return
+    import ctypes
+    import torch
+    from pywave_b200 import _lib as L
+    from pywave_b200 import build as B
+    from pywave_b200 import fwi3d
+    B.build()
+    torch.cuda.set_device(local)
+    st = torch.cuda.current_stream().cuda_stream
+    lib = L.lib()
+    vt, vs = fwi3d_models(21 + rank)
+    geom = fwi3d_geom(ns, nt)
+    wav = fwi3d_wavelet(nt)
+    a, keep = fwi3d.fwi3d_args(vt.shape, geom, 0, FWI_BUDGET)
+    dev = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).cuda()
+    vt_d = dev(vt.flatten(order="F"))
+    vs_d = dev(vs.flatten(order="F"))
+    wav_d = dev(wav)
+    nr = a.nrx * a.nry
+    dobs_d = torch.empty(ns * nr * nt, device="cuda")
+    L.check(lib.pw_pfwi3d_forward(a, vt_d.data_ptr(), wav_d.data_ptr(), dobs_d.data_ptr(), st))
+    g_d = torch.empty(vt.size, device="cuda")
+    J = ctypes.c_double(0.0)
+
+    def grad():
+        L.check(lib.pw_pfwi3d_gradient(a, vs_d.data_ptr(), wav_d.data_ptr(), dobs_d.data_ptr(),
+                                       None, g_d.data_ptr(), ctypes.byref(J), 0, st))
+        return L.last_timing()
+
+    for _ in range(args.warmup):
+        grad()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches, loops = 0, []
+    e0.record()
+    for _ in range(args.steps):
+        ms, nst, tot = grad()
+        loops.append(ms)
+        launches += tot
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    k, nsb, nbytes, rc = L.last_fwi_plan()
+    pad = (F3_NZ + 2 * F3_NB) * (F3_NX + 2 * F3_NB) * (F3_NY + 2 * F3_NB)
+    # algorithmic bytes per padded point-step-shot as in fwi2d (forward 20 B +
+    # exact adjoint 28 B), plus the recomputed forward steps (20 B each)
+    alg = (48.0 + 20.0 * (rc - 1.0)) * pad * nt * ns
+    peak, peak_kind = peaks()
+    loop_ms = statistics.median(loops)
+    achieved = alg / (loop_ms / 1e3) / 1e9
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"FWI gradients/s (3-D exact adjoint, {ns} shots)",
+            "value": job_rate(1, args.steps, world, ms), "unit": "gradients/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (FP64 misfit)",
+            "data": "synthetic (seeded gradient model with a 4.5 km/s salt body, start = smoothed)",
+            "config": {"workload": f"3-D FWI gradient {F3_NZ}x{F3_NX}x{F3_NY} h=12.5m nt={nt} "
+                                   f"dt=1ms shots={ns} receivers=160x160 nb={F3_NB} 12 Hz",
+                       "padded_cells": pad},
+            # forward (recomputed steps included) and adjoint point-updates
+            "point_updates_per_s": pad * nt * ns * (rc + 1.0) / (ms / args.steps / 1e3),
+            "checkpoint": {"budget_bytes": FWI_BUDGET, "interval_k": k, "shots_per_batch": nsb,
+                           "device_bytes": nbytes, "recompute_factor": rc},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "pf3_step_kernel FWD + ADJ_EXACT (whole gradient loop)",
+                         "alg_bytes_per_gradient": alg, "loop_ms": loop_ms,
+                         "peak_source": peak_kind},
+            "cpu_baseline": {"value": None, "unit": "gradients/s", "cores": 0,
+                             "kind": "unavailable",
+                             "sample": "the reference has no 3-D FWI"},
+            "clocks": clocks}), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -971,6 +1109,8 @@ def main():
         return run_batch2d(args, world, rank, local)
     if args.workload == "c1":
         return run_c1(args, world, rank, local)
+    if args.workload == "fwi3d":
+        return run_fwi3d(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, rank)
 

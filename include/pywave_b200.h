@@ -186,6 +186,42 @@ int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const flo
  * (wave_fwigradient.c:116). */
 int pw_last_fwi_plan(int *ckpt_k, int *shots_per_batch, long long *bytes, double *recompute);
 
+/* ------------------------------------------------------------ pfwi 3-D --- */
+
+/* The 3-D extension of pfwi's acoustic scheme (the reference has no 3-D FWI:
+ * its 2-D step, wave_fwimodeling.c:21-114 and wave_fwiutil.c:19-223, on
+ * three axes with an 8th-order Laplacian per axis, a sponge on all six faces
+ * and edge-replicated padding; oracle/pw_oracle3d_body.h states it in full). */
+typedef struct pw_fwi3d_args {
+  int nz, nx, ny;       /* interior model size */
+  float dz, dx, dy;
+  int nt;
+  float dt;
+  int nb;               /* sponge width on every face (>= 5) */
+  float coef;           /* sponge coefficient, bc[i] = expf(-(coef*(nb-i))^2) */
+  int ns;               /* shots */
+  const int *src;       /* host [ns][3]: source (z, x, y), interior indices; the
+                           spike is smoothed by the rect-2 triangle on each axis */
+  int nrx, nry;         /* receivers on the grid (rx[i], ry[j]), trace j*nrx + i */
+  const int *rx, *ry;   /* host, interior indices */
+  int rz;               /* receiver depth, interior index */
+  int flags;            /* PW_HOST_PTRS | PW_NO_CFL_CHECK */
+  long long hbm_budget; /* as pw_fwi_args.hbm_budget */
+} pw_fwi3d_args;
+
+/* 3-D forward modelling of all shots.  vel [ny][nx][nz], wav [nt],
+ * data [ns][nry*nrx][nt] (traces recorded before each step, as pfwi does). */
+int pw_pfwi3d_forward(const pw_fwi3d_args *a, const float *vel, const float *wav, float *data,
+                      void *stream);
+
+/* 3-D exact-adjoint FWI gradient of J = 0.5 sum w (d - dobs)^2 over all
+ * shots (J in FP64), checkpointed as pw_pfwi_gradient's EXACT mode under
+ * a->hbm_budget (pw_last_fwi_plan reports the plan).  No reference
+ * counterpart.  weight [nr][nt] or NULL (1); grad [ny][nx][nz] = dJ/dv. */
+int pw_pfwi3d_gradient(const pw_fwi3d_args *a, const float *vel, const float *wav,
+                       const float *dobs, const float *weight, float *grad, double *misfit,
+                       int ckpt_k, void *stream);
+
 /* gradient_av's tail (wave_fwigradient.c:244-255): triangle smoothing
  * rect x rect (wave_fwiutil.c:298-335) and the scale factor; *scaling <= 0 on
  * entry means "first call": it is set to 0.1/max|grad| as the reference's

@@ -30,7 +30,8 @@ _lib = None
 
 def build(force: bool = False) -> str:
     """Compile the oracle restatement (gcc, no FMA contraction)."""
-    srcs = [os.path.join(HERE, f) for f in ("pw_oracle.c", "pw_oracle_body.h")]
+    srcs = [os.path.join(HERE, f) for f in ("pw_oracle.c", "pw_oracle_body.h",
+                                             "pw_oracle3d_body.h")]
     stale = (not os.path.exists(LIB_PATH)) or any(
         os.path.getmtime(s) > os.path.getmtime(LIB_PATH) for s in srcs)
     if force or stale:
@@ -84,6 +85,18 @@ def lib():
             f = getattr(L, "or_pfwi_misfit_" + sfx)
             f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 2 + geo
                           + [rp, rp, rp, C.c_void_p])
+            f.restype = real
+            geo3 = [C.c_int] * 4 + [C.c_float] * 3 + [C.c_int, C.c_float, C.c_float, C.c_int,
+                                                        _i32p, C.c_int, C.c_int, C.c_int, _i32p,
+                                                        _i32p]
+            f = getattr(L, "or_pf3_forward_" + sfx)
+            f.argtypes = geo3 + [rp, rp, rp]
+            f.restype = None
+            f = getattr(L, "or_pf3_gradient_exact_" + sfx)
+            f.argtypes = geo3 + [rp, rp, rp, C.c_void_p, rp]
+            f.restype = real
+            f = getattr(L, "or_pf3_misfit_" + sfx)
+            f.argtypes = geo3 + [rp, rp, rp, C.c_void_p]
             f.restype = real
         _lib = L
     return _lib
@@ -307,4 +320,61 @@ def pfwi_misfit(vel, wav, dobs, nb, coef, dz, dx, dt, geo, ns, weight=None, prec
     wt = None if weight is None else np.ascontiguousarray(np.asarray(weight).astype(R))
     return float(getattr(lib(), "or_pfwi_misfit_" + precision)(
         nz, nx, nb, dz, dx, nt, dt, coef, *_geo_args(geo, ns), v, w, _dobs_flat(dobs, R),
+        None if wt is None else wt.ctypes.data))
+
+
+# --------------------------------------------------------------------------
+# 3-D extension of the pfwi scheme (pw_oracle3d_body.h; no reference 3-D FWI)
+# --------------------------------------------------------------------------
+
+def _geo3(vel, g):
+    nz, nx, ny = vel.shape
+    src = np.ascontiguousarray(np.asarray(g["src"], np.int32).reshape(-1))
+    rx = np.ascontiguousarray(np.asarray(g["rx"], np.int32))
+    ry = np.ascontiguousarray(np.asarray(g["ry"], np.int32))
+    return (nz, nx, ny, int(g["nb"]), float(g["dz"]), float(g["dx"]), float(g["dy"]),
+            int(g["nt"]), float(g["dt"]), float(g["coef"]), len(src) // 3, src, int(g["rz"]),
+            len(rx), len(ry), rx, ry)
+
+
+def _vel3(vel, R):
+    # (nz, nx, ny) -> [ny][nx][nz]
+    return np.ascontiguousarray(np.asarray(vel, np.float32).transpose(2, 1, 0).astype(R))
+
+
+def pf3_forward(vel, wav, g, precision="f32"):
+    """3-D forward modelling; vel (nz, nx, ny); g: dict nb, dz, dx, dy, nt, dt,
+    coef, src [(z, x, y)], rz, rx, ry.  Returns data [ns][nry*nrx][nt]."""
+    R = np.float32 if precision == "f32" else np.float64
+    geo = _geo3(vel, g)
+    ns, nr, nt = geo[10], geo[13] * geo[14], geo[7]
+    out = np.zeros(ns * nr * nt, R)
+    getattr(lib(), "or_pf3_forward_" + precision)(*geo, _vel3(vel, R),
+                                                 np.ascontiguousarray(np.asarray(wav).astype(R)),
+                                                 out)
+    return out.reshape(ns, nr, nt)
+
+
+def pf3_gradient_exact(vel, wav, dobs, g, weight=None, precision="f64"):
+    """Exact adjoint gradient dJ/dv (nz, nx, ny) and J (whole history in host
+    memory: small grids only)."""
+    R = np.float32 if precision == "f32" else np.float64
+    geo = _geo3(vel, g)
+    nz, nx, ny = vel.shape
+    grad = np.zeros(nz * nx * ny, R)
+    wt = None if weight is None else np.ascontiguousarray(np.asarray(weight).astype(R))
+    J = getattr(lib(), "or_pf3_gradient_exact_" + precision)(
+        *geo, _vel3(vel, R), np.ascontiguousarray(np.asarray(wav).astype(R)),
+        np.ascontiguousarray(np.asarray(dobs).astype(R).reshape(-1)),
+        None if wt is None else wt.ctypes.data, grad)
+    return grad.reshape(ny, nx, nz).transpose(2, 1, 0), float(J)
+
+
+def pf3_misfit(vel, wav, dobs, g, weight=None, precision="f64"):
+    R = np.float32 if precision == "f32" else np.float64
+    geo = _geo3(vel, g)
+    wt = None if weight is None else np.ascontiguousarray(np.asarray(weight).astype(R))
+    return float(getattr(lib(), "or_pf3_misfit_" + precision)(
+        *geo, _vel3(vel, R), np.ascontiguousarray(np.asarray(wav).astype(R)),
+        np.ascontiguousarray(np.asarray(dobs).astype(R).reshape(-1)),
         None if wt is None else wt.ctypes.data))

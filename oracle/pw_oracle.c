@@ -17,7 +17,9 @@
  *   triangle smoothing       pywave/src/wave_triangle.c:177-238 (np_smooth2)
  *   residual weighting       pywave/src/wave_fwiutil.c:225-296
  * plus the exact discrete adjoint of the pfwi forward step (FP64), derived
- * for this project and checked against finite differences in tests/.
+ * for this project and checked against finite differences in tests/, and
+ * the 3-D extension of the pfwi scheme with its exact adjoint
+ * (pw_oracle3d_body.h; the reference has no 3-D FWI).
  *
  * The body is instantiated twice (pw_oracle_body.h): REAL=float reproduces
  * the reference's float evaluation order operation by operation (no FMA
@@ -162,6 +164,7 @@ void or_residual_weights(int nt, int nr, int wtn1, int wtn2, int woffn1, int wof
 #define SFX(name) name##_f32
 #define PW_F32 1
 #include "pw_oracle_body.h"
+#include "pw_oracle3d_body.h"
 #undef REAL
 #undef SFX
 #undef PW_F32
@@ -170,6 +173,7 @@ void or_residual_weights(int nt, int nr, int wtn1, int wtn2, int woffn1, int wof
 #define SFX(name) name##_f64
 #define PW_F32 0
 #include "pw_oracle_body.h"
+#include "pw_oracle3d_body.h"
 #undef REAL
 #undef SFX
 #undef PW_F32

@@ -66,6 +66,15 @@ class FwiArgs(C.Structure):
                 ("hbm_budget", C.c_longlong)]
 
 
+class Fwi3dArgs(C.Structure):
+    _fields_ = [("nz", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("dz", C.c_float),
+                ("dx", C.c_float), ("dy", C.c_float), ("nt", C.c_int), ("dt", C.c_float),
+                ("nb", C.c_int), ("coef", C.c_float), ("ns", C.c_int),
+                ("src", C.POINTER(C.c_int)), ("nrx", C.c_int), ("nry", C.c_int),
+                ("rx", C.POINTER(C.c_int)), ("ry", C.POINTER(C.c_int)), ("rz", C.c_int),
+                ("flags", C.c_int), ("hbm_budget", C.c_longlong)]
+
+
 _lib = None
 _lock = threading.Lock()
 _vp = C.c_void_p
@@ -83,6 +92,9 @@ _SIGS = {
     "pw_gradient_postprocess": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int,
                                           _vp]),
     "pw_fwi": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp, C.POINTER(C.c_int), _vp]),
+    "pw_pfwi3d_forward": (C.c_int, [C.POINTER(Fwi3dArgs), _vp, _vp, _vp, _vp]),
+    "pw_pfwi3d_gradient": (C.c_int, [C.POINTER(Fwi3dArgs), _vp, _vp, _vp, _vp, _vp, _vp,
+                                     C.c_int, _vp]),
     "pw_last_fwi_plan": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int),
                                    C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
     "pw_last_error": (C.c_char_p, []),

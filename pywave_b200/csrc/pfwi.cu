@@ -413,7 +413,8 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
 // FP64 misfit and residual, one thread per (shot, it, ir):
 //   REFERENCE: r = dobs - d, J += 0.5 r^2 (unweighted), adjoint source r*w
 //   EXACT:     r = d - dobs, J += 0.5 w r^2, adjoint source w*r
-// d, dobs, res: [shot][nt][nr]; w: [nr][nt] (residual_weighting layout).
+// d, dobs, res: [shot][nt][nr]; w: [nr][nt] (residual_weighting layout) or
+// null (every weight 1).
 __global__ void residual_kernel(const float *d, const float *dobs, const float *w, float *res,
                                 int ns, int nt, int nr, int exact, double *misfit) {
   const long long n = (long long)ns * nt * nr;
@@ -422,7 +423,7 @@ __global__ void residual_kernel(const float *d, const float *dobs, const float *
        i += (long long)gridDim.x * blockDim.x) {
     const int ir = int(i % nr);
     const int it = int((i / nr) % nt);
-    const float wt = w[(size_t)ir * nt + it];
+    const float wt = w ? w[(size_t)ir * nt + it] : 1.f;
     if (exact) {
       const float r = fsub(d[i], dobs[i]);
       acc += 0.5 * (double)wt * (double)r * (double)r;
@@ -1477,5 +1478,752 @@ extern "C" int pw_gradient_postprocess(int nz, int nx, int rect, int waterz, flo
   if (host) PW_TRY(to_host(grad, g, n * 4, true, st));
   PW_CUDA(cudaMemcpyAsync(scaling, sc, 4, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
   PW_CUDA(cudaStreamSynchronize(st));
+  return PW_OK;
+}
+
+// =========================================================================
+// 3-D extension of the pfwi scheme (config: 400 x 400 x 200 batched FWI
+// gradient).  The reference has no 3-D FWI; the scheme restates its 2-D
+// acoustic step (wave_fwimodeling.c:21-114, wave_fwiutil.c:19-223) on three
+// axes, exactly as the FP64 / FP32 oracle of oracle/pw_oracle3d_body.h does:
+//   term = ((Tx / dx^2 + Tz / dz^2) + Ty / dy^2) + r w_n   (each T the
+//          8th-order sum, zero outside [4, pad-4) on every axis; the
+//          divisions as products with 1/h^2 rounded to float),
+//   next = S(2 a - S b + V term),  S = Sy(Sx(Sz u)),  V = (v v) dt^2.
+// Field layout: z contiguous with a 4-cell halo in front, 4 halo columns and
+// 4 halo planes on each side:  off(iz, ix, iy) = (iz + 4) + sx (ix + 4) +
+// sy (iy + 4), sx = lz (a multiple of 32 floats), sy = lz (pnx + 8).
+// =========================================================================
+namespace pw {
+namespace pf3 {
+
+using pf::FWD;
+using pf::ADJ_EXACT;
+constexpr int MAXS3 = 16;    // shots per launch
+constexpr int MAXSRC = 64;   // source-map cells per shot
+constexpr int XT = 16;       // columns per CTA
+constexpr int NR = 3;        // ring planes (plane y, y + 1, y + 2 in flight)
+
+struct Shot {
+  int nsrc;
+  int sz0, sz1, sx0, sx1, sy0, sy1;  // bounding box of the source cells
+  int scell[MAXSRC];                 // iz | ix << 11 | iy << 22
+  float sw[MAXSRC];
+};
+
+struct Args {
+  int pnz, pnx, pny, lz;
+  long long sx, sy, fstride;
+  int nz4, ZT, nzc, ych;
+  float c0, c1, c2, c3, c4, rdx2, rdz2, rdy2;
+  int nshots;
+  const float *cur[MAXS3];
+  float *nxt[MAXS3];
+  const float *V;
+  const float *bz, *bx, *by;
+  int it, nt;
+  const Shot *shots;
+  int rz, nrx, nr;
+  const int *rxmap, *rymap;  // receiver index along x / y, or -1
+  const float *wav;
+  float *rec;                // FWD: traces [shot][nt][nr] or null
+  float *tout;               // FWD: term of this step [shot] (field layout) or null
+  long long tout_stride;
+  const float *res;          // ADJ: residual [shot][nt][nr]
+  const float *tin;          // ADJ: forward term of this step [shot]
+  long long tin_stride;
+  float *grad;               // ADJ: phi * term accumulators (field layout) [shot]
+  long long gstride;
+};
+
+__host__ __device__ inline long long off3(const Args &a, int iz, int ix, int iy) {
+  return (long long)(iz + 4) + a.sx * (ix + 4) + a.sy * (iy + 4);
+}
+
+// One step over the CTA's ZT float4 x XT column tile, marching y: the tile of
+// plane y (with a 1-float4 z halo and 4 halo columns each side) is staged in
+// a 3-plane cp.async ring with one CTA barrier per plane; the y neighbours
+// come from a 9-deep register queue of the thread's own float4.
+template <int MODE>
+__global__ void __launch_bounds__(512) pf3_step_kernel(const __grid_constant__ Args a) {
+  extern __shared__ float4 sm3[];
+  constexpr int NST = MODE == FWD ? 2 : 4;  // own streams: prev, V (, term, gradient)
+  const int ZT = a.ZT, TZ = ZT + 2, TX = XT + 8;
+  const int nthr = ZT * XT;
+  const int tid = threadIdx.x, zt = tid % ZT, xt = tid / ZT;
+  const int s = blockIdx.z;
+  const int zc = blockIdx.x % a.nzc, xc = blockIdx.x / a.nzc;
+  const int z4 = zc * ZT + zt, x = xc * XT + xt;
+  const int y0 = blockIdx.y * a.ych, y1 = min(a.pny, y0 + a.ych);
+  const bool live = z4 < a.nz4 && x < a.pnx;
+  const int iz0 = 4 * z4;
+  const int tile_n = TZ * TX, slot_n = tile_n + NST * nthr;
+  const float *cur = a.cur[s];
+  float *nxt = a.nxt[s];
+  const float *tin = MODE == ADJ_EXACT ? a.tin + s * a.tin_stride : nullptr;
+  float *gs = MODE == ADJ_EXACT ? a.grad + s * a.gstride : nullptr;
+  const long long sy = a.sy;
+  // own float4 in plane 0 (a safe in-range cell for idle threads)
+  const long long o0 = live ? off3(a, iz0, x, 0) : off3(a, 0, 0, 0);
+  // tile copies: element e = tid + k nthr of the TZ x TX tile, tz fastest
+  constexpr int MAXCP = 4;  // TZ * TX <= 4 * nthr for ZT >= 4
+  long long cpo[MAXCP];
+  bool cok[MAXCP];
+#pragma unroll
+  for (int k = 0; k < MAXCP; k++) {
+    const int e = tid + k * nthr;
+    const int tz = e % TZ, tx = e / TZ;
+    const int zz = zc * ZT - 1 + tz, col = xc * XT - 4 + tx;
+    // the float4 at 4 zz + 4 must lie in the column, the column in the halo
+    cok[k] = e < tile_n && zz >= -1 && 4 * zz + 8 <= a.lz && col >= -4 && col < a.pnx + 4;
+    cpo[k] = cok[k] ? (long long)(4 * zz + 4) + a.sx * (col + 4) + sy * 4 : 0;
+  }
+  auto issue = [&](int p, int rs) {  // plane p into ring slot rs
+    if (p < y1) {
+      float4 *dst = sm3 + rs * slot_n;
+      const long long py = sy * p;
+#pragma unroll
+      for (int k = 0; k < MAXCP; k++) {
+        const int e = tid + k * nthr;
+        if (e < tile_n) pf::cp16(dst + e, cur + (cok[k] ? cpo[k] + py : 0), cok[k]);
+      }
+      float4 *own = dst + tile_n + tid;
+      pf::cp16(own, nxt + o0 + py, live);
+      pf::cp16(own + nthr, a.V + o0 + py, live);
+      if (MODE == ADJ_EXACT) {
+        pf::cp16(own + 2 * nthr, tin + o0 + py, live);
+        pf::cp16(own + 3 * nthr, gs + o0 + py, live);
+      }
+    }
+    pf::cp_commit();
+  };
+
+  float bzf[4];
+  bool lz_ok[4], zin[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int iz = iz0 + e;
+    bzf[e] = (live && iz < a.pnz) ? a.bz[iz] : 1.f;
+    lz_ok[e] = iz >= 4 && iz < a.pnz - 4;
+    zin[e] = iz < a.pnz;
+  }
+  const float bxf = live ? a.bx[x] : 1.f;
+  const bool lx_ok = x >= 4 && x < a.pnx - 4;
+  const bool rec_row = live && a.rz >= iz0 && a.rz < iz0 + 4;
+  const int rx_i = rec_row ? a.rxmap[x] : -1;
+  const Shot &sh = a.shots[s];
+  const bool src_zx = MODE == FWD && live && iz0 <= sh.sz1 && iz0 + 3 >= sh.sz0 && x >= sh.sx0 &&
+                      x <= sh.sx1;
+  const int ci = (xt + 4) * TZ + zt + 1;  // own float4 in the tile
+
+  // y queue: q[k] = own float4 of plane y - 4 + k
+  float4 q[9];
+  const float *pc = cur + o0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) q[k] = __ldg(reinterpret_cast<const float4 *>(pc + sy * (y0 - 4 + k)));
+  float4 qn = __ldg(reinterpret_cast<const float4 *>(pc + sy * (y0 + 4)));
+  issue(y0, 0);
+  issue(y0 + 1, 1);
+  int rs = 0;  // ring slot of plane y
+  for (int y = y0; y < y1; y++) {
+    pf::cp_wait<1>();
+    __syncthreads();  // plane y staged; every thread is done with plane y - 1
+    issue(y + 2, rs == 0 ? 2 : rs - 1);  // into the slot plane y - 1 left
+    q[8] = qn;
+    if (y + 1 < y1) qn = __ldg(reinterpret_cast<const float4 *>(pc + sy * (y + 5)));
+    const float4 *tile = sm3 + rs * slot_n;
+    const float4 *own = tile + tile_n + tid;
+    if (live) {
+      const float4 c = q[4];
+      const float4 L = tile[ci - 1], R = tile[ci + 1];
+      const float4 xm1 = tile[ci - TZ], xp1 = tile[ci + TZ];
+      const float4 xm2 = tile[ci - 2 * TZ], xp2 = tile[ci + 2 * TZ];
+      const float4 xm3 = tile[ci - 3 * TZ], xp3 = tile[ci + 3 * TZ];
+      const float4 xm4 = tile[ci - 4 * TZ], xp4 = tile[ci + 4 * TZ];
+      const float4 pv = own[0], V4 = own[nthr];
+      const float byf = a.by[y];
+      const bool ly_ok = y >= 4 && y < a.pny - 4;
+      const long long o = o0 + sy * y;
+      int trace = -1;
+      if (rec_row && rx_i >= 0) {
+        const int ry_j = a.rymap[y];
+        if (ry_j >= 0) trace = ry_j * a.nrx + rx_i;
+      }
+      if (MODE == FWD && trace >= 0 && a.rec)
+        a.rec[((size_t)s * a.nt + a.it) * a.nr + trace] = pf::el(c, a.rz - iz0);
+      const bool src_here = src_zx && y >= sh.sy0 && y <= sh.sy1;
+      float4 term4, res4;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const float cv = pf::el(c, e);
+        float tx = fmul(a.c0, cv);
+        tx = fadd(tx, fmul(a.c1, fadd(pf::el(xp1, e), pf::el(xm1, e))));
+        tx = fadd(tx, fmul(a.c2, fadd(pf::el(xp2, e), pf::el(xm2, e))));
+        tx = fadd(tx, fmul(a.c3, fadd(pf::el(xp3, e), pf::el(xm3, e))));
+        tx = fadd(tx, fmul(a.c4, fadd(pf::el(xp4, e), pf::el(xm4, e))));
+        float tz = fmul(a.c0, cv);
+        tz = fadd(tz, fmul(a.c1, fadd(pf::znb(L, c, R, e, 1), pf::znb(L, c, R, e, -1))));
+        tz = fadd(tz, fmul(a.c2, fadd(pf::znb(L, c, R, e, 2), pf::znb(L, c, R, e, -2))));
+        tz = fadd(tz, fmul(a.c3, fadd(pf::znb(L, c, R, e, 3), pf::znb(L, c, R, e, -3))));
+        tz = fadd(tz, fmul(a.c4, fadd(pf::znb(L, c, R, e, 4), pf::znb(L, c, R, e, -4))));
+        float ty = fmul(a.c0, cv);
+        ty = fadd(ty, fmul(a.c1, fadd(pf::el(q[5], e), pf::el(q[3], e))));
+        ty = fadd(ty, fmul(a.c2, fadd(pf::el(q[6], e), pf::el(q[2], e))));
+        ty = fadd(ty, fmul(a.c3, fadd(pf::el(q[7], e), pf::el(q[1], e))));
+        ty = fadd(ty, fmul(a.c4, fadd(pf::el(q[8], e), pf::el(q[0], e))));
+        float t = (lz_ok[e] && lx_ok && ly_ok)
+                      ? fadd(fadd(fmul(tx, a.rdx2), fmul(tz, a.rdz2)), fmul(ty, a.rdy2))
+                      : 0.f;
+        const int iz = iz0 + e;
+        if (MODE == FWD) {
+          if (src_here) {
+            const int key = iz | (x << 11) | (y << 22);
+            for (int k = 0; k < sh.nsrc; k++)
+              if (sh.scell[k] == key) t = fadd(t, fmul(sh.sw[k], a.wav[a.it]));
+          }
+        } else if (trace >= 0 && iz == a.rz) {
+          t = fadd(t, a.res[((size_t)s * a.nt + a.it) * a.nr + trace]);
+        }
+        pf::set_el(term4, e, t);
+        const float p = fmul(byf, fmul(bxf, fmul(bzf[e], pf::el(pv, e))));
+        float v = fadd(fsub(fmul(2.f, cv), p), fmul(pf::el(V4, e), t));
+        v = fmul(byf, fmul(bxf, fmul(bzf[e], v)));
+        pf::set_el(res4, e, zin[e] ? v : 0.f);
+      }
+      *reinterpret_cast<float4 *>(nxt + o) = res4;
+      if (MODE == FWD && a.tout)
+        *reinterpret_cast<float4 *>(a.tout + s * a.tout_stride + o) = term4;
+      if (MODE == ADJ_EXACT) {
+        const float4 tf = own[2 * nthr];
+        float4 g = own[3 * nthr];
+        g.x = fadd(g.x, fmul(c.x, tf.x));
+        g.y = fadd(g.y, fmul(c.y, tf.y));
+        g.z = fadd(g.z, fmul(c.z, tf.z));
+        g.w = fadd(g.w, fmul(c.w, tf.w));
+        *reinterpret_cast<float4 *>(gs + o) = g;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) q[k] = q[k + 1];
+    rs = rs == 2 ? 0 : rs + 1;
+  }
+  pf::cp_wait_all();
+}
+
+// V = (v v) dt^2 on the padded grid (edge replication on every face)
+__global__ void pad_V3_kernel(const float *vel, int nz, int nx, int ny, int nb, Args g, float dt2,
+                              float *V) {
+  const long long n = (long long)g.pnz * g.pnx * g.pny;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int iz = int(i % g.pnz), ix = int((i / g.pnz) % g.pnx), iy = int(i / ((long long)g.pnz * g.pnx));
+    const int jz = min(max(iz - nb, 0), nz - 1), jx = min(max(ix - nb, 0), nx - 1);
+    const int jy = min(max(iy - nb, 0), ny - 1);
+    const float v = vel[((size_t)jy * nx + jx) * nz + jz];
+    V[off3(g, iz, ix, iy)] = fmul(fmul(v, v), dt2);
+  }
+}
+
+// dJ/dv = 2 / v * sum of the accumulators of the padded cells that pad3d
+// copies from the interior cell (edge replication adjoint)
+__global__ void fold_grad3_kernel(const float *gacc, const float *vel, int nz, int nx, int ny,
+                                  int nb, Args g, float *grad) {
+  const long long n = (long long)nz * nx * ny;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int jz = int(i % nz), jx = int((i / nz) % nx), jy = int(i / ((long long)nz * nx));
+    const int z_lo = jz == 0 ? 0 : jz + nb, z_hi = jz == nz - 1 ? g.pnz - 1 : jz + nb;
+    const int x_lo = jx == 0 ? 0 : jx + nb, x_hi = jx == nx - 1 ? g.pnx - 1 : jx + nb;
+    const int y_lo = jy == 0 ? 0 : jy + nb, y_hi = jy == ny - 1 ? g.pny - 1 : jy + nb;
+    double s = 0.0;
+    for (int iy = y_lo; iy <= y_hi; iy++)
+      for (int ix = x_lo; ix <= x_hi; ix++)
+        for (int iz = z_lo; iz <= z_hi; iz++) s += (double)gacc[off3(g, iz, ix, iy)];
+    grad[i] = (float)(2.0 * s / (double)vel[i]);
+  }
+}
+
+struct Setup3 {
+  pw_fwi3d_args a;
+  Args g;  // geometry part of the step arguments
+  std::vector<float> bz, bx, by;
+  std::vector<Shot> shots;
+  std::vector<int> rxmap, rymap;
+  int nr;
+};
+
+// Source map of one shot: the spike at padded (sz, sx, sy) smoothed by the
+// rect-2 triangle along z and x (pf::source_map) and along y.
+static int source_map3(int sz, int sx, int sy, const Setup3 &S, Shot &sh) {
+  pf::ShotGeo g2;
+  PW_TRY(pf::source_map(sx, sz, S.g.pnz, S.g.pnx, g2));
+  const int pny = S.g.pny, r = 6;
+  const int y_lo = std::max(0, sy - r), y_hi = std::min(pny - 1, sy + r);
+  const bool full = y_lo == 0 || y_hi == pny - 1;
+  const int ys = full ? 0 : y_lo, nyw = full ? pny : y_hi - y_lo + 1;
+  std::vector<float> fy(nyw, 0.f), tmp;
+  fy[sy - ys] = 1.f;
+  pf::smooth_line_host(2, nyw, fy.data(), 0, 1, tmp);
+  sh.nsrc = 0;
+  sh.sz0 = sh.sx0 = sh.sy0 = 1 << 30;
+  sh.sz1 = sh.sx1 = sh.sy1 = -1;
+  for (int j = 0; j < nyw; j++) {
+    if (fy[j] == 0.f) continue;
+    const int gy = j + ys;
+    PW_CHECK(gy >= 4 && gy < pny - 4, PW_ERR_SHAPE,
+             "source map reaches the zero border of the padded grid");
+    for (int k = 0; k < g2.nsrc; k++) {
+      PW_CHECK(sh.nsrc < MAXSRC, PW_ERR_SHAPE, "source map has too many cells");
+      const int gx = g2.scell[k] >> 16, gz = g2.scell[k] & 0xffff;
+      sh.scell[sh.nsrc] = gz | (gx << 11) | (gy << 22);
+      sh.sw[sh.nsrc] = g2.sw[k] * fy[j];
+      sh.nsrc++;
+      sh.sz0 = std::min(sh.sz0, gz); sh.sz1 = std::max(sh.sz1, gz);
+      sh.sx0 = std::min(sh.sx0, gx); sh.sx1 = std::max(sh.sx1, gx);
+      sh.sy0 = std::min(sh.sy0, gy); sh.sy1 = std::max(sh.sy1, gy);
+    }
+  }
+  return PW_OK;
+}
+
+static int setup3(const pw_fwi3d_args *a, Setup3 &S) {
+  PW_CHECK(a != nullptr, PW_ERR_VALUE, "null args");
+  S.a = *a;
+  PW_CHECK(a->nz >= 1 && a->nx >= 1 && a->ny >= 1 && a->nt >= 1 && a->ns >= 1 && a->nb >= 5,
+           PW_ERR_SHAPE, "sizes must be positive and nb >= 5 (nz=%d nx=%d ny=%d nt=%d ns=%d nb=%d)",
+           a->nz, a->nx, a->ny, a->nt, a->ns, a->nb);
+  PW_CHECK(a->dx > 0 && a->dy > 0 && a->dz > 0 && a->dt > 0, PW_ERR_VALUE,
+           "spacings must be positive");
+  PW_CHECK(a->src && a->rx && a->ry && a->nrx >= 1 && a->nry >= 1, PW_ERR_VALUE,
+           "sources and receivers are required");
+  Args &g = S.g;
+  memset(&g, 0, sizeof g);
+  const int nb = a->nb;
+  g.pnz = a->nz + 2 * nb;
+  g.pnx = a->nx + 2 * nb;
+  g.pny = a->ny + 2 * nb;
+  PW_CHECK(g.pnz < 2048 && g.pnx < 2048 && g.pny < 512, PW_ERR_SHAPE,
+           "padded grid beyond 2047 x 2047 x 511");
+  g.lz = (int)round_up(4 + round_up(g.pnz, 4) + 4, 32);
+  g.sx = g.lz;
+  g.sy = (long long)g.lz * (g.pnx + 8);
+  g.fstride = g.sy * (g.pny + 8) + 64;
+  g.nz4 = ceil_div(g.pnz, 4);
+  const int nzc = ceil_div(g.nz4, 32);
+  g.ZT = std::max(4, ceil_div(g.nz4, nzc));
+  g.nzc = ceil_div(g.nz4, g.ZT);
+  const float c0 = -205. / 72, c1 = 8. / 5, c2 = -1. / 5, c3 = 8. / 315, c4 = -1. / 560;
+  g.c0 = c0; g.c1 = c1; g.c2 = c2; g.c3 = c3; g.c4 = c4;
+  g.rdz2 = 1.f / (a->dz * a->dz);
+  g.rdx2 = 1.f / (a->dx * a->dx);
+  g.rdy2 = 1.f / (a->dy * a->dy);
+  g.nt = a->nt;
+  std::vector<float> bc(nb);
+  for (int i = 0; i < nb; i++) {
+    const float tmp = a->coef * (nb - i);
+    bc[i] = expf(-tmp * tmp);
+  }
+  auto axis = [&](int n, std::vector<float> &f) {
+    f.assign(n, 1.f);
+    for (int i = 0; i < nb; i++) f[i] = bc[i];
+    for (int i = n - nb; i < n; i++) f[i] = bc[n - i - 1];
+  };
+  axis(g.pnz, S.bz);
+  axis(g.pnx, S.bx);
+  axis(g.pny, S.by);
+  // receivers: the nrx x nry grid (rx[i], ry[j]) at depth rz, trace j nrx + i
+  PW_CHECK(a->rz >= 0 && a->rz < a->nz, PW_ERR_SHAPE, "receiver depth outside the model");
+  g.rz = a->rz + nb;
+  g.nrx = a->nrx;
+  S.nr = a->nrx * a->nry;
+  g.nr = S.nr;
+  S.rxmap.assign(g.pnx, -1);
+  S.rymap.assign(g.pny, -1);
+  for (int i = 0; i < a->nrx; i++) {
+    PW_CHECK(a->rx[i] >= 0 && a->rx[i] < a->nx, PW_ERR_SHAPE, "receiver x index %d outside", i);
+    PW_CHECK(S.rxmap[a->rx[i] + nb] < 0, PW_ERR_SHAPE, "receiver x index %d repeated", i);
+    S.rxmap[a->rx[i] + nb] = i;
+  }
+  for (int j = 0; j < a->nry; j++) {
+    PW_CHECK(a->ry[j] >= 0 && a->ry[j] < a->ny, PW_ERR_SHAPE, "receiver y index %d outside", j);
+    PW_CHECK(S.rymap[a->ry[j] + nb] < 0, PW_ERR_SHAPE, "receiver y index %d repeated", j);
+    S.rymap[a->ry[j] + nb] = j;
+  }
+  S.shots.assign(a->ns, Shot{});
+  for (int is = 0; is < a->ns; is++) {
+    const int z = a->src[3 * is], x = a->src[3 * is + 1], y = a->src[3 * is + 2];
+    PW_CHECK(z >= 0 && z < a->nz && x >= 0 && x < a->nx && y >= 0 && y < a->ny, PW_ERR_SHAPE,
+             "shot %d: source (z=%d, x=%d, y=%d) outside the model", is, z, x, y);
+    PW_TRY(source_map3(z + nb, x + nb, y + nb, S, S.shots[is]));
+  }
+  return PW_OK;
+}
+
+static size_t smem3(const Args &g, int mode) {
+  const int nthr = g.ZT * XT;
+  const int slot = (g.ZT + 2) * (XT + 8) + (mode == FWD ? 2 : 4) * nthr;
+  return (size_t)NR * slot * sizeof(float4);
+}
+
+template <int MODE>
+static int launch3_t(const Args &p, cudaStream_t st) {
+  const size_t smem = smem3(p, MODE);
+  static bool attr = false;
+  if (!attr) {
+    int dev = 0, maxsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncSetAttribute(pf3_step_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+    cudaGetLastError();
+    attr = true;
+  }
+  const dim3 grid((unsigned)(p.nzc * ceil_div(p.pnx, XT)), (unsigned)ceil_div(p.pny, p.ych),
+                  (unsigned)p.nshots);
+  pf3_step_kernel<MODE><<<grid, p.ZT * XT, smem, st>>>(p);
+  PW_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+static int launch3(const Args &p, int mode, cudaStream_t st) {
+  return mode == FWD ? launch3_t<FWD>(p, st) : launch3_t<ADJ_EXACT>(p, st);
+}
+
+// planes per CTA: enough CTAs for every SM a few times over
+static int plan_ych(const Args &g, int nshots) {
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long cols = (long long)g.nzc * ceil_div(g.pnx, XT) * nshots;
+  int ych = g.pny;
+  while (ych > 16 && cols * ceil_div(g.pny, ych) < 8LL * nsm) ych = (ych + 1) / 2;
+  return ych;
+}
+
+}  // namespace pf3
+}  // namespace pw
+
+using namespace pw::pf3;
+
+// common device state of a 3-D call
+namespace pw {
+namespace pf3 {
+struct Bound3 {
+  size_t o_V, o_A, o_B, o_bz, o_bx, o_by, o_shots, o_rxm, o_rym, o_wav;
+};
+static void carve3(const Setup3 &S, int nsb, Carve &cv, Bound3 &b) {
+  const size_t fb = (size_t)S.g.fstride * 4;
+  b.o_V = cv.add(fb);
+  b.o_A = cv.add((size_t)nsb * fb);
+  b.o_B = cv.add((size_t)nsb * fb);
+  b.o_bz = cv.add(S.bz.size() * 4);
+  b.o_bx = cv.add(S.bx.size() * 4);
+  b.o_by = cv.add(S.by.size() * 4);
+  b.o_shots = cv.add(sizeof(Shot) * S.shots.size());
+  b.o_rxm = cv.add(S.rxmap.size() * 4);
+  b.o_rym = cv.add(S.rymap.size() * 4);
+  b.o_wav = cv.add((size_t)S.a.nt * 4);
+}
+static int upload3(const Setup3 &S, char *base, const Bound3 &b, const float *wav, bool host,
+                   cudaStream_t st) {
+  PW_CUDA(cudaMemcpyAsync(base + b.o_bz, S.bz.data(), S.bz.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + b.o_bx, S.bx.data(), S.bx.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + b.o_by, S.by.data(), S.by.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + b.o_shots, S.shots.data(), sizeof(Shot) * S.shots.size(),
+                          cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + b.o_rxm, S.rxmap.data(), S.rxmap.size() * 4,
+                          cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + b.o_rym, S.rymap.data(), S.rymap.size() * 4,
+                          cudaMemcpyHostToDevice, st));
+  PW_TRY(to_device(base + b.o_wav, wav, (size_t)S.a.nt * 4, host, st));
+  return PW_OK;
+}
+static void bind3(const Setup3 &S, char *base, const Bound3 &b, Args &p) {
+  p = S.g;
+  p.V = at<float>(base, b.o_V);
+  p.bz = at<float>(base, b.o_bz);
+  p.bx = at<float>(base, b.o_bx);
+  p.by = at<float>(base, b.o_by);
+  p.shots = at<Shot>(base, b.o_shots);
+  p.rxmap = at<int>(base, b.o_rxm);
+  p.rymap = at<int>(base, b.o_rym);
+  p.wav = at<float>(base, b.o_wav);
+}
+static int prep_vel3(const Setup3 &S, const float *vel, bool host, char *base, size_t o_vel,
+                     size_t o_mx, const Bound3 &b, const float **d_vel, cudaStream_t st) {
+  const size_t nvel = (size_t)S.a.nz * S.a.nx * S.a.ny;
+  *d_vel = vel;
+  if (host) {
+    PW_TRY(to_device(base + o_vel, vel, nvel * 4, true, st));
+    *d_vel = at<float>(base, o_vel);
+  }
+  unsigned *mx = at<unsigned>(base, o_mx);
+  PW_CUDA(cudaMemsetAsync(mx, 0, 8, st));
+  pf::vel_check_kernel<<<296, 256, 0, st>>>(*d_vel, (long long)nvel, mx);
+  PW_CUDA(cudaGetLastError());
+  unsigned hv[2] = {0, 0};
+  PW_CUDA(cudaMemcpyAsync(hv, mx, 8, cudaMemcpyDeviceToHost, st));
+  PW_CUDA(cudaStreamSynchronize(st));
+  float vmax;
+  memcpy(&vmax, &hv[0], 4);
+  PW_CHECK(hv[1] == 0 && vmax > 0.f, PW_ERR_VALUE, "velocity has non-finite or non-positive values");
+  if (!(S.a.flags & PW_NO_CFL_CHECK)) {
+    // 8th-order leapfrog in 3-D: v dt / h <= 0.453 (measured limit)
+    const float h = std::min(S.a.dx, std::min(S.a.dy, S.a.dz));
+    const float cfl = vmax * S.a.dt / h;
+    PW_CHECK(cfl <= 0.453f, PW_ERR_CFL, "unstable: vmax*dt/h = %g exceeds 0.453", cfl);
+  }
+  pad_V3_kernel<<<1184, 256, 0, st>>>(*d_vel, S.a.nz, S.a.nx, S.a.ny, S.a.nb, S.g,
+                                      S.a.dt * S.a.dt, at<float>(base, b.o_V));
+  PW_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+}  // namespace pf3
+}  // namespace pw
+
+extern "C" int pw_pfwi3d_forward(const pw_fwi3d_args *a, const float *vel, const float *wav,
+                                 float *data, void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  Setup3 S;
+  PW_TRY(setup3(a, S));
+  const bool host = (a->flags & PW_HOST_PTRS) != 0;
+  const int ns = a->ns, nt = a->nt, nr = S.nr;
+  const int nsb = std::min(ns, MAXS3);
+  const size_t nvel = (size_t)a->nz * a->nx * a->ny;
+  const size_t fs = (size_t)S.g.fstride;
+  Carve cv;
+  Bound3 b;
+  carve3(S, nsb, cv, b);
+  const size_t o_vel = cv.add(host ? nvel * 4 : 0);
+  const size_t o_rec = cv.add((size_t)ns * nt * nr * 4);
+  const size_t o_out = cv.add(host ? (size_t)ns * nt * nr * 4 : 0);
+  const size_t o_mx = cv.add(16);
+  Workspace &ws = Workspace::for_current_device();
+  std::lock_guard<std::mutex> lock(ws.mutex());
+  PW_TRY(ws.reserve(cv.total()));
+  char *base = ws.base();
+  PW_CUDA(cudaMemsetAsync(base, 0, cv.total(), st));
+  const float *d_vel;
+  PW_TRY(upload3(S, base, b, wav, host, st));
+  PW_TRY(prep_vel3(S, vel, host, base, o_vel, o_mx, b, &d_vel, st));
+  Args p;
+  bind3(S, base, b, p);
+  float *rec = at<float>(base, o_rec);
+  LoopTimer timer(st);
+  timer.start();
+  long long launches = 0;
+  for (int s0 = 0; s0 < ns; s0 += nsb) {
+    const int nb_ = std::min(nsb, ns - s0);
+    float *A[MAXS3], *B[MAXS3];
+    for (int s = 0; s < nb_; s++) {
+      A[s] = at<float>(base, b.o_A) + s * fs;
+      B[s] = at<float>(base, b.o_B) + s * fs;
+    }
+    PW_CUDA(cudaMemsetAsync(base + b.o_A, 0, (size_t)nsb * fs * 4, st));
+    PW_CUDA(cudaMemsetAsync(base + b.o_B, 0, (size_t)nsb * fs * 4, st));
+    p.nshots = nb_;
+    p.shots = at<Shot>(base, b.o_shots) + s0;
+    p.rec = rec + (size_t)s0 * nt * nr;
+    p.ych = plan_ych(S.g, nb_);
+    for (int it = 0; it < nt; it++) {
+      p.it = it;
+      for (int s = 0; s < nb_; s++) {
+        p.cur[s] = A[s];
+        p.nxt[s] = B[s];
+      }
+      PW_TRY(launch3(p, FWD, st));
+      launches++;
+      for (int s = 0; s < nb_; s++) std::swap(A[s], B[s]);
+    }
+  }
+  timer.stop();
+  // [shot][nt][nr] -> [shot][nr][nt]
+  float *dst = host ? at<float>(base, o_out) : data;
+  for (int s = 0; s < ns; s++) {
+    dim3 tb(32, 8), tg(ceil_div(nr, 32), ceil_div(nt, 32));
+    pf::transpose_kernel<<<tg, tb, 0, st>>>(rec + (size_t)s * nt * nr, dst + (size_t)s * nt * nr,
+                                            nt, nr);
+  }
+  PW_CUDA(cudaGetLastError());
+  if (host) PW_TRY(to_host(data, dst, (size_t)ns * nt * nr * 4, true, st));
+  PW_CUDA(cudaStreamSynchronize(st));
+  timer.finish(launches, launches + 3 + ns);
+  return PW_OK;
+}
+
+extern "C" int pw_pfwi3d_gradient(const pw_fwi3d_args *a, const float *vel, const float *wav,
+                                  const float *dobs, const float *weight, float *grad,
+                                  double *misfit, int ckpt_k, void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  Setup3 S;
+  PW_TRY(setup3(a, S));
+  const bool host = (a->flags & PW_HOST_PTRS) != 0;
+  const int ns = a->ns, nt = a->nt, nr = S.nr;
+  const size_t nvel = (size_t)a->nz * a->nx * a->ny;
+  const size_t fs = (size_t)S.g.fstride;
+  Workspace &ws = Workspace::for_current_device();
+  std::lock_guard<std::mutex> lock(ws.mutex());
+  // checkpoint plan: the 2-D planner's rule on 3-D fields
+  pf::Setup P{};
+  P.a.nt = nt;
+  P.a.ns = std::min(ns, MAXS3);
+  P.a.hbm_budget = a->hbm_budget;
+  P.fstride = S.g.fstride;
+  const ExactPlan ep = plan_exact(P, ckpt_k, ws.capacity());
+  const int k = ep.k, nsb = ep.nsb, nck = (nt + k - 1) / k;
+  plan_record().k = k;
+  plan_record().nsb = nsb;
+  plan_record().recompute = ep.recompute;
+  Carve cv;
+  Bound3 b;
+  carve3(S, nsb, cv, b);
+  const size_t o_vel = cv.add(host ? nvel * 4 : 0);
+  const size_t o_w = cv.add(weight ? (size_t)nr * nt * 4 : 0);
+  const size_t o_dobs = cv.add((size_t)ns * nt * nr * 4);  // [shot][nt][nr]
+  const size_t o_dobs_in = cv.add(host ? (size_t)ns * nt * nr * 4 : 0);
+  const size_t o_d = cv.add((size_t)nsb * nt * nr * 4);
+  const size_t o_res = cv.add((size_t)nsb * nt * nr * 4);
+  const size_t o_ck = cv.add((size_t)nsb * nck * 2 * fs * 4);
+  const size_t o_tb = cv.add((size_t)nsb * k * fs * 4);
+  const size_t o_ga = cv.add(fs * 4);
+  const size_t o_gs = cv.add(nsb > 1 ? (size_t)nsb * fs * 4 : 0);
+  const size_t o_grad = cv.add(nvel * 4);
+  const size_t o_mis = cv.add(16);
+  const size_t o_mx = cv.add(16);
+  PW_TRY(ws.reserve(cv.total()));
+  plan_record().bytes = (long long)cv.total();
+  char *base = ws.base();
+  // checkpoints and segment terms are written before they are read
+  PW_CUDA(cudaMemsetAsync(base, 0, o_ck, st));
+  PW_CUDA(cudaMemsetAsync(base + o_ga, 0, cv.total() - o_ga, st));
+  const float *d_vel;
+  PW_TRY(upload3(S, base, b, wav, host, st));
+  PW_TRY(prep_vel3(S, vel, host, base, o_vel, o_mx, b, &d_vel, st));
+  float *d_w = nullptr;
+  if (weight) {
+    PW_TRY(to_device(base + o_w, weight, (size_t)nr * nt * 4, host, st));
+    d_w = at<float>(base, o_w);
+  }
+  {
+    const float *src = dobs;
+    if (host) {
+      PW_TRY(to_device(base + o_dobs_in, dobs, (size_t)ns * nt * nr * 4, true, st));
+      src = at<float>(base, o_dobs_in);
+    }
+    for (int s = 0; s < ns; s++) {
+      dim3 tb(32, 8), tg(ceil_div(nt, 32), ceil_div(nr, 32));
+      pf::transpose_kernel<<<tg, tb, 0, st>>>(src + (size_t)s * nr * nt,
+                                              at<float>(base, o_dobs) + (size_t)s * nt * nr, nr,
+                                              nt);
+    }
+    PW_CUDA(cudaGetLastError());
+  }
+  Args p;
+  bind3(S, base, b, p);
+  float *gacc = at<float>(base, o_ga), *gslices = at<float>(base, o_gs);
+  double *dmis = at<double>(base, o_mis);
+  p.grad = nsb > 1 ? gslices : gacc;
+  p.gstride = nsb > 1 ? (long long)fs : 0;
+  LoopTimer timer(st);
+  timer.start();
+  long long launches = 0;
+  for (int s0 = 0; s0 < ns; s0 += nsb) {
+    const int nb_ = std::min(nsb, ns - s0);
+    float *A[MAXS3], *B[MAXS3];
+    for (int s = 0; s < nb_; s++) {
+      A[s] = at<float>(base, b.o_A) + s * fs;
+      B[s] = at<float>(base, b.o_B) + s * fs;
+    }
+    PW_CUDA(cudaMemsetAsync(base + b.o_A, 0, (size_t)nsb * fs * 4, st));
+    PW_CUDA(cudaMemsetAsync(base + b.o_B, 0, (size_t)nsb * fs * 4, st));
+    p.nshots = nb_;
+    p.shots = at<Shot>(base, b.o_shots) + s0;
+    p.ych = plan_ych(S.g, nb_);
+    float *dd = at<float>(base, o_d), *res = at<float>(base, o_res);
+    float *ck = at<float>(base, o_ck), *tb = at<float>(base, o_tb);
+    // ---- forward: traces, checkpoints, the last segment's terms
+    p.rec = dd;
+    p.tout_stride = (long long)k * fs;
+    const int n_last = (nck - 1) * k;
+    for (int it = 0; it < nt; it++) {
+      if (it % k == 0 && it < n_last) {
+        const int m = it / k;
+        for (int s = 0; s < nb_; s++) {
+          float *c = ck + ((size_t)s * nck + m) * 2 * fs;
+          PW_CUDA(cudaMemcpyAsync(c, A[s], fs * 4, cudaMemcpyDeviceToDevice, st));
+          PW_CUDA(cudaMemcpyAsync(c + fs, B[s], fs * 4, cudaMemcpyDeviceToDevice, st));
+        }
+      }
+      p.tout = it >= n_last ? tb + (size_t)(it - n_last) * fs : nullptr;
+      p.it = it;
+      for (int s = 0; s < nb_; s++) {
+        p.cur[s] = A[s];
+        p.nxt[s] = B[s];
+      }
+      PW_TRY(launch3(p, FWD, st));
+      launches++;
+      for (int s = 0; s < nb_; s++) std::swap(A[s], B[s]);
+    }
+    p.rec = nullptr;
+    p.tout = nullptr;
+    // ---- FP64 misfit and the weighted residual
+    pf::residual_kernel<<<592, 256, 0, st>>>(dd, at<float>(base, o_dobs) + (size_t)s0 * nt * nr,
+                                             d_w, res, nb_, nt, nr, 1, dmis);
+    PW_CUDA(cudaGetLastError());
+    p.res = res;
+    // ---- backward by segments (the adjoint pair reuses the forward pair)
+    PW_CUDA(cudaMemsetAsync(base + b.o_A, 0, (size_t)nsb * fs * 4, st));
+    PW_CUDA(cudaMemsetAsync(base + b.o_B, 0, (size_t)nsb * fs * 4, st));
+    float *adjA[MAXS3], *adjB[MAXS3];
+    for (int s = 0; s < nb_; s++) {
+      adjA[s] = at<float>(base, b.o_A) + s * fs;
+      adjB[s] = at<float>(base, b.o_B) + s * fs;
+    }
+    p.tin_stride = (long long)k * fs;
+    for (int m = nck - 1; m >= 0; m--) {
+      const int n0 = m * k, n1 = std::min(nt, n0 + k);
+      float *FA[MAXS3], *FB[MAXS3];
+      for (int s = 0; s < nb_; s++) {
+        FA[s] = ck + ((size_t)s * nck + m) * 2 * fs;
+        FB[s] = FA[s] + fs;
+      }
+      for (int n = n0; n < n1 && m < nck - 1; n++) {  // the last segment is kept
+        p.it = n;
+        for (int s = 0; s < nb_; s++) {
+          p.cur[s] = FA[s];
+          p.nxt[s] = FB[s];
+        }
+        p.tout = tb + (size_t)(n - n0) * fs;
+        PW_TRY(launch3(p, FWD, st));
+        launches++;
+        for (int s = 0; s < nb_; s++) std::swap(FA[s], FB[s]);
+      }
+      p.tout = nullptr;
+      for (int n = n1 - 1; n >= n0; n--) {
+        p.it = n;
+        for (int s = 0; s < nb_; s++) {
+          p.cur[s] = adjA[s];
+          p.nxt[s] = adjB[s];
+        }
+        p.tin = tb + (size_t)(n - n0) * fs;
+        PW_TRY(launch3(p, ADJ_EXACT, st));
+        launches++;
+        for (int s = 0; s < nb_; s++) std::swap(adjA[s], adjB[s]);
+      }
+    }
+    p.tin = nullptr;
+    if (nsb > 1) {
+      pf::sum_slices_kernel<<<592, 256, 0, st>>>(gslices, nb_, (long long)fs, gacc);
+      PW_CUDA(cudaGetLastError());
+      PW_CUDA(cudaMemsetAsync(gslices, 0, (size_t)nb_ * fs * 4, st));
+      launches++;
+    }
+  }
+  timer.stop();
+  float *gdev = at<float>(base, o_grad);
+  fold_grad3_kernel<<<592, 256, 0, st>>>(gacc, d_vel, a->nz, a->nx, a->ny, a->nb, S.g, gdev);
+  PW_CUDA(cudaGetLastError());
+  PW_TRY(to_host(grad, gdev, nvel * 4, host, st));
+  if (misfit) PW_CUDA(cudaMemcpyAsync(misfit, dmis, 8, cudaMemcpyDeviceToHost, st));
+  PW_CUDA(cudaStreamSynchronize(st));
+  timer.finish(launches, launches + 8);
   return PW_OK;
 }
