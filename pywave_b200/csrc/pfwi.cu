@@ -441,9 +441,20 @@ __global__ void residual_kernel(const float *d, const float *dobs, const float *
   if (threadIdx.x < 32) {
     double v = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (threadIdx.x == 0) atomicAdd(misfit, v);
+    if (threadIdx.x == 0) misfit[1 + blockIdx.x] = v;  // block sums, added in order below
   }
 }
+
+// misfit[0] += the block sums misfit[1 .. nblocks] in block order (the same
+// bits on every run, whatever order the blocks ran in)
+__global__ void misfit_sum_kernel(double *misfit, int nblocks) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = misfit[0];
+    for (int b = 0; b < nblocks; b++) s += misfit[1 + b];
+    misfit[0] = s;
+  }
+}
+constexpr int RESID_BLOCKS = 592;
 
 // total[i] += slice_0[i] + slice_1[i] + ... in shot order (deterministic)
 __global__ void sum_slices_kernel(const float *slices, int nb, long long n, float *total) {
@@ -1230,7 +1241,7 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   const size_t o_gs = cv.add(nsb > 1 ? (size_t)nsb * gslice * 4 : 0);
   const size_t o_grad = cv.add(nvel * 4);
   const size_t o_m2v3 = cv.add(exact ? 0 : nvel * 4);
-  const size_t o_mis = cv.add(16);
+  const size_t o_mis = cv.add(8 * (1 + RESID_BLOCKS));
   const size_t o_mx = cv.add(16);
   PW_TRY(ws.reserve(cv.total()));
   if (exact) plan_record().bytes = (long long)cv.total();
@@ -1343,8 +1354,10 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
     p.snap = nullptr;
     p.tout = nullptr;
     // ---- residual and FP64 misfit
-    residual_kernel<<<592, 256, 0, st>>>(dd, at<float>(base, o_dobs) + (size_t)s0 * nt * nr,
-                                         at<float>(base, o_w), res, nb_, nt, nr, exact ? 1 : 0, dmis);
+    residual_kernel<<<RESID_BLOCKS, 256, 0, st>>>(dd, at<float>(base, o_dobs) + (size_t)s0 * nt * nr,
+                                                  at<float>(base, o_w), res, nb_, nt, nr,
+                                                  exact ? 1 : 0, dmis);
+    misfit_sum_kernel<<<1, 32, 0, st>>>(dmis, RESID_BLOCKS);
     PW_CUDA(cudaGetLastError());
     p.res = res;
     if (!exact) {
@@ -2086,7 +2099,7 @@ extern "C" int pw_pfwi3d_gradient(const pw_fwi3d_args *a, const float *vel, cons
   const size_t o_ga = cv.add(fs * 4);
   const size_t o_gs = cv.add(nsb > 1 ? (size_t)nsb * fs * 4 : 0);
   const size_t o_grad = cv.add(nvel * 4);
-  const size_t o_mis = cv.add(16);
+  const size_t o_mis = cv.add(8 * (1 + RESID_BLOCKS));
   const size_t o_mx = cv.add(16);
   PW_TRY(ws.reserve(cv.total()));
   plan_record().bytes = (long long)cv.total();
@@ -2165,8 +2178,9 @@ extern "C" int pw_pfwi3d_gradient(const pw_fwi3d_args *a, const float *vel, cons
     p.rec = nullptr;
     p.tout = nullptr;
     // ---- FP64 misfit and the weighted residual
-    pf::residual_kernel<<<592, 256, 0, st>>>(dd, at<float>(base, o_dobs) + (size_t)s0 * nt * nr,
-                                             d_w, res, nb_, nt, nr, 1, dmis);
+    pf::residual_kernel<<<pf::RESID_BLOCKS, 256, 0, st>>>(
+        dd, at<float>(base, o_dobs) + (size_t)s0 * nt * nr, d_w, res, nb_, nt, nr, 1, dmis);
+    pf::misfit_sum_kernel<<<1, 32, 0, st>>>(dmis, pf::RESID_BLOCKS);
     PW_CUDA(cudaGetLastError());
     p.res = res;
     // ---- backward by segments (the adjoint pair reuses the forward pair)

@@ -21,7 +21,7 @@ def _case(seed=1, ns=2, nt=160):
     t = np.arange(nt) * 0.001 - 0.05
     a = (np.pi * 20 * t) ** 2
     wav = (1e3 * (1 - 2 * a) * np.exp(-a)).astype(np.float32)
-    src = [(3, 6 + 10 * i, 5 + 6 * i) for i in range(ns)]
+    src = [(3, 5 + 5 * i, 4 + 4 * i) for i in range(ns)]
     geom = dict(nb=8, coef=0.02, dz=0.01, dx=0.01, dy=0.01, nt=nt, dt=0.001, src=src, rz=1,
                 rx=list(range(1, nx - 1, 3)), ry=list(range(1, ny - 1, 3)))
     return vt, vs, wav, geom
