@@ -1103,11 +1103,12 @@ extern "C" int pw_pfwi_forward(const pw_fwi_args *a, const float *vel, const flo
 // recomputes the (nck - 1) k steps before it: the recompute factor (forward
 // steps run / nt) is 1 + (nck - 1) k / nt.  Once the shots of a batch fill
 // the GPU a step costs in proportion to its shots, so the planner picks,
-// over batch sizes nsb = ns, ns/2, ... (down to 2 shots, the smallest whose
-// shot slices are summed in the same order as a full batch), the largest k
-// that fits the budget, and among those the plan with the least recompute,
-// then the largest batch.  k = nt stores every term and recomputes nothing;
-// a fixed ckpt_k > 0 keeps k and only shrinks the batch if needed.
+// over batch sizes nsb = ns, ns/2, ..., 1 (every batch sums its shots' slices
+// into the gradient in shot order, so the result does not depend on nsb),
+// the largest k that fits the budget, and among those the plan with the
+// least recompute, then the largest batch.  k = nt stores every term and
+// recomputes nothing; a fixed ckpt_k > 0 keeps k and only shrinks the batch
+// if needed.
 struct ExactPlan {
   int k = 0, nsb = 0;
   double recompute = 1.0;
@@ -1141,10 +1142,7 @@ static ExactPlan plan_exact(const Setup &S, int ckpt_k, size_t held) {
     int k;
     if (ckpt_k > 0) {
       k = std::min(ckpt_k, nt);
-      if (need(k, nb) > budget && nb > 1) {
-        if (nb <= 2) break;
-        continue;
-      }
+      if (need(k, nb) > budget && nb > 1) continue;
     } else if (need(nt, nb) <= budget) {
       k = nt;
     } else if (need(kmin, nb) <= budget) {
@@ -1169,12 +1167,12 @@ static ExactPlan plan_exact(const Setup &S, int ckpt_k, size_t held) {
       }
       if (ckpt_k > 0 || rc == 1.0) break;  // nothing better below
     }
-    if (nb <= 2) break;
+    if (nb == 1) break;
   }
   if (best.k == 0) {
-    // nothing fits the budget: the smallest working set (one batch of two
-    // shots or one, k = sqrt(2 nt)); the allocation reports if even that fails
-    best.nsb = std::min(nsb_max, 2);
+    // nothing fits the budget: the smallest working set (one shot, k =
+    // sqrt(2 nt)); the allocation reports if even that fails
+    best.nsb = 1;
     best.k = ckpt_k > 0 ? std::min(ckpt_k, nt) : kmin;
     best.recompute = recompute(best.k);
     best.bytes = (size_t)need(best.k, best.nsb);
@@ -1238,7 +1236,10 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   // shots of one launch run in different CTAs: each accumulates its gradient
   // in its own slice, summed into the total in shot order after the batch
   const size_t gslice = exact ? (size_t)S.fstride : nvel;
-  const size_t o_gs = cv.add(nsb > 1 ? (size_t)nsb * gslice * 4 : 0);
+  // exact mode: always through the slices (one shot per batch too), so the
+  // shots are summed in the same order whatever the batch size
+  const bool sliced = exact || nsb > 1;
+  const size_t o_gs = cv.add(sliced ? (size_t)nsb * gslice * 4 : 0);
   const size_t o_grad = cv.add(nvel * 4);
   const size_t o_m2v3 = cv.add(exact ? 0 : nvel * 4);
   const size_t o_mis = cv.add(8 * (1 + RESID_BLOCKS));
@@ -1293,8 +1294,8 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   p.wdt2 = (a->dt * interval) * (a->dt * interval);
   float *gtotal = exact ? gacc : gdev;
   float *gslices = at<float>(base, o_gs);
-  p.grad = nsb > 1 ? gslices : gtotal;
-  p.gstride = nsb > 1 ? (long long)gslice : 0;
+  p.grad = sliced ? gslices : gtotal;
+  p.gstride = sliced ? (long long)gslice : 0;
   const size_t fs = (size_t)S.fstride;
   long long launches = 0;
   LoopTimer timer(st);
@@ -1429,7 +1430,7 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
       p.tin = nullptr;
       p.imaging = 0;
     }
-    if (nsb > 1) {
+    if (sliced) {
       sum_slices_kernel<<<592, 256, 0, st>>>(gslices, nb_, (long long)gslice, gtotal);
       PW_CUDA(cudaGetLastError());
       PW_CUDA(cudaMemsetAsync(gslices, 0, (size_t)nb_ * gslice * 4, st));
@@ -2097,7 +2098,7 @@ extern "C" int pw_pfwi3d_gradient(const pw_fwi3d_args *a, const float *vel, cons
   const size_t o_ck = cv.add((size_t)nsb * nck * 2 * fs * 4);
   const size_t o_tb = cv.add((size_t)nsb * k * fs * 4);
   const size_t o_ga = cv.add(fs * 4);
-  const size_t o_gs = cv.add(nsb > 1 ? (size_t)nsb * fs * 4 : 0);
+  const size_t o_gs = cv.add((size_t)nsb * fs * 4);  // shot slices, summed in shot order
   const size_t o_grad = cv.add(nvel * 4);
   const size_t o_mis = cv.add(8 * (1 + RESID_BLOCKS));
   const size_t o_mx = cv.add(16);
@@ -2133,8 +2134,8 @@ extern "C" int pw_pfwi3d_gradient(const pw_fwi3d_args *a, const float *vel, cons
   bind3(S, base, b, p);
   float *gacc = at<float>(base, o_ga), *gslices = at<float>(base, o_gs);
   double *dmis = at<double>(base, o_mis);
-  p.grad = nsb > 1 ? gslices : gacc;
-  p.gstride = nsb > 1 ? (long long)fs : 0;
+  p.grad = gslices;
+  p.gstride = (long long)fs;
   LoopTimer timer(st);
   timer.start();
   long long launches = 0;
@@ -2224,7 +2225,7 @@ extern "C" int pw_pfwi3d_gradient(const pw_fwi3d_args *a, const float *vel, cons
       }
     }
     p.tin = nullptr;
-    if (nsb > 1) {
+    {
       pf::sum_slices_kernel<<<592, 256, 0, st>>>(gslices, nb_, (long long)fs, gacc);
       PW_CUDA(cudaGetLastError());
       PW_CUDA(cudaMemsetAsync(gslices, 0, (size_t)nb_ * fs * 4, st));

@@ -140,7 +140,8 @@ def test_exact_gradient_independent_of_hbm_budget(golden, cuda_lib):
         print(f"budget {budget >> 20} MiB: k {k}, shots per batch {nsb}, held {nbytes / 2**20:.1f} "
               f"MiB, recompute factor {rc:.3f}")
         assert np.array_equal(gb, ref), budget
-        assert Jb == Jr
+        # the FP64 misfit's partial sums follow the batching
+        assert abs(Jb - Jr) <= 1e-12 * abs(Jr)
     assert plans[0][1] == 400 and plans[0][4] == 1.0  # the default budget keeps every term
     assert plans[-1][1] < plans[1][1] and plans[-1][4] > 1.0
     for budget, k, nsb, nbytes, rc in plans[1:]:
