@@ -894,22 +894,21 @@ __device__ __forceinline__ void flush_path_counts(const StepArgs &a, int lane,
 }
 
 // cp.async ring of the warp-tile kernel (CTA = the G group warps of WZ x WX
-// tiles, as with the TMA ring).  NC = 1: one ring of TILE_NS slots, each the
+// tiles, as with the TMA ring).  !SPLIT: one ring of TILE_NS slots, each the
 // A patch of a plane with this warp's B and vv cells of that plane (copied
-// four planes before their use).  NC = 2: an A ring of TILE_NS patches and a
+// four planes before their use).  SPLIT: an A ring of TILE_NS patches and a
 // separate ring of TILE_BV_NS planes of B and vv, copied two planes before
-// their use, which keeps the larger patches within the shared memory of
-// three resident CTAs.
+// their use: less shared memory per warp (more resident warps) for a few
+// more instructions per plane.
 constexpr int TILE_BV_NS = 3;
-__host__ __device__ constexpr int tile_cp_ws(int nc) {  // float4 per warp
-  return nc == 1 ? TILE_NS * tile_slot(1) : TILE_NS * tile_tp(nc) + TILE_BV_NS * 64 * nc;
+__host__ __device__ constexpr int tile_cp_ws(int nc, bool split) {  // float4 per warp
+  return !split ? TILE_NS * tile_slot(nc) : TILE_NS * tile_tp(nc) + TILE_BV_NS * 64 * nc;
 }
 
-template <bool TRI, bool SNAP, int NC>
+template <bool TRI, bool SNAP, int NC, bool SPLIT>
 __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
   extern __shared__ float4 tsm[];
   constexpr int NS = TILE_NS, D = NS - 3, TP = tile_tp(NC), BVS = 64 * NC;
-  constexpr bool SPLIT = NC > 1;
   constexpr int ASTEP = SPLIT ? TP : tile_slot(NC);  // float4 between A slots
   constexpr int CPL = (TP + 31) / 32;                // A-patch copies per lane per plane
   static_assert(NS == 5, "the y loop is unrolled by the queue length 5");
@@ -927,7 +926,7 @@ __global__ void __launch_bounds__(TILE_MAXT) tile_kernel(const StepArgs a) {
     }
   const long long sx = g.sx, sy = g.sy;
   const long long safe = sx * g.hx + sy * g.hy;
-  float4 *ring = tsm + (size_t)w * tile_cp_ws(NC);  // A slots (with B / vv when !SPLIT)
+  float4 *ring = tsm + (size_t)w * tile_cp_ws(NC, SPLIT);  // A slots (B / vv too when !SPLIT)
   float4 *bvring = ring + NS * TP;                  // SPLIT: TILE_BV_NS planes of [B, vv]
   const int y0 = blockIdx.y * a.ych;
   const int y1 = min(g.ny, y0 + a.ych);
@@ -1493,15 +1492,24 @@ static int plan_march(bool tri, int G, int nsm, Plan &p) {
   return PW_OK;
 }
 
+// split B / vv ring of the cp.async kernel: with two columns per lane, or
+// when PW_AFD_SPLIT=1
+static bool tile_split(int nc) {
+  if (nc > 1) return true;
+  const char *e = getenv("PW_AFD_SPLIT");
+  return e && e[0] == '1';
+}
+
 static size_t tile_smem(int threads, bool tma, int nc) {
   const size_t nw = (size_t)threads / 32;
-  if (!tma) return nw * tile_cp_ws(nc) * sizeof(float4);
+  if (!tma) return nw * tile_cp_ws(nc, tile_split(nc)) * sizeof(float4);
   return nw * tile_ws(nc) * sizeof(float4) + nw * TILE_NS * sizeof(unsigned long long);
 }
 
-template <bool TRI, bool SNAP, bool TMA, int NC>
+template <bool TRI, bool SNAP, bool TMA, int NC, bool SPLIT = (NC > 1)>
 static void *tile_ptr() {
-  void *f = TMA ? (void *)tile_kernel_tma<TRI, SNAP, NC> : (void *)tile_kernel<TRI, SNAP, NC>;
+  void *f = TMA ? (void *)tile_kernel_tma<TRI, SNAP, NC>
+                : (void *)tile_kernel<TRI, SNAP, NC, SPLIT>;
   static bool once = [f] {
     // as much as a block may opt into (the planner only picks launchable tiles)
     int dev = 0, maxsm = 0;
@@ -1518,7 +1526,10 @@ static void *tile_ptr() {
 
 template <bool TRI, bool SNAP>
 static void *tile_fn_t(bool tma, int nc) {
-  if (!tma) return nc == 2 ? tile_ptr<TRI, SNAP, false, 2>() : tile_ptr<TRI, SNAP, false, 1>();
+  if (!tma) {
+    if (nc == 2) return tile_ptr<TRI, SNAP, false, 2>();
+    return tile_split(1) ? tile_ptr<TRI, SNAP, false, 1, true>() : tile_ptr<TRI, SNAP, false, 1>();
+  }
   return nc == 2 ? tile_ptr<TRI, SNAP, true, 2>() : tile_ptr<TRI, SNAP, true, 1>();
 }
 static void *tile_fn(bool tri, bool snap, bool tma, int nc) {
@@ -1620,7 +1631,7 @@ static int plan_tile(bool tri, int G, int nsm, bool tma, Plan &p) {
             "afd tile plan: G=%d S=%d nzc=%d WZ=%d WX=%d NC=%d ych=%d threads=%d grid=%ux%u "
             "score=%.3f ring=%s\n",
             G, S, p.nzc, bz, bx, bnc, by, p.threads, p.grid.x, p.grid.y, best,
-            tma ? "tma" : "cp.async");
+            tma ? "tma" : (tile_split(bnc) ? "cp.async+split" : "cp.async"));
   return PW_OK;
 }
 

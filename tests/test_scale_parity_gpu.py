@@ -43,13 +43,14 @@ def _plan_grid(err: str):
 
 # ------------------------------------------------------------ afd 3-D ----
 
-# (ring filling, PW_AFD_TMA, columns per lane)
-RINGS = [("cp.async", "0", "1"), ("cp.async", "0", "2"), ("tma", "1", "1"), ("tma", "1", "2")]
+# (ring filling as the plan prints it, PW_AFD_TMA, columns per lane, PW_AFD_SPLIT)
+RINGS = [("cp.async", "0", "1", "0"), ("cp.async+split", "0", "1", "1"),
+         ("cp.async+split", "0", "2", "0"), ("tma", "1", "1", "0"), ("tma", "1", "2", "0")]
 
 
-@pytest.mark.parametrize("ring,env,nc", RINGS)
+@pytest.mark.parametrize("ring,env,nc,split", RINGS)
 def test_afd3d_untapered_paths_bit_exact_vs_reference(golden, cuda_lib, monkeypatch, capfd, ring,
-                                                      env, nc):
+                                                      env, nc, split):
     """80 x 72 x 64 interior, nbt 10, 2 sources, nt 60: traces and snapshots
     identical to the reference's afd3d with either ring filling (per-lane
     cp.async or TMA tile loads) and one or two columns per lane, every
@@ -64,11 +65,12 @@ def test_afd3d_untapered_paths_bit_exact_vs_reference(golden, cuda_lib, monkeypa
     monkeypatch.setenv("PW_AFD_VERBOSE", "1")
     monkeypatch.setenv("PW_AFD_TMA", env)
     monkeypatch.setenv("PW_AFD_NC", nc)
+    monkeypatch.setenv("PW_AFD_SPLIT", split)
     d, w = pw.afd3d(vel, wavelet=g["rick"], **kw)
     err = capfd.readouterr().err
     c = _counts(err)[-1]
     print(err)
-    assert f"ring={ring}" in err and f"NC={nc}" in err
+    assert re.search(rf"ring={re.escape(ring)}\s", err) and f"NC={nc}" in err
     assert all(c[f"fwd_path{k}"] > 0 for k in range(4))
     assert any(gy > 1 for _, gy in _plan_grid(err))
     assert np.array_equal(d[::3, ::4, ::4], g["traces_dec"])
@@ -78,9 +80,9 @@ def test_afd3d_untapered_paths_bit_exact_vs_reference(golden, cuda_lib, monkeypa
     assert M.digest(w) == str(g["snaps_digest"])
 
 
-@pytest.mark.parametrize("ring,env,nc", RINGS)
+@pytest.mark.parametrize("ring,env,nc,split", RINGS)
 def test_afd3d_tri_untapered_paths_bit_exact_vs_reference(golden, cuda_lib, monkeypatch, capfd,
-                                                          ring, env, nc):
+                                                          ring, env, nc, split):
     """Time reversal of one x-band group's traces on the same grid: every
     snapshot identical to the reference's with either ring filling, every
     taper path taken."""
@@ -96,12 +98,13 @@ def test_afd3d_tri_untapered_paths_bit_exact_vs_reference(golden, cuda_lib, monk
     monkeypatch.setenv("PW_AFD_VERBOSE", "1")
     monkeypatch.setenv("PW_AFD_TMA", env)
     monkeypatch.setenv("PW_AFD_NC", nc)
+    monkeypatch.setenv("PW_AFD_SPLIT", split)
     _, wt = pw.afd3d(vel, nt=kw["nt"], dt=0.001, ax=kw["ax"], ay=kw["ay"], az=kw["az"],
                      jsnap=M.BIG3D_TRI_JSNAP, dat=dg, tri=True, nbt=10, ct=0.02)
     err = capfd.readouterr().err
     c = _counts(err)[-1]
     print(err)
-    assert f"ring={ring}" in err and f"NC={nc}" in err
+    assert re.search(rf"ring={re.escape(ring)}\s", err) and f"NC={nc}" in err
     assert all(c[f"tri_path{k}"] > 0 for k in range(4))
     assert tuple(wt.shape) == tuple(g["tri_shape"])
     assert np.array_equal(wt[::4, ::4, ::4, 0], g["tri_last_dec"])
