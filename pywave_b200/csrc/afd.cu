@@ -1492,12 +1492,14 @@ static int plan_march(bool tri, int G, int nsm, Plan &p) {
   return PW_OK;
 }
 
-// split B / vv ring of the cp.async kernel: with two columns per lane, or
-// when PW_AFD_SPLIT=1
+// split B / vv ring of the cp.async kernel (3 slots of B and vv beside the
+// 5-slot A ring, less shared memory per warp, so more warps resident): the
+// default; PW_AFD_SPLIT=0 selects one 5-slot ring of [A, B, vv] at one
+// column per lane
 static bool tile_split(int nc) {
   if (nc > 1) return true;
   const char *e = getenv("PW_AFD_SPLIT");
-  return e && e[0] == '1';
+  return !(e && e[0] == '0');
 }
 
 static size_t tile_smem(int threads, bool tma, int nc) {
