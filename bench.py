@@ -48,10 +48,11 @@ def parse():
     p.add_argument("--no-fwi2d", action="store_true",
                    help="tri3d: skip the secondary 2-D FWI gradients/s field")
     p.add_argument("--workload", default="tri3d",
-                   choices=["tri3d", "fwi2d", "batch2d", "c1", "fwi3d"],
+                   choices=["tri3d", "fwi2d", "batch2d", "c1", "fwi3d", "lstri"],
                    help="tri3d: the 3-D TRI image (default); fwi2d: 2-D FWI gradients/s; "
                         "batch2d: uneven 2-D forward shots in one batch; c1: one 2-D shot; "
-                        "fwi3d: 3-D FWI gradients/s")
+                        "fwi3d: 3-D FWI gradients/s; lstri: pfwi mode 4 source inversion")
+    p.add_argument("--lstri-niter", type=int, default=30, help="lstri: CG iterations per shot")
     p.add_argument("--fwi3d-nt", type=int, default=2500, help="fwi3d: time samples")
     p.add_argument("--fwi3d-shots", type=int, default=16, help="fwi3d: shots per gradient")
     p.add_argument("--shots", type=int, default=32, help="fwi2d: shots per gradient")
@@ -1098,6 +1099,195 @@ def run_fwi3d(args, world, rank, local):
             "clocks": clocks}), flush=True)
 
 
+# pfwi passive mode 4 at the size of the reference's passive demos
+# (demos/test_pfwi_mod2d.py): 130 x 334 at 8 x 12 m, nb 60, nt 3001, 3 shots,
+# 30 CG iterations of the source inversion per shot
+LS_NZ, LS_NX, LS_DZ, LS_DX, LS_NT, LS_DT, LS_NB, LS_COEF, LS_NS = \
+    130, 334, 0.008, 0.012, 3001, 0.001, 60, 0.005, 3
+
+
+def lstri_par(niter, ns=LS_NS):
+    return dict(nz=LS_NZ, nx=LS_NX, dz=LS_DZ, dx=LS_DX, oz=0, ox=0, nt=LS_NT, dt=LS_DT, ot=0,
+                ns=ns, ds=0.1, os=0.0, nb=LS_NB, coef=LS_COEF, f0=10, acqui_type=1, interval=1,
+                niter=niter)
+
+
+def lstri_case(seed, ns=LS_NS):
+    """Velocity 1.8 -> 3.0 km/s with depth plus 0.2 seeded noise; per shot
+    three buried point sources carrying 10 Hz Ricker pulses of amplitude 1e6
+    at seeded delays (the demos' source scale)."""
+    rng = np.random.default_rng(seed)
+    z = np.arange(LS_NZ, dtype=np.float32)[:, None]
+    vel = (1.8 + 1.2 * z / LS_NZ + 0.2 * rng.random((LS_NZ, LS_NX))).astype(np.float32)
+    src = np.zeros((ns, LS_NT, LS_NX, LS_NZ), np.float32)  # [ns][nt][nx][nz]
+    t = np.arange(LS_NT) * LS_DT
+    for s in range(ns):
+        for _ in range(3):
+            iz, ix = int(rng.integers(60, 125)), int(rng.integers(20, LS_NX - 20))
+            a = (np.pi * 10.0 * (t - float(rng.uniform(0.1, 0.5)))) ** 2
+            src[s, :, ix, iz] = (1e6 * (1 - 2 * a) * np.exp(-a)).astype(np.float32)
+    return vel, src
+
+
+def _ls_ref_worker(kind):
+    """One lstric modelling call (inv 0) of one shot at the benchmark size by
+    the reference itself (oracle/_ref pfwicfun; kind "port": the oracle's
+    restatement); returns (point-updates, seconds)."""
+    sys.path.insert(0, ROOT)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    vel, src = lstri_case(7, ns=1)
+    par = lstri_par(1, ns=1)
+    pts = (LS_NZ + 2 * LS_NB) * (LS_NX + 2 * LS_NB) * LS_NT
+    if kind == "reference":
+        sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+        import pfwicfun  # the reference's own extension module
+        from pywave_b200.pfwi import fillpar, pararray
+        arr = pararray(fillpar(dict(par, inv=0)))
+        q = np.full(LS_NZ * LS_NX, 1e4, np.float32)
+        flat = np.ascontiguousarray(src[0].reshape(-1))  # [nt][nx][nz] = F-order (nz,nx,nt)
+        t0 = time.perf_counter()
+        pfwicfun.lstric(vel.flatten(order="F"), q, np.zeros(LS_NT, np.float32), flat, arr)
+    else:
+        from oracle import oracle as O
+        m = src[0].transpose(2, 1, 0)
+        t0 = time.perf_counter()
+        O.timerev(False, vel, LS_NT, LS_NB, LS_COEF, LS_DZ, LS_DX, LS_DT, mod=m)
+    return pts, time.perf_counter() - t0
+
+
+def _ls_cpu(workers):
+    for kind in ("reference", "port"):
+        try:
+            res = pool_map(_ls_ref_worker, [(kind,)] * workers, timeout_s=600)
+            return sum(r[0] for r in res) / max(r[1] for r in res) / 1e9, kind
+        except Exception:  # noqa: BLE001
+            continue
+    raise RuntimeError("neither the reference nor the port ran")
+
+
+def run_lstri(args, world, rank, local):
+    niter = args.lstri_niter
+    pad = (LS_NZ + 2 * LS_NB) * (LS_NX + 2 * LS_NB)
+    cfg = {"workload": f"pfwi mode 4 LS-TRI source inversion {LS_NZ}x{LS_NX} dz=8m dx=12m "
+                       f"nt={LS_NT} nb={LS_NB} shots={LS_NS} CG iterations={niter}",
+           "padded_cells": pad}
+    metric = "Gpt-updates/s (2-D time-reversal operator, LS-TRI inversion)"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        workers = max(1, min(os.cpu_count() or 1, 16))
+        rates = []
+        for i in range(args.warmup + args.steps):
+            v, kind = _ls_cpu(workers)
+            if i >= args.warmup:
+                rates.append(v)
+        value = statistics.median(rates)
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": value, "unit": "Gpt/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "Gpt/s", "cores": workers, "kind": kind,
+                             "sample": f"one lstric modelling call (inv 0, one shot, nt={LS_NT}) "
+                                       f"per process, {workers} single-threaded processes"},
+            "e2e": {"value": value, "unit": "Gpt/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    import torch.distributed as dist
+    from pywave_b200 import _lib as L
+    from pywave_b200 import build as B
+    from pywave_b200 import lstri, pfwicfun
+    from pywave_b200.pfwi import fillpar, pararray
+    B.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    vel, src = lstri_case(7 + rank)
+    par = lstri_par(niter)
+    v_d = torch.from_numpy(np.ascontiguousarray(vel.T)).cuda()
+    s_d = torch.from_numpy(src).cuda()
+    d_d = torch.empty((LS_NS, LS_NX, LS_NT), device="cuda")
+    lstri.lstri_forward_torch(v_d, s_d, d_d, par)  # the observed data
+    inv_d = torch.empty_like(s_d)
+    del s_d
+
+    def step():
+        lstri.lstri_invert_torch(v_d, d_d, inv_d, par)
+        return L.last_timing()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = Clocks(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    e0.record()
+    for _ in range(args.steps):
+        launches += step()[2]
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    updates = pad * LS_NT * 2 * niter * LS_NS  # adjoint + modelling per iteration
+    # one modelling operator alone, timed on the device (resident launch)
+    fwd_ms = []
+    scratch = torch.empty_like(d_d[0])
+    for _ in range(3):
+        lstri.timerev_torch(False, v_d, dict(par, ns=1), inv_d[0], scratch)
+        fwd_ms.append(L.last_timing()[0])
+    op_ms = statistics.median(fwd_ms)
+    # fp32 issue bound of one 16-SM cluster: 40 float operations per cell
+    # (Laplacian 30, update 3, two sponge products, injection 2)
+    sm_clk = (clocks or {}).get("sm_mhz") or 1965.0
+    cluster_flops = 16 * 128 * sm_clk * 1e6
+    op_flops = 40.0 * pad * LS_NT
+    # end to end through the drop-in module: host data in, host source field out
+    e2e = None
+    if not args.no_e2e:
+        dh = np.ascontiguousarray(d_d.cpu().numpy().reshape(-1))  # [ns][nx][nt]
+        arr = pararray(fillpar(dict(par, inv=1)))
+        q = np.full(LS_NZ * LS_NX, 1e4, np.float32)
+        t0 = time.perf_counter()
+        out = pfwicfun.lstric(vel.flatten(order="F"), q, np.zeros(LS_NT, np.float32), dh, arr)
+        wall = time.perf_counter() - t0
+        e2e = {"value": updates / wall / 1e9, "unit": "Gpt/s",
+               "h2d_bytes_per_step": int(dh.nbytes + vel.nbytes),
+               "d2h_bytes_per_step": int(out.nbytes)}
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0:
+        workers = max(1, min(os.cpu_count() or 1, 16))
+        v, kind = _ls_cpu(workers)
+        cpu = {"value": v, "unit": "Gpt/s", "cores": workers, "kind": kind,
+               "sample": f"one lstric modelling call (inv 0, one shot, nt={LS_NT}) per process, "
+                         f"{workers} single-threaded processes"}
+    peak, peak_kind = peaks()
+    src_bytes = 4.0 * LS_NZ * LS_NX * LS_NT  # the modelling operator reads the source field
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": job_rate(updates, args.steps, world, ms) / 1e9,
+            "unit": "Gpt/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 CG dots)",
+            "data": "synthetic (seeded layered model, 3 buried Ricker sources per shot)",
+            "config": cfg, "inversions_per_s": 1000.0 * args.steps / ms,
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": src_bytes / (op_ms / 1e3) / 1e9,
+                         "peak": peak, "unit": "GB/s",
+                         "frac": src_bytes / (op_ms / 1e3) / 1e9 / peak, "traffic": None,
+                         "kernel": "tr::resident_kernel modelling (one shot, one launch)",
+                         "op_ms": op_ms, "peak_source": peak_kind,
+                         "cluster_fp32_frac": op_flops / (op_ms / 1e3) / cluster_flops,
+                         "note": "one 16-SM cluster per shot: bound by that cluster's fp32 "
+                                 "issue and its per-step barrier, not by HBM"},
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks}), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1111,6 +1301,8 @@ def main():
         return run_c1(args, world, rank, local)
     if args.workload == "fwi3d":
         return run_fwi3d(args, world, rank, local)
+    if args.workload == "lstri":
+        return run_lstri(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, rank)
 

@@ -240,6 +240,35 @@ int pw_gradient_postprocess(int nz, int nx, int rect, int waterz, float *grad, f
 int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav, const float *dobs,
            float *vinv, int *iters_done, void *stream);
 
+/* ---------------------------------------------- pfwi mode 4: LS-TRI --- */
+
+/* pfwi's passive mode 4 without velocity update (pfwicfun.lstric,
+ * pywave/src/pfwi.c:1031-1444).  Geometry from pw_fwi_args: nz, nx, dz, dx,
+ * nt, dt, ns, nb (>= 4), coef, rz (the data row is padded row rz + nb; the
+ * pararray parser sets rz = 1 as pfwi.c:1319 does), niter (CG iterations),
+ * flags (PW_HOST_PTRS).  vel [nx][nz]; a shot's source field
+ * [nt][nx][nz]; a shot's data [nx][nt].  Fields and data are bit-identical
+ * to the reference's timerev_lop (wave_triutil.c:48-316). */
+
+/* timerev_lop with add = 0, one shot (wave_triutil.c:86-180): adj = 0 maps
+ * mod to dat, adj = 1 maps dat to mod. */
+int pw_timerev(const pw_fwi_args *a, int adj, const float *vel, float *mod, float *dat,
+               void *stream);
+
+/* lstric with inv = 0 (lstri, wave_fwi.c:121-175): data [ns][nx][nt] of the
+ * source fields src [ns][nt][nx][nz]; every shot in one launch. */
+int pw_lstri_forward(const pw_fwi_args *a, const float *vel, const float *src, float *data,
+                     void *stream);
+
+/* lstric with inv = 1 (lstri_op, wave_fwigradient.c:454-520): per shot,
+ * a->niter conjugate-gradient iterations of np_solver / np_cgstep
+ * (wave_bigsolver.c:1170, wave_cgstep.c:16) from a zero source field;
+ * src [ns][nt][nx][nz] out, data [ns][nx][nt] in.  The CG step vectors carry
+ * over from one shot to the next within the call, as the reference's do;
+ * dot products run in FP64 in a fixed block order. */
+int pw_lstri_invert(const pw_fwi_args *a, const float *vel, const float *data, float *src,
+                    void *stream);
+
 /* ------------------------------------------------------------ utility --- */
 
 const char *pw_last_error(void);

@@ -31,7 +31,7 @@ _lib = None
 def build(force: bool = False) -> str:
     """Compile the oracle restatement (gcc, no FMA contraction)."""
     srcs = [os.path.join(HERE, f) for f in ("pw_oracle.c", "pw_oracle_body.h",
-                                             "pw_oracle3d_body.h")]
+                                             "pw_oracle3d_body.h", "pw_oracle_lstri_body.h")]
     stale = (not os.path.exists(LIB_PATH)) or any(
         os.path.getmtime(s) > os.path.getmtime(LIB_PATH) for s in srcs)
     if force or stale:
@@ -98,6 +98,12 @@ def lib():
             f = getattr(L, "or_pf3_misfit_" + sfx)
             f.argtypes = geo3 + [rp, rp, rp, C.c_void_p]
             f.restype = real
+            f = getattr(L, "or_lstri_" + sfx)
+            f.argtypes = [C.c_int] * 7 + [C.c_float] * 4 + [C.c_int, _f32p, rp, rp, C.c_void_p]
+            f.restype = None
+            f = getattr(L, "or_timerev_" + sfx)
+            f.argtypes = [C.c_int] * 6 + [C.c_float] * 4 + [_f32p, rp, rp]
+            f.restype = None
         _lib = L
     return _lib
 
@@ -378,3 +384,57 @@ def pf3_misfit(vel, wav, dobs, g, weight=None, precision="f64"):
         *geo, _vel3(vel, R), np.ascontiguousarray(np.asarray(wav).astype(R)),
         np.ascontiguousarray(np.asarray(dobs).astype(R).reshape(-1)),
         None if wt is None else wt.ctypes.data))
+
+
+# --------------------------------------------------------------------------
+# pfwi passive mode 4: timerev_lop and the LS-TRI inversion
+# (pw_oracle_lstri_body.h; wave_triutil.c:48-316, wave_fwi.c:121,
+# wave_bigsolver.c:1170, wave_cgstep.c:16)
+# --------------------------------------------------------------------------
+
+def _vel2(vel):
+    # (nz, nx) -> [nx][nz]
+    return np.ascontiguousarray(np.asarray(vel, np.float32).T)
+
+
+def timerev(adj, vel, nt, nb, coef, dz, dx, dt, rz=1, mod=None, dat=None, precision="f32"):
+    """One application of timerev_lop: adj=False maps mod (nz, nx, nt) to
+    data (nt, nx); adj=True maps dat (nt, nx) to mod (nz, nx, nt)."""
+    R = np.float32 if precision == "f32" else np.float64
+    nz, nx = np.shape(vel)
+    if adj:
+        d = np.ascontiguousarray(np.asarray(dat).astype(R).T)  # [nx][nt]
+        m = np.zeros(nt * nx * nz, R)
+    else:
+        m = np.ascontiguousarray(np.asarray(mod).astype(R).transpose(2, 1, 0))  # [nt][nx][nz]
+        d = np.zeros(nx * nt, R)
+    getattr(lib(), "or_timerev_" + precision)(int(adj), nz, nx, nt, nb, rz, dt, dx, dz, coef,
+                                              _vel2(vel), m.reshape(-1), d.reshape(-1))
+    if adj:
+        return m.reshape(nt, nx, nz).transpose(2, 1, 0)
+    return d.reshape(nx, nt).T
+
+
+def lstri(inv, vel, par, src=None, data=None, precision="f32"):
+    """pfwicfun.lstric restated: inv=0 maps src (nz, nx, nt, ns) to data
+    (nt, nx, ns); inv=1 inverts data for src with par['niter'] CG
+    iterations per shot.  par: nz, nx, dz, dx, nt, dt, ns, nb, coef, niter.
+    Returns (result, iterations per shot)."""
+    R = np.float32 if precision == "f32" else np.float64
+    nz, nx = np.shape(vel)
+    nt, ns = int(par["nt"]), int(par["ns"])
+    if inv:
+        d = np.ascontiguousarray(np.asarray(data).astype(R).reshape(nt, nx, ns).transpose(2, 1, 0))
+        s = np.zeros((ns, nt, nx, nz), R)
+    else:
+        s = np.ascontiguousarray(np.asarray(src).astype(R).reshape(nz, nx, nt, ns)
+                                 .transpose(3, 2, 1, 0))
+        d = np.zeros((ns, nx, nt), R)
+    iters = np.zeros(ns, np.int32)
+    getattr(lib(), "or_lstri_" + precision)(
+        int(inv), nz, nx, nt, ns, int(par["nb"]), int(par.get("rz", 1)), float(par["dt"]),
+        float(par["dx"]), float(par["dz"]), float(par["coef"]), int(par.get("niter", 0)),
+        _vel2(vel), s.reshape(-1), d.reshape(-1), iters.ctypes.data)
+    if inv:
+        return s.transpose(3, 2, 1, 0), iters
+    return d.transpose(2, 1, 0), iters

@@ -19,7 +19,11 @@
  * plus the exact discrete adjoint of the pfwi forward step (FP64), derived
  * for this project and checked against finite differences in tests/, and
  * the 3-D extension of the pfwi scheme with its exact adjoint
- * (pw_oracle3d_body.h; the reference has no 3-D FWI).
+ * (pw_oracle3d_body.h; the reference has no 3-D FWI), and pfwi's passive
+ * mode 4 (pw_oracle_lstri_body.h): the time-reversal operator timerev_lop
+ * (pywave/src/wave_triutil.c:48-316) and the LS-TRI source inversion by
+ * np_solver / np_cgstep (wave_fwi.c:121, wave_bigsolver.c:1170,
+ * wave_cgstep.c:16).
  *
  * The body is instantiated twice (pw_oracle_body.h): REAL=float reproduces
  * the reference's float evaluation order operation by operation (no FMA
@@ -31,6 +35,7 @@
  * by tests/golden/make_golden.py from the reference compiled under oracle/_ref).
  */
 #include <math.h>
+#include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -165,6 +170,7 @@ void or_residual_weights(int nt, int nr, int wtn1, int wtn2, int woffn1, int wof
 #define PW_F32 1
 #include "pw_oracle_body.h"
 #include "pw_oracle3d_body.h"
+#include "pw_oracle_lstri_body.h"
 #undef REAL
 #undef SFX
 #undef PW_F32
@@ -174,6 +180,7 @@ void or_residual_weights(int nt, int nr, int wtn1, int wtn2, int woffn1, int wof
 #define PW_F32 0
 #include "pw_oracle_body.h"
 #include "pw_oracle3d_body.h"
+#include "pw_oracle_lstri_body.h"
 #undef REAL
 #undef SFX
 #undef PW_F32

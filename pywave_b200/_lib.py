@@ -95,6 +95,9 @@ _SIGS = {
     "pw_pfwi3d_forward": (C.c_int, [C.POINTER(Fwi3dArgs), _vp, _vp, _vp, _vp]),
     "pw_pfwi3d_gradient": (C.c_int, [C.POINTER(Fwi3dArgs), _vp, _vp, _vp, _vp, _vp, _vp,
                                      C.c_int, _vp]),
+    "pw_timerev": (C.c_int, [C.POINTER(FwiArgs), C.c_int, _vp, _vp, _vp, _vp]),
+    "pw_lstri_forward": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp]),
+    "pw_lstri_invert": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp]),
     "pw_last_fwi_plan": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int),
                                    C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
     "pw_last_error": (C.c_char_p, []),

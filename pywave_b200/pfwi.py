@@ -1,8 +1,10 @@
 """``pfwi`` and ``fillpar`` with the reference's signatures (pywave/pfwi.py:5, :262).
 
-Modes 1 (modelling) and 2 (FWI) run on the GPU engine; mode 3 (RTM) does
-nothing, as in the reference (pfwi.py:114-119); mode 4 (passive source)
-raises ``NotImplementedError``.  As in the reference only ``par`` is read:
+Modes 1 (modelling), 2 (FWI) and 4 without velocity update (passive
+modelling and least-squares time-reversal source inversion, lstric) run on
+the GPU engine; mode 3 (RTM) does nothing, as in the reference
+(pfwi.py:114-119); mode 4 with velocity update (pfwic) raises
+``NotImplementedError``.  As in the reference only ``par`` is read:
 the keyword arguments after ``mode`` are accepted and ignored
 (pfwi.py:29-61).
 """
@@ -23,8 +25,9 @@ def pararray(par):
 
 def pfwi(vel, q, wav, src, data=None, mode=1, media=1, inv=0, verb=1, nb=60, coef=0.005, acq=1,
          ss=[0, 0.2, 1], f0=10, waterz=-30, niter=30, conv_e=0.01, par=None):
-    """Acoustic modelling (mode 1) or FWI (mode 2).  Returns
-    ``(data, vinv, grad, src, mwt)`` like pywave.pfwi."""
+    """Acoustic modelling (mode 1), FWI (mode 2) or passive modelling /
+    source inversion (mode 4).  Returns ``(data, vinv, grad, src, mwt)``
+    like pywave.pfwi."""
     par = fillpar(par)
     if mode == 1:
         v = np.asarray(vel).flatten(order="F").astype(np.float32)
@@ -44,9 +47,30 @@ def pfwi(vel, q, wav, src, data=None, mode=1, media=1, inv=0, verb=1, nb=60, coe
     if mode == 3:
         return data, None, None, src, None
     if mode == 4:
-        raise NotImplementedError("passive-source mode 4 (lstric / pfwic) is not built")
+        return _mode4(vel, q, wav, src, data, par)
     print("Wrong mode")
     return 0
+
+
+def _mode4(vel, q, wav, src, data, par):
+    """pfwi.py:121-251: passive modelling (inv False) or source inversion
+    (inv True, onlysrc True) through lstric; passive FWI (onlysrc False)
+    is pfwic."""
+    v = np.asarray(vel).flatten(order="F").astype(np.float32)
+    qq = np.asarray(q).flatten(order="F").astype(np.float32)
+    w = np.asarray(wav).flatten(order="F").astype(np.float32)
+    if par["inv"]:
+        if not par["onlysrc"]:
+            raise NotImplementedError("passive-source FWI (pfwi mode=4, pfwi.c:1507) is not built")
+        par["inv"] = 1
+        d = np.asarray(data).flatten(order="F").astype(np.float32)
+        s = lstric(v, qq, w, d, pararray(par))
+        s = s.reshape(par["nz"], par["nx"], par["nt"], par["ns"], order="F")
+        return [], None, None, s, []
+    s = np.asarray(src).flatten(order="F").astype(np.float32)
+    d = lstric(v, qq, w, s, pararray(par))
+    d = d.reshape(par["nt"], par["nx"], par["ns"], order="F")
+    return d, [], [], [], []
 
 
 def fillpar(par):

@@ -5,9 +5,11 @@ arguments (``(vel, q, wav, pararray)`` and ``(vel, q, wav, data, pararray)``,
 pfwi.c:85 and :555) and return the same flat float32 arrays
 (``nt*nx*ns`` traces, time fastest, shot slowest; ``nz*nx*niter`` models).
 The quality factor ``q`` is read and ignored, as the acoustic path ignores it
-(pfwi.c:864 sends every call to the acoustic gradient).  The passive-source
-entry points ``lstric`` and ``pfwic`` (mode 4) are not built on this engine
-and raise ``NotImplementedError``.
+(pfwi.c:864 sends every call to the acoustic gradient).  ``lstric``
+(passive mode 4 without velocity update, pfwi.c:1031) takes
+``(vel, q, wav, datasrc, pararray)`` and returns the data (``inv`` = 0) or
+the inverted source field (``inv`` = 1); ``pfwic`` (passive FWI,
+pfwi.c:1507) is not built on this engine and raises ``NotImplementedError``.
 """
 from __future__ import annotations
 
@@ -54,8 +56,33 @@ def fwic(vel, q, wav, data, pararray):
     return vinv
 
 
-def lstric(*args, **kwargs):
-    raise NotImplementedError("passive least-squares TRI (pfwi mode=4, pfwi.c:1031) is not built")
+def lstric(vel, q, wav, datasrc, pararray):
+    """Passive least-squares time-reversal imaging (pfwi.c:1031-1444 -> lstri).
+
+    ``pararray[9]`` (inv) = 0: ``datasrc`` is the source field of every shot
+    (nz*nx*nt*ns, z fastest) and the result the data (nt*nx*ns, time
+    fastest).  inv = 1: ``datasrc`` is the data and the result the source
+    field inverted by ``pararray[19]`` (niter) conjugate-gradient iterations
+    per shot.  ``q`` and ``wav`` are read and ignored (lstri uses neither)."""
+    par = L.f32(pararray).reshape(-1)
+    a = _args(par)
+    inv = int(par[9])
+    vel = L.f32(vel).reshape(-1)
+    ds = L.f32(datasrc).reshape(-1)
+    nm, nd = a.nz * a.nx * a.nt, a.nx * a.nt
+    if vel.size != a.nz * a.nx:
+        raise L.ShapeError(L.PW_ERR_SHAPE, "vel must hold nz*nx values")
+    if inv:
+        if ds.size != nd * a.ns:
+            raise L.ShapeError(L.PW_ERR_SHAPE, "data must hold nt*nx*ns values")
+        out = np.empty(nm * a.ns, np.float32)
+        L.check(L.lib().pw_lstri_invert(a, L.ptr(vel), L.ptr(ds), L.ptr(out), None))
+    else:
+        if ds.size != nm * a.ns:
+            raise L.ShapeError(L.PW_ERR_SHAPE, "src must hold nz*nx*nt*ns values")
+        out = np.empty(nd * a.ns, np.float32)
+        L.check(L.lib().pw_lstri_forward(a, L.ptr(vel), L.ptr(ds), L.ptr(out), None))
+    return out
 
 
 def pfwic(*args, **kwargs):

@@ -24,8 +24,8 @@ import sys
 
 import numpy as np
 
-from models import (BIG3D, BIG3D_BAND, BIG3D_TRI_JSNAP, MID, big3d_velocity, digest, mid_models,
-                    mid_wavelet, pfwi_scale_case)
+from models import (BIG3D, BIG3D_BAND, BIG3D_TRI_JSNAP, LSTRI, MID, big3d_velocity, digest,
+                    lstri_case, mid_models, mid_wavelet, pfwi_scale_case)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
@@ -155,6 +155,40 @@ def make_pfwi_mid(pf, R):
                         **{"par_" + k: np.asarray(v) for k, v in MID.items()})
 
 
+def _lstri_inv_child(out_path):
+    """Runs in a fresh process: the reference's CG keeps its search
+    directions in statics for the life of the process (wave_cgstep.c:28-33),
+    so the inversion golden starts from a process that never ran it."""
+    pf = load("pfwi")
+    vel, src = lstri_case()
+    nz, nx, nt, ns = src.shape
+    q = np.full(vel.shape, 1e4, np.float32)
+    wav = np.zeros(nt, np.float32)
+    par = dict(LSTRI, inv=False)
+    data = quiet(pf.pfwi, vel, q, wav, src, mode=4, par=dict(par))[0]
+    par = dict(LSTRI, inv=True, onlysrc=True, onlyvel=False)
+    srcinv = quiet(pf.pfwi, vel, q, wav, src, data=data, mode=4, par=dict(par))[3]
+    np.savez(out_path, data=data, srcinv=srcinv)
+
+
+def make_lstri():
+    """pfwi mode 4 (lstric, pfwi.c:1031): modelling from a distributed source
+    field (inv = 0) and least-squares time-reversal source inversion by
+    conjugate gradients (inv = 1, niter 6), 20 x 24, 2 shots, nt 200."""
+    import subprocess
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "lstri.npz")
+        code = ("import sys; sys.path.insert(0, %r); import make_golden as M; "
+                "M._lstri_inv_child(%r)" % (HERE, path))
+        subprocess.run([sys.executable, "-c", code], check=True, env=dict(os.environ))
+        with np.load(path) as z:
+            data, srcinv = z["data"], z["srcinv"]
+    vel, src = lstri_case()
+    np.savez_compressed(os.path.join(HERE, "lstri.npz"), vel=vel, src_digest=digest(src),
+                        data=data, srcinv=srcinv)
+
+
 class _Recorder:
     """Stands in for an extension module: records each call's arguments and
     returns the real module's result."""
@@ -246,7 +280,8 @@ def main(names=()):
     R = refdrv()
     R.refdrv_forward.argtypes = [np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")] * 5
     extra = {"afd3d_big": lambda: make_afd3d_big(a3, R), "pfwi_scale": lambda: make_pfwi_scale(R),
-             "pfwi_mid": lambda: make_pfwi_mid(pf, R), "dropin": make_dropin}
+             "pfwi_mid": lambda: make_pfwi_mid(pf, R), "dropin": make_dropin,
+             "lstri": make_lstri}
     if names:
         for n in names:
             extra[n]()

@@ -106,3 +106,29 @@ def mid_wavelet(nt):
     t = np.arange(nt) * 0.001 - 0.12
     a = (np.pi * 10.0 * t) ** 2
     return (1e6 * (1 - 2 * a) * np.exp(-a)).astype(np.float32)
+
+
+# ---- passive mode 4 (lstric): distributed sources, 24 x 32, 2 shots -------
+LSTRI = dict(nz=20, nx=24, dz=0.01, dx=0.01, oz=0.0, ox=0.0, nt=200, dt=0.001, ot=0.0, ns=2,
+             ds=0.1, os=0.05, nb=20, coef=0.005, f0=15.0, acqui_type=1, interval=1, niter=6)
+
+
+def lstri_case():
+    """Velocity (nz, nx) and the source field src (nz, nx, nt, ns) of the
+    pfwi mode-4 fixtures: per shot three point sources carrying seeded,
+    delayed 15 Hz Ricker pulses of amplitude 1e3 (the demos scale theirs by
+    1e6, demos/test_pfwi_vel2d.py)."""
+    p = LSTRI
+    rng = np.random.default_rng(9)
+    nz, nx, nt, ns = p["nz"], p["nx"], p["nt"], p["ns"]
+    z = np.arange(nz, dtype=np.float32)[:, None]
+    vel = (1.8 + 0.6 * z / nz + 0.1 * rng.random((nz, nx))).astype(np.float32)
+    t = np.arange(nt) * p["dt"]
+    src = np.zeros((nz, nx, nt, ns), np.float32)
+    for s in range(ns):
+        for _ in range(3):
+            iz, ix = int(rng.integers(5, nz - 3)), int(rng.integers(3, nx - 3))
+            t0 = float(rng.uniform(0.03, 0.1))
+            a = (np.pi * 15.0 * (t - t0)) ** 2
+            src[iz, ix, :, s] += (1e3 * (1 - 2 * a) * np.exp(-a)).astype(np.float32)
+    return vel, src

@@ -187,5 +187,6 @@ def test_pfwi_errors(cuda_lib):
                os=0.1, nb=10, coef=0.005, f0=10, acqui_type=1, interval=1, niter=1)
     with pytest.raises(ValueError):  # 2.0 * 0.01 / 0.01 > 0.555
         pw.pfwi(vel, q, np.zeros(50, np.float32), None, mode=1, par=par)
-    with pytest.raises(NotImplementedError):
-        pw.pfwi(vel, q, np.zeros(50, np.float32), None, mode=4, par=dict(par, inv=True))
+    with pytest.raises(NotImplementedError):  # passive FWI (pfwic)
+        pw.pfwi(vel, q, np.zeros(50, np.float32), None, mode=4,
+                par=dict(par, inv=True, onlysrc=False))
