@@ -53,6 +53,7 @@ def parse():
                         "batch2d: uneven 2-D forward shots in one batch; c1: one 2-D shot; "
                         "fwi3d: 3-D FWI gradients/s; lstri: pfwi mode 4 source inversion")
     p.add_argument("--lstri-niter", type=int, default=30, help="lstri: CG iterations per shot")
+    p.add_argument("--lstri-nt", type=int, default=3001, help="lstri: time samples")
     p.add_argument("--fwi3d-nt", type=int, default=2500, help="fwi3d: time samples")
     p.add_argument("--fwi3d-shots", type=int, default=16, help="fwi3d: shots per gradient")
     p.add_argument("--shots", type=int, default=32, help="fwi2d: shots per gradient")
@@ -1106,21 +1107,21 @@ LS_NZ, LS_NX, LS_DZ, LS_DX, LS_NT, LS_DT, LS_NB, LS_COEF, LS_NS = \
     130, 334, 0.008, 0.012, 3001, 0.001, 60, 0.005, 3
 
 
-def lstri_par(niter, ns=LS_NS):
-    return dict(nz=LS_NZ, nx=LS_NX, dz=LS_DZ, dx=LS_DX, oz=0, ox=0, nt=LS_NT, dt=LS_DT, ot=0,
+def lstri_par(niter, ns=LS_NS, nt=LS_NT):
+    return dict(nz=LS_NZ, nx=LS_NX, dz=LS_DZ, dx=LS_DX, oz=0, ox=0, nt=nt, dt=LS_DT, ot=0,
                 ns=ns, ds=0.1, os=0.0, nb=LS_NB, coef=LS_COEF, f0=10, acqui_type=1, interval=1,
                 niter=niter)
 
 
-def lstri_case(seed, ns=LS_NS):
+def lstri_case(seed, ns=LS_NS, nt=LS_NT):
     """Velocity 1.8 -> 3.0 km/s with depth plus 0.2 seeded noise; per shot
     three buried point sources carrying 10 Hz Ricker pulses of amplitude 1e6
     at seeded delays (the demos' source scale)."""
     rng = np.random.default_rng(seed)
     z = np.arange(LS_NZ, dtype=np.float32)[:, None]
     vel = (1.8 + 1.2 * z / LS_NZ + 0.2 * rng.random((LS_NZ, LS_NX))).astype(np.float32)
-    src = np.zeros((ns, LS_NT, LS_NX, LS_NZ), np.float32)  # [ns][nt][nx][nz]
-    t = np.arange(LS_NT) * LS_DT
+    src = np.zeros((ns, nt, LS_NX, LS_NZ), np.float32)  # [ns][nt][nx][nz]
+    t = np.arange(nt) * LS_DT
     for s in range(ns):
         for _ in range(3):
             iz, ix = int(rng.integers(60, 125)), int(rng.integers(20, LS_NX - 20))
@@ -1167,10 +1168,10 @@ def _ls_cpu(workers):
 
 
 def run_lstri(args, world, rank, local):
-    niter = args.lstri_niter
+    niter, nt = args.lstri_niter, args.lstri_nt
     pad = (LS_NZ + 2 * LS_NB) * (LS_NX + 2 * LS_NB)
     cfg = {"workload": f"pfwi mode 4 LS-TRI source inversion {LS_NZ}x{LS_NX} dz=8m dx=12m "
-                       f"nt={LS_NT} nb={LS_NB} shots={LS_NS} CG iterations={niter}",
+                       f"nt={nt} nb={LS_NB} shots={LS_NS} CG iterations={niter}",
            "padded_cells": pad}
     metric = "Gpt-updates/s (2-D time-reversal operator, LS-TRI inversion)"
     if args.impl == "reference":
@@ -1205,11 +1206,11 @@ def run_lstri(args, world, rank, local):
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    vel, src = lstri_case(7 + rank)
-    par = lstri_par(niter)
+    vel, src = lstri_case(7 + rank, nt=nt)
+    par = lstri_par(niter, nt=nt)
     v_d = torch.from_numpy(np.ascontiguousarray(vel.T)).cuda()
     s_d = torch.from_numpy(src).cuda()
-    d_d = torch.empty((LS_NS, LS_NX, LS_NT), device="cuda")
+    d_d = torch.empty((LS_NS, LS_NX, nt), device="cuda")
     lstri.lstri_forward_torch(v_d, s_d, d_d, par)  # the observed data
     inv_d = torch.empty_like(s_d)
     del s_d
@@ -1234,7 +1235,7 @@ def run_lstri(args, world, rank, local):
     torch.cuda.synchronize()
     clocks = clk.stop()
     ms = max_over_ranks(e0.elapsed_time(e1), world)
-    updates = pad * LS_NT * 2 * niter * LS_NS  # adjoint + modelling per iteration
+    updates = pad * nt * 2 * niter * LS_NS  # adjoint + modelling per iteration
     # one modelling operator alone, timed on the device (resident launch)
     fwd_ms = []
     scratch = torch.empty_like(d_d[0])
@@ -1246,7 +1247,7 @@ def run_lstri(args, world, rank, local):
     # (Laplacian 30, update 3, two sponge products, injection 2)
     sm_clk = (clocks or {}).get("sm_mhz") or 1965.0
     cluster_flops = 16 * 128 * sm_clk * 1e6
-    op_flops = 40.0 * pad * LS_NT
+    op_flops = 40.0 * pad * nt
     # end to end through the drop-in module: host data in, host source field out
     e2e = None
     if not args.no_e2e:
@@ -1254,7 +1255,7 @@ def run_lstri(args, world, rank, local):
         arr = pararray(fillpar(dict(par, inv=1)))
         q = np.full(LS_NZ * LS_NX, 1e4, np.float32)
         t0 = time.perf_counter()
-        out = pfwicfun.lstric(vel.flatten(order="F"), q, np.zeros(LS_NT, np.float32), dh, arr)
+        out = pfwicfun.lstric(vel.flatten(order="F"), q, np.zeros(nt, np.float32), dh, arr)
         wall = time.perf_counter() - t0
         e2e = {"value": updates / wall / 1e9, "unit": "Gpt/s",
                "h2d_bytes_per_step": int(dh.nbytes + vel.nbytes),
@@ -1267,7 +1268,7 @@ def run_lstri(args, world, rank, local):
                "sample": f"one lstric modelling call (inv 0, one shot, nt={LS_NT}) per process, "
                          f"{workers} single-threaded processes"}
     peak, peak_kind = peaks()
-    src_bytes = 4.0 * LS_NZ * LS_NX * LS_NT  # the modelling operator reads the source field
+    src_bytes = 4.0 * LS_NZ * LS_NX * nt  # the modelling operator reads the source field
     if rank == 0:
         print(json.dumps({
             "metric": metric, "value": job_rate(updates, args.steps, world, ms) / 1e9,

@@ -143,7 +143,8 @@ def check(rc: int):
 
 
 def ptr(a):
-    """Raw address of a C-contiguous numpy array or a CUDA torch tensor."""
+    """Raw address of a C-contiguous numpy array or a CUDA torch tensor.
+    No reference is kept: the caller holds the array for the whole call."""
     if a is None:
         return None
     if isinstance(a, np.ndarray):

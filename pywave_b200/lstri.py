@@ -62,7 +62,8 @@ def lstri_forward(vel, src, par):
     s = np.asarray(src, np.float32).reshape(a.nz, a.nx, a.nt, a.ns)
     s = np.ascontiguousarray(s.transpose(3, 2, 1, 0))
     d = np.empty((a.ns, a.nx, a.nt), np.float32)
-    L.check(L.lib().pw_lstri_forward(a, L.ptr(_vel(vel)), L.ptr(s), L.ptr(d), None))
+    v = _vel(vel)  # held here: ptr() keeps no reference
+    L.check(L.lib().pw_lstri_forward(a, L.ptr(v), L.ptr(s), L.ptr(d), None))
     return d.transpose(2, 1, 0)
 
 
@@ -73,7 +74,8 @@ def lstri_invert(vel, data, par):
     d = np.asarray(data, np.float32).reshape(a.nt, a.nx, a.ns)
     d = np.ascontiguousarray(d.transpose(2, 1, 0))
     s = np.empty((a.ns, a.nt, a.nx, a.nz), np.float32)
-    L.check(L.lib().pw_lstri_invert(a, L.ptr(_vel(vel)), L.ptr(d), L.ptr(s), None))
+    v = _vel(vel)
+    L.check(L.lib().pw_lstri_invert(a, L.ptr(v), L.ptr(d), L.ptr(s), None))
     return s.transpose(3, 2, 1, 0)
 
 
