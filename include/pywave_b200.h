@@ -178,6 +178,16 @@ int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const flo
                      const float *dobs, const float *weight, float *grad, double *misfit,
                      int ckpt_k, void *stream);
 
+/* The same gradient with distributed sources instead of the point source
+ * and wavelet (pfwi's passive mode 4 with velocity update): gradient_pas_av
+ * (wave_fwigradient.c:667-870, set up by gradient_pas_init :528-663 as pfwic
+ * does: velocity only, source weight 1, no multiscale filter).  Each
+ * forward step adds src[shot][it][ix][iz] to the term of the interior
+ * cell (ix, iz).  src [ns][nt][nx][nz]; the other arguments as above. */
+int pw_pfwi_gradient_passive(const pw_fwi_args *a, int mode, const float *vel, const float *src,
+                             const float *dobs, const float *weight, float *grad, double *misfit,
+                             int ckpt_k, void *stream);
+
 /* Checkpoint plan of the calling thread's last PW_GRAD_EXACT gradient: the
  * interval k, the shots per batch, the device bytes the call held and the
  * recompute factor (forward steps run / nt; 1 = nothing recomputed).  The
@@ -239,6 +249,13 @@ int pw_gradient_postprocess(int nz, int nx, int rect, int waterz, float *grad, f
  *   iters_done number of completed iterations. */
 int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav, const float *dobs,
            float *vinv, int *iters_done, void *stream);
+
+/* Passive-source FWI as pfwic runs it (pywave/src/pfwi.c:1507-2036 -> pfwi,
+ * wave_fwi.c:212-322): pw_fwi's optimiser with gradient_pas_av on the
+ * source fields src [ns][nt][nx][nz] and the line-search step reset to 1
+ * every 5 iterations (optpar->repeat).  vinv and iters_done as pw_fwi. */
+int pw_pfwi_passive(const pw_fwi_args *a, const float *vel0, const float *src, const float *dobs,
+                    float *vinv, int *iters_done, void *stream);
 
 /* ---------------------------------------------- pfwi mode 4: LS-TRI --- */
 

@@ -78,6 +78,11 @@ def lib():
             f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 2 + [C.c_int]
                           + geo + [rp, rp, rp, rp, rp])
             f.restype = real
+            f = getattr(L, "or_pfwi_gradient_pas_" + sfx)
+            f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 2 + [C.c_int]
+                          + [C.c_int, C.c_int, _i32p, _i32p, _i32p, C.c_int, C.c_int]
+                          + [rp, rp, rp, rp, rp])
+            f.restype = real
             f = getattr(L, "or_pfwi_gradient_exact_" + sfx)
             f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 2 + geo
                           + [rp, rp, rp, C.c_void_p, rp])
@@ -286,6 +291,25 @@ def pfwi_gradient_ref(vel, wav, dobs, nb, coef, dz, dx, dt, geo, ns, interval=1,
     f = getattr(lib(), "or_pfwi_gradient_ref_" + precision)(
         nz, nx, nb, dz, dx, nt, dt, coef, interval, *_geo_args(geo, ns), v, w,
         _dobs_flat(dobs, R), np.ascontiguousarray(np.asarray(weight, np.float32).astype(R)), g)
+    return g.reshape(nz, nx, order="F"), float(f)
+
+
+def pfwi_gradient_pas(vel, src, dobs, nb, coef, dz, dx, dt, geo, ns, nt, interval=1,
+                      weight=None, precision="f32"):
+    """gradient_pas_av (pfwic's passive gradient) before scaling/smoothing;
+    src (nz, nx, nt, ns) source fields, dobs (nt, nr, ns).  Returns
+    (grad (nz, nx), fcost)."""
+    R = np.float32 if precision == "f32" else np.float64
+    nz, nx = vel.shape
+    if weight is None:
+        weight = residual_weights(nt, geo["nr"])
+    v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F").astype(R))
+    sv = np.ascontiguousarray(np.asarray(src, np.float32).flatten(order="F").astype(R))
+    g = np.zeros(nz * nx, R)
+    f = getattr(lib(), "or_pfwi_gradient_pas_" + precision)(
+        nz, nx, nb, dz, dx, nt, dt, coef, interval, ns, geo["nr"], geo["r0v"], geo["r02"],
+        geo["nr2"], geo["drv"], geo["rz"], v, sv, _dobs_flat(dobs, R),
+        np.ascontiguousarray(np.asarray(weight, np.float32).astype(R)), g)
     return g.reshape(nz, nx, order="F"), float(f)
 
 

@@ -241,15 +241,29 @@ static void SFX(pf_source_map)(int sx, int sz, int pnx, int pnz, REAL *rr)
 /* One leapfrog step of the pfwi scheme: p2 = 2 p1 - p0 + v^2 dt^2 term
  * (wave_fwimodeling.c:92-96), then rotate and sponge p0 and p1
  * (:99-103).  Arrays rotate through the three pointers. */
-static void SFX(pf_update)(REAL **p0, REAL **p1, REAL **p2, const REAL *vp, const REAL *term,
-                           REAL dt2, const REAL *bc, int pnx, int pnz, int nb)
+static void SFX(pf_update_in)(REAL **p0, REAL **p1, REAL **p2, const REAL *vp, const REAL *term,
+                              REAL dt2, const REAL *bc, int pnx, int pnz, int nb, int inner)
 {
     size_t np = (size_t)pnx * pnz;
-    for (size_t j = 0; j < np; j++)
-        (*p2)[j] = 2 * (*p1)[j] - (*p0)[j] + vp[j] * vp[j] * dt2 * term[j];
+    if (inner) {  /* gradient_pas_av (wave_fwigradient.c:740-745): [4, pad-4) only */
+        for (int ix = 4; ix < pnx - 4; ix++)
+            for (int iz = 4; iz < pnz - 4; iz++) {
+                size_t j = (size_t)ix * pnz + iz;
+                (*p2)[j] = 2 * (*p1)[j] - (*p0)[j] + vp[j] * vp[j] * dt2 * term[j];
+            }
+    } else {
+        for (size_t j = 0; j < np; j++)
+            (*p2)[j] = 2 * (*p1)[j] - (*p0)[j] + vp[j] * vp[j] * dt2 * term[j];
+    }
     REAL *t = *p0; *p0 = *p1; *p1 = *p2; *p2 = t;
     SFX(pf_apply_sponge)(*p0, bc, pnx, pnz, nb);
     SFX(pf_apply_sponge)(*p1, bc, pnx, pnz, nb);
+}
+
+static void SFX(pf_update)(REAL **p0, REAL **p1, REAL **p2, const REAL *vp, const REAL *term,
+                           REAL dt2, const REAL *bc, int pnx, int pnz, int nb)
+{
+    SFX(pf_update_in)(p0, p1, p2, vp, term, dt2, bc, pnx, pnz, nb, 0);
 }
 
 /* forward_modeling_a (wave_fwimodeling.c:21-114).
@@ -295,12 +309,12 @@ void SFX(or_pfwi_forward)(int nz, int nx, int nb, float dz, float dx, int nt, fl
  * scaling and gradient_smooth2 (:244-255).  weight: [nr][nt] residual
  * weights (residual_weighting).  grad: [nx][nz] (zeroed here).  Returns the
  * misfit 0.5*sum((dobs-d)^2), accumulated as the reference does. */
-REAL SFX(or_pfwi_gradient_ref)(int nz, int nx, int nb, float dz, float dx, int nt, float dt,
-                               float coef, int interval,
-                               int ns, const int *sx, int sz, int nr, const int *r0v,
-                               const int *r02, const int *nr2, int drv, int rz,
-                               const REAL *vel, const REAL *wav, const REAL *dobs,
-                               const REAL *weight, REAL *grad)
+static REAL SFX(pf_gradient_core)(int nz, int nx, int nb, float dz, float dx, int nt, float dt,
+                                  float coef, int interval,
+                                  int ns, const int *sx, int sz, int nr, const int *r0v,
+                                  const int *r02, const int *nr2, int drv, int rz,
+                                  const REAL *vel, const REAL *wav, const REAL *dsrc,
+                                  const REAL *dobs, const REAL *weight, REAL *grad)
 {
     const int pnz = nz + 2 * nb, pnx = nx + 2 * nb;
     const size_t np = (size_t)pnz * pnx, nzx = (size_t)nz * nx;
@@ -326,7 +340,7 @@ REAL SFX(or_pfwi_gradient_ref)(int nz, int nx, int nb, float dz, float dx, int n
         REAL *p0 = a, *p1 = b, *p2 = c;
         memset(p0, 0, np * sizeof(REAL)); memset(p1, 0, np * sizeof(REAL)); memset(p2, 0, np * sizeof(REAL));
         memset(pp, 0, (size_t)nr * nt * sizeof(REAL));
-        SFX(pf_source_map)(sx[is], sz, pnx, pnz, rr);
+        if (!dsrc) SFX(pf_source_map)(sx[is], sz, pnx, pnz, rr);
         int wit = 0;
         for (int it = 0; it < nt; it++) {
             for (int ir = 0; ir < nr2[is]; ir++) {
@@ -340,8 +354,15 @@ REAL SFX(or_pfwi_gradient_ref)(int nz, int nx, int nb, float dz, float dx, int n
                 wit++;
             }
             SFX(pf_laplace)(p1, term, pnx, pnz, dx2, dz2);
-            for (size_t j = 0; j < np; j++) term[j] += rr[j] * wav[it];
-            SFX(pf_update)(&p0, &p1, &p2, vp, term, dt2, bc, pnx, pnz, nb);
+            if (dsrc) {  /* gradient_pas_av (wave_fwigradient.c:732-737) */
+                const REAL *w3 = dsrc + ((size_t)is * nt + it) * nzx;
+                for (int ix = 0; ix < nx; ix++)
+                    for (int iz = 0; iz < nz; iz++)
+                        term[(size_t)(ix + nb) * pnz + iz + nb] += w3[(size_t)ix * nz + iz];
+            } else {
+                for (size_t j = 0; j < np; j++) term[j] += rr[j] * wav[it];
+            }
+            SFX(pf_update_in)(&p0, &p1, &p2, vp, term, dt2, bc, pnx, pnz, nb, dsrc != NULL);
         }
         wit--;
         const REAL *dd = dobs + (size_t)is * nr * nt;
@@ -360,7 +381,13 @@ REAL SFX(or_pfwi_gradient_ref)(int nz, int nx, int nb, float dz, float dx, int n
                 int rx = r0v[is] + ir * drv;
                 term[(size_t)rx * pnz + rz] += pp[(size_t)(r02[is] + ir) * nt + it];
             }
-            {
+            if (dsrc) {  /* gradient_pas_av (:812-817): [4, pad-4) only */
+                for (int ix = 4; ix < pnx - 4; ix++)
+                    for (int iz = 4; iz < pnz - 4; iz++) {
+                        size_t j = (size_t)ix * pnz + iz;
+                        p2[j] = 2 * p1[j] - p0[j] + vp[j] * vp[j] * dt2 * term[j];
+                    }
+            } else {
                 size_t npp = np;
                 for (size_t j = 0; j < npp; j++)
                     p2[j] = 2 * p1[j] - p0[j] + vp[j] * vp[j] * dt2 * term[j];
@@ -388,6 +415,33 @@ REAL SFX(or_pfwi_gradient_ref)(int nz, int nx, int nb, float dz, float dx, int n
     }
     free(vp); free(rr); free(a); free(b); free(c); free(term); free(bc); free(wave); free(pp);
     return fcost;
+}
+
+REAL SFX(or_pfwi_gradient_ref)(int nz, int nx, int nb, float dz, float dx, int nt, float dt,
+                               float coef, int interval,
+                               int ns, const int *sx, int sz, int nr, const int *r0v,
+                               const int *r02, const int *nr2, int drv, int rz,
+                               const REAL *vel, const REAL *wav, const REAL *dobs,
+                               const REAL *weight, REAL *grad)
+{
+    return SFX(pf_gradient_core)(nz, nx, nb, dz, dx, nt, dt, coef, interval, ns, sx, sz, nr, r0v,
+                                 r02, nr2, drv, rz, vel, wav, NULL, dobs, weight, grad);
+}
+
+/* gradient_pas_av (wave_fwigradient.c:667-852) as pfwic sets it up
+ * (gradient_pas_init :528-663 with onlyvel: source weight gwt = 1, no
+ * multiscale filter): gradient_av with the source field dsrc
+ * [ns][nt][nx][nz] added to the interior's term and the update restricted to
+ * [4, pad-4).  Raw, before the scaling and gradient_smooth2b (waterz =
+ * waterzb = 0, the same smoothing as gradient_smooth2 with waterz 0). */
+REAL SFX(or_pfwi_gradient_pas)(int nz, int nx, int nb, float dz, float dx, int nt, float dt,
+                               float coef, int interval, int ns, int nr, const int *r0v,
+                               const int *r02, const int *nr2, int drv, int rz,
+                               const REAL *vel, const REAL *dsrc, const REAL *dobs,
+                               const REAL *weight, REAL *grad)
+{
+    return SFX(pf_gradient_core)(nz, nx, nb, dz, dx, nt, dt, coef, interval, ns, NULL, 0, nr, r0v,
+                                 r02, nr2, drv, rz, vel, NULL, dsrc, dobs, weight, grad);
 }
 
 /* Exact discrete adjoint of the pfwi forward scheme.

@@ -3,8 +3,9 @@
  * Test infrastructure only: compiled by oracle/Makefile together with the
  * UNMODIFIED reference sources (pywave/src/*.c, read in place) into
  * oracle/_ref/libpwref.so.  It exposes entry points the reference's Python
- * glue never returns -- the raw gradient of gradient_av, the unscaled Ricker
- * table of fdm2d -- so the oracle restatement can be pinned against them.
+ * glue never returns -- the raw gradients of gradient_av and gradient_pas_av,
+ * the unscaled Ricker table of fdm2d -- so the oracle restatement can be
+ * pinned against them.
  *
  * Parameter set-up mirrors pywave/src/pfwi.c:743-860 (fwic) and
  * pfwi.c:260-300 (forward_modeling_ac).
@@ -111,4 +112,44 @@ void refdrv_gradient(const float *par, float *vel, float *q, float *wav,
     fwipar->rectz = rect;
     gradient_init(d, soupar, acpar, array, fwipar, false);
     gradient_av(array->vv, fcost, grad);
+}
+
+/* gradient_pas_init + one gradient_pas_av call (wave_fwigradient.c:528-870)
+ * as pfwic sets them up (pfwi.c:1780-1890: velocity only, so the source
+ * weight is 1 and no source inversion runs), with the caller's smoothing
+ * radius.  src: [ns][nt][nx][nz] source fields.  The output includes the
+ * first-call 0.1/max|g| scaling. */
+void refdrv_gradient_pas(const float *par, float *vel, float *q, float *wav, float *dobs,
+                         float *src, int rect, float *grad, float *fcost)
+{
+    np_sou soupar = (np_sou)np_alloc(1, sizeof(*soupar));
+    np_acqui acpar = (np_acqui)np_alloc(1, sizeof(*acpar));
+    np_vec array = (np_vec)np_alloc(1, sizeof(*array));
+    np_fwi fwipar = (np_fwi)np_alloc(1, sizeof(*fwipar));
+    fill_acpar(acpar, soupar, par);
+    np_pas paspar = passive_init(acpar);
+    paspar->inv = true;
+    paspar->onlysrc = false;
+    paspar->onlyvel = true;
+    preparation(vel, q, wav, acpar, soupar, array);
+    const int nz = acpar->nz, nx = acpar->nx, nt = acpar->nt, ns = acpar->ns;
+    float ***d = np_floatalloc3(nt, nx, ns);
+    memcpy(d[0][0], dobs, sizeof(float) * nt * nx * ns);
+    float ****w = np_floatalloc4(nz, nx, nt, ns);
+    memcpy(w[0][0][0], src, sizeof(float) * (size_t)nz * nx * nt * ns);
+    fwipar->onlygrad = false;
+    fwipar->grad_type = 1;
+    fwipar->misfit_type = 1;
+    fwipar->opt_type = 1;
+    fwipar->wt1 = acpar->t0;
+    fwipar->wt2 = acpar->t0 + (acpar->nt - 1) * acpar->dt;
+    fwipar->woff1 = acpar->r0;
+    fwipar->woff2 = acpar->r0 + (acpar->nr - 1) * acpar->dr;
+    fwipar->oreo = false;
+    fwipar->waterz = 0;
+    fwipar->waterzb = 0;
+    fwipar->rectx = rect;
+    fwipar->rectz = rect;
+    gradient_pas_init(d, w, NULL, soupar, acpar, array, fwipar, paspar, false);
+    gradient_pas_av(array->vv, fcost, grad);
 }

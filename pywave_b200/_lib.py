@@ -95,6 +95,10 @@ _SIGS = {
     "pw_pfwi3d_forward": (C.c_int, [C.POINTER(Fwi3dArgs), _vp, _vp, _vp, _vp]),
     "pw_pfwi3d_gradient": (C.c_int, [C.POINTER(Fwi3dArgs), _vp, _vp, _vp, _vp, _vp, _vp,
                                      C.c_int, _vp]),
+    "pw_pfwi_gradient_passive": (C.c_int, [C.POINTER(FwiArgs), C.c_int, _vp, _vp, _vp, _vp, _vp,
+                                           C.POINTER(C.c_double), C.c_int, _vp]),
+    "pw_pfwi_passive": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp, C.POINTER(C.c_int),
+                                  _vp]),
     "pw_timerev": (C.c_int, [C.POINTER(FwiArgs), C.c_int, _vp, _vp, _vp, _vp]),
     "pw_lstri_forward": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp]),
     "pw_lstri_invert": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp]),

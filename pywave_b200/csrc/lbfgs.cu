@@ -115,9 +115,12 @@ struct Buffers {
 using namespace pw;
 using namespace pw::lb;
 
-extern "C" int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav, const float *dobs,
-                      float *vinv, int *iters_done, void *stream) {
-  PW_CHECK(a && vel0 && wav && dobs && vinv, PW_ERR_VALUE, "null argument");
+// fwi (wave_fwi.c:24-119; wav: point sources, gradient_av) and pfwi
+// (wave_fwi.c:212-322; dsrc: a source field per shot, gradient_pas_av, and
+// alpha reset to 1 every `repeat` iterations, optpar->repeat = 5 in pfwic)
+static int fwi_impl(const pw_fwi_args *a, const float *vel0, const float *wav, const float *dsrc,
+                    const float *dobs, float *vinv, int *iters_done, int repeat, void *stream) {
+  PW_CHECK(a && vel0 && (wav || dsrc) && dobs && vinv, PW_ERR_VALUE, "null argument");
   cudaStream_t st = (cudaStream_t)stream;
   const bool host = (a->flags & PW_HOST_PTRS) != 0;
   const long long n = (long long)a->nz * a->nx;
@@ -126,7 +129,7 @@ extern "C" int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav,
   const int npair = 20, nls = 20, rect = 3, waterz = 0;
   const float c1 = 1e-4f, c2 = 0.9f, factor = 10.f, v1 = 0.f, v2 = 10.f, conv_error = 0.01f;
   Buffers B;
-  float *x, *g, *d, *xk, *sk, *yk, *q, *wav_d = nullptr, *dobs_d = nullptr;
+  float *x, *g, *d, *xk, *sk, *yk, *q, *wav_d = nullptr, *dobs_d = nullptr, *dsrc_d = nullptr;
   double *acc;
   PW_TRY(B.alloc(&x, n));
   PW_TRY(B.alloc(&g, n));
@@ -137,24 +140,38 @@ extern "C" int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav,
   PW_TRY(B.alloc(&yk, n * npair));
   PW_TRY(B.alloc(&acc, DOT_BLOCKS + 1));
   const long long nd = (long long)a->ns * a->nx * a->nt;
+  const long long nsf = (long long)a->ns * n * a->nt;  // passive source fields
   if (host) {
-    PW_TRY(B.alloc(&wav_d, a->nt));
+    if (wav) {
+      PW_TRY(B.alloc(&wav_d, a->nt));
+      PW_CUDA(cudaMemcpyAsync(wav_d, wav, a->nt * 4, cudaMemcpyHostToDevice, st));
+    }
+    if (dsrc) {
+      PW_TRY(B.alloc(&dsrc_d, nsf));
+      PW_CUDA(cudaMemcpyAsync(dsrc_d, dsrc, (size_t)nsf * 4, cudaMemcpyHostToDevice, st));
+    }
     PW_TRY(B.alloc(&dobs_d, nd));
-    PW_CUDA(cudaMemcpyAsync(wav_d, wav, a->nt * 4, cudaMemcpyHostToDevice, st));
     PW_CUDA(cudaMemcpyAsync(dobs_d, dobs, nd * 4, cudaMemcpyHostToDevice, st));
   }
   PW_TRY(to_device(x, vel0, n * 4, host, st));
   pw_fwi_args ga = *a;
   ga.flags &= ~PW_HOST_PTRS;
   const float *gwav = host ? wav_d : wav, *gdobs = host ? dobs_d : dobs;
+  const float *gdsrc = host ? dsrc_d : dsrc;
   float scaling = 0.f;  // gradient_av's static: set by the first gradient
   float *dsc;
   PW_TRY(B.alloc(&dsc, 1));
   Dev D{st, n, acc};
-  // gradient_av + gradient_smooth2 (wave_fwigradient.c:93-255)
+  // gradient_av + gradient_smooth2 (wave_fwigradient.c:93-255), or
+  // gradient_pas_av + gradient_smooth2b (:667-870; waterz = waterzb = 0
+  // there, so the two smoothings coincide)
   auto gradient = [&](float *xv, float *fcost) -> int {
     double J = 0.0;
-    PW_TRY(pw_pfwi_gradient(&ga, PW_GRAD_REFERENCE, xv, gwav, gdobs, nullptr, g, &J, 0, st));
+    if (gdsrc)
+      PW_TRY(pw_pfwi_gradient_passive(&ga, PW_GRAD_REFERENCE, xv, gdsrc, gdobs, nullptr, g, &J, 0,
+                                      st));
+    else
+      PW_TRY(pw_pfwi_gradient(&ga, PW_GRAD_REFERENCE, xv, gwav, gdobs, nullptr, g, &J, 0, st));
     PW_CUDA(cudaMemcpyAsync(dsc, &scaling, 4, cudaMemcpyHostToDevice, st));
     PW_TRY(pw_gradient_postprocess(a->nz, a->nx, rect, waterz, g, dsc, 0, st));
     PW_CUDA(cudaMemcpyAsync(&scaling, dsc, 4, cudaMemcpyDeviceToHost, st));
@@ -172,6 +189,7 @@ extern "C" int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav,
   if (!host) PW_CUDA(cudaMemsetAsync(vinv, 0, (size_t)n * niter * 4, st));
   else memset(vinv, 0, (size_t)n * niter * 4);
   for (iter = 0; iter < niter; iter++) {
+    if (repeat > 0 && iter % repeat == 0) alpha = 1.f;
     if (iter == 0) {
       PW_TRY(D.axpby(-1.0, g, 0.0, d));
     } else {
@@ -255,4 +273,16 @@ extern "C" int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav,
   PW_CUDA(cudaStreamSynchronize(st));
   if (iters_done) *iters_done = iter;
   return PW_OK;
+}
+
+extern "C" int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav, const float *dobs,
+                      float *vinv, int *iters_done, void *stream) {
+  PW_CHECK(wav != nullptr, PW_ERR_VALUE, "null wavelet");
+  return fwi_impl(a, vel0, wav, nullptr, dobs, vinv, iters_done, 0, stream);
+}
+
+extern "C" int pw_pfwi_passive(const pw_fwi_args *a, const float *vel0, const float *src,
+                               const float *dobs, float *vinv, int *iters_done, void *stream) {
+  PW_CHECK(src != nullptr, PW_ERR_VALUE, "null source field");
+  return fwi_impl(a, vel0, nullptr, src, dobs, vinv, iters_done, 5, stream);
 }

@@ -77,6 +77,9 @@ struct PfArgs {
   const ShotGeo *geo;         // [nshots] (device)
   int rz, drv, nr;
   const float *wav;           // forward: wavelet [nt]
+  const float *dsrc;          // forward, passive sources: field [shot][nt][nx][nz] added to the
+                              // term of every interior cell (replaces the wavelet), or null
+  long long dsrc_stride;      // floats between the shots' source fields
   float *rec;                 // forward: traces [shot][nt][nr] or null
   float *snap;                // forward: interior snapshot for this step [shot][nx][nz] or null
   long long snap_stride;      // floats between shots' snapshots
@@ -110,6 +113,12 @@ __device__ __forceinline__ void cp16(float4 *dst, const float *src, bool valid) 
   const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
   const int n = valid ? 16 : 0;
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(n)
+               : "memory");
+}
+__device__ __forceinline__ void cp4(float *dst, const float *src, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src), "r"(n)
                : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
@@ -190,7 +199,7 @@ __device__ __forceinline__ void div4x2(const float (&tx)[4], const float (&tz)[4
 }
 
 // One pfwi step over a z column segment of ZW float4 marching along x.
-template <int ZW, int P, int MODE>
+template <int ZW, int P, int MODE, bool PAS = false>
 __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
   constexpr int W = ZW + 2;   // curr plane (float4) incl. z halo
   constexpr int NC = P + 10;  // curr planes (x-4..x+4 live, P ahead, 1 slack)
@@ -201,6 +210,7 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
   float4 *s_V = s_prev + NP * ZW;
   float4 *s_t = s_V + NP * ZW;  // ADJ_EXACT: forward term tile
   float4 *s_g = s_t + NP * ZW;  // ADJ_EXACT: this shot's gradient slice
+  float4 *s_d = s_t;            // FWD with passive sources: the step's source field
 
   const int tid = threadIdx.x;
   const int s = blockIdx.x;  // shot of the batch: fastest, so the shots of one x chunk
@@ -256,6 +266,20 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
         cp16(s_t + (j % NP) * ZW + tid, live ? tin + o : tin, live && a.imaging);
         cp16(s_g + (j % NP) * ZW + tid, live ? gs + o : gs, live && a.imaging);
       }
+      if (MODE == FWD && PAS) {
+        // the interior cells' source samples of plane x0 + j (zero elsewhere)
+        const int x = x0 + j;
+        const bool xin = live && x >= a.nb && x < a.nb + a.nx;
+        const float *row = a.dsrc + s * a.dsrc_stride +
+                           ((long long)a.it * a.nx + (xin ? x - a.nb : 0)) * a.nz;
+        float *dst = reinterpret_cast<float *>(s_d + (j % NP) * ZW + tid);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int iz = iz0 + e;
+          const bool ok = xin && iz >= a.nb && iz < a.nb + a.nz;
+          cp4(dst + e, ok ? row + (iz - a.nb) : a.dsrc, ok);
+        }
+      }
     };
     for (int k = 0; k < 8; k++) issue_cur(k);
 #pragma unroll
@@ -309,6 +333,8 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
         const float4 L = pl[ci - 1], R = pl[ci + 1];
         const float4 pv = s_prev[(i % NP) * ZW + tid];
         const float4 V4 = s_V[(i % NP) * ZW + tid];
+        const float4 dv = (MODE == FWD && PAS) ? s_d[(i % NP) * ZW + tid]
+                                               : make_float4(0.f, 0.f, 0.f, 0.f);
         const float bxf = a.bx[x];
         const bool lx_ok = x >= 4 && x < a.pnx - 4;
         const long long o = o_c + (long long)lz * x;
@@ -358,7 +384,14 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
           const int iz = iz0 + e;
           const float cv = el(c, e);
           float t = (lz_ok[e] && lx_ok) ? fadd(qx[e], qz[e]) : 0.f;
-          if (MODE == FWD) {
+          if (MODE == FWD && PAS) {
+            // gradient_pas_av (wave_fwigradient.c:732-737): the interior's source
+            // sample; its update covers the stencil's cells only, so none is
+            // added on the 4-cell rim
+            if (lz_ok[e] && lx_ok && iz >= a.nb && iz < a.nb + a.nz && x >= a.nb &&
+                x < a.nb + a.nx)
+              t = fadd(t, el(dv, e));
+          } else if (MODE == FWD) {
             if (src_here)
               for (int k = 0; k < sg.nsrc; k++)
                 if (sg.scell[k] == ((x << 16) | iz)) t = fadd(t, fmul(sg.sw[k], a.wav[a.it]));
@@ -781,7 +814,8 @@ struct Setup {
   size_t smem;
 };
 
-static int setup(const pw_fwi_args *a, Setup &S) {
+// passive: distributed sources (pfwi mode 4) -- no point source per shot
+static int setup(const pw_fwi_args *a, Setup &S, bool passive = false) {
   PW_CHECK(a != nullptr, PW_ERR_VALUE, "null args");
   S.a = *a;
   PW_CHECK(a->nz >= 1 && a->nx >= 1 && a->nt >= 1 && a->ns >= 1 && a->nb >= 1, PW_ERR_SHAPE,
@@ -838,6 +872,12 @@ static int setup(const pw_fwi_args *a, Setup &S) {
     PW_CHECK(g.r02 >= 0 && g.r02 + g.nr2 <= S.nr && g.r0v >= 0 &&
                  g.r0v + (g.nr2 - 1) * S.drv < S.pnx,
              PW_ERR_SHAPE, "shot %d: receivers outside the grid", is);
+    if (passive) {  // an empty source map
+      g.nsrc = 0;
+      g.sx0 = g.sz0 = 1;
+      g.sx1 = g.sz1 = 0;
+      continue;
+    }
     const int sx = s0_v + is * ds_v;
     PW_CHECK(sx >= 0 && sx < S.pnx && S.sz >= 0 && S.sz < S.pnz, PW_ERR_SHAPE,
              "shot %d: source (x=%d, z=%d) outside the padded grid", is, sx, S.sz);
@@ -865,13 +905,14 @@ static size_t smem_for(int zw, int mode) {
                                                                (PFP + 2) * zw);
 }
 
-template <int ZW, int MODE>
+template <int ZW, int MODE, bool PAS = false>
 static int launch_one(const Setup &S, const PfArgs &p, cudaStream_t st) {
-  const size_t smem = smem_for(ZW, MODE);
+  // the forward step with passive sources adds a ring of source planes
+  const size_t smem = smem_for(ZW, MODE) + (PAS ? (size_t)(PFP + 2) * ZW * sizeof(float4) : 0);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(pf_step_kernel<ZW, PFP, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+    cudaFuncSetAttribute(pf_step_kernel<ZW, PFP, MODE, PAS>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
   // x planes per CTA: long enough to amortise the 8-plane prologue, short
@@ -879,12 +920,14 @@ static int launch_one(const Setup &S, const PfArgs &p, cudaStream_t st) {
   int xch = 128;
   while (xch > 16 && (long long)p.nshots * S.ztiles * ceil_div(S.pnx, xch) < 6LL * S.nsm) xch /= 2;
   const dim3 grid(p.nshots, ceil_div(S.pnx, xch), S.ztiles);
-  pf_step_kernel<ZW, PFP, MODE><<<grid, ZW, smem, st>>>(p, xch);
+  pf_step_kernel<ZW, PFP, MODE, PAS><<<grid, ZW, smem, st>>>(p, xch);
   PW_CUDA(cudaGetLastError());
   return PW_OK;
 }
 
 static int launch(const Setup &S, const PfArgs &p, int mode, cudaStream_t st) {
+  if (mode == FWD && p.dsrc)
+    return S.zw == 64 ? launch_one<64, FWD, true>(S, p, st) : launch_one<128, FWD, true>(S, p, st);
   if (S.zw == 64) {
     if (mode == FWD) return launch_one<64, FWD>(S, p, st);
     if (mode == ADJ_REF) return launch_one<64, ADJ_REF>(S, p, st);
@@ -990,7 +1033,7 @@ static int upload_common(const Setup &S, char *base, size_t o_geo, size_t o_bz, 
                           cudaMemcpyHostToDevice, st));
   PW_CUDA(cudaMemcpyAsync(base + o_bz, S.bz.data(), S.bz.size() * 4, cudaMemcpyHostToDevice, st));
   PW_CUDA(cudaMemcpyAsync(base + o_bx, S.bx.data(), S.bx.size() * 4, cudaMemcpyHostToDevice, st));
-  PW_TRY(to_device(base + o_wav, wav, (size_t)S.a.nt * 4, host, st));
+  if (wav) PW_TRY(to_device(base + o_wav, wav, (size_t)S.a.nt * 4, host, st));
   return PW_OK;
 }
 
@@ -1191,13 +1234,18 @@ static PlanRecord &plan_record() {
   return r;
 }
 
-extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const float *wav,
-                                const float *dobs, const float *weight, float *grad,
-                                double *misfit, int ckpt_k, void *stream) {
+namespace pw {
+namespace pf {
+// The gradient of pw_pfwi_gradient (wav: point sources) and of
+// pw_pfwi_gradient_passive (dsrc: a source field per shot, [ns][nt][nx][nz]).
+static int gradient_impl(const pw_fwi_args *a, int mode, const float *vel, const float *wav,
+                         const float *dsrc, const float *dobs, const float *weight, float *grad,
+                         double *misfit, int ckpt_k, void *stream) {
   cudaStream_t st = (cudaStream_t)stream;
   PW_CHECK(mode == PW_GRAD_REFERENCE || mode == PW_GRAD_EXACT, PW_ERR_VALUE, "bad gradient mode");
+  PW_CHECK(vel && dobs && grad && (wav || dsrc), PW_ERR_VALUE, "null array");
   Setup S;
-  PW_TRY(setup(a, S));
+  PW_TRY(setup(a, S, dsrc != nullptr));
   const bool host = (a->flags & PW_HOST_PTRS) != 0;
   const bool per_shot = (a->flags & PW_PER_SHOT) != 0;
   const int ns = a->ns, nt = a->nt, nr = S.nr, nz = a->nz, nx = a->nx;
@@ -1244,6 +1292,8 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   const size_t o_m2v3 = cv.add(exact ? 0 : nvel * 4);
   const size_t o_mis = cv.add(8 * (1 + RESID_BLOCKS));
   const size_t o_mx = cv.add(16);
+  const size_t nsrcf = (size_t)nvel * nt;  // one shot's source field
+  const size_t o_dsrc = cv.add(dsrc && host ? (size_t)ns * nsrcf * 4 : 0);
   PW_TRY(ws.reserve(cv.total()));
   if (exact) plan_record().bytes = (long long)cv.total();
   char *base = ws.base();
@@ -1258,6 +1308,11 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   }
   PW_TRY(check_vel_cfl(S, d_vel, nvel, st, at<unsigned>(base, o_mx)));
   PW_TRY(upload_common(S, base, o_geo, o_bz, o_bx, o_wav, wav, host, st));
+  const float *d_dsrc = dsrc;
+  if (dsrc && host) {
+    PW_TRY(to_device(base + o_dsrc, dsrc, (size_t)ns * nsrcf * 4, true, st));
+    d_dsrc = at<float>(base, o_dsrc);
+  }
   if (weight) PW_TRY(to_device(base + o_w, weight, (size_t)nr * nt * 4, host, st));
   else PW_CUDA(cudaMemcpyAsync(base + o_w, wts.data(), wts.size() * 4, cudaMemcpyHostToDevice, st));
   {
@@ -1325,6 +1380,8 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
     };
     p.nshots = nb_;
     p.geo = at<ShotGeo>(base, o_geo) + s0;
+    p.dsrc = d_dsrc ? d_dsrc + (size_t)s0 * nsrcf : nullptr;
+    p.dsrc_stride = (long long)nsrcf;
     float *dd = at<float>(base, o_d);
     float *res = at<float>(base, o_res);
     float *ck = at<float>(base, o_ck);
@@ -1447,6 +1504,22 @@ extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel
   PW_CUDA(cudaStreamSynchronize(st));
   timer.finish(launches, launches + 8);
   return PW_OK;
+}
+}  // namespace pf
+}  // namespace pw
+
+extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const float *wav,
+                                const float *dobs, const float *weight, float *grad,
+                                double *misfit, int ckpt_k, void *stream) {
+  PW_CHECK(wav != nullptr, PW_ERR_VALUE, "null wavelet");
+  return gradient_impl(a, mode, vel, wav, nullptr, dobs, weight, grad, misfit, ckpt_k, stream);
+}
+
+extern "C" int pw_pfwi_gradient_passive(const pw_fwi_args *a, int mode, const float *vel,
+                                        const float *src, const float *dobs, const float *weight,
+                                        float *grad, double *misfit, int ckpt_k, void *stream) {
+  PW_CHECK(src != nullptr, PW_ERR_VALUE, "null source field");
+  return gradient_impl(a, mode, vel, nullptr, src, dobs, weight, grad, misfit, ckpt_k, stream);
 }
 
 extern "C" int pw_last_fwi_plan(int *ckpt_k, int *shots_per_batch, long long *bytes,

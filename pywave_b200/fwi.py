@@ -69,6 +69,27 @@ def gradient(vel, wav, dobs, par, mode="exact", ckpt_k=0, per_shot=False, weight
     return g.reshape(a.nz, a.nx, order="F"), J.value
 
 
+def gradient_passive(vel, src, dobs, par, mode="reference", ckpt_k=0, per_shot=False,
+                     weight=None, hbm_budget=0):
+    """The same gradient with distributed sources (pfwi's passive mode 4,
+    gradient_pas_av, wave_fwigradient.c:667-870): src (nz, nx, nt, ns)
+    source fields in place of the point source and wavelet."""
+    flags = L.PW_HOST_PTRS | (L.PW_PER_SHOT if per_shot else 0)
+    a = fwi_args(par, flags, hbm_budget)
+    v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F"))
+    sv = np.ascontiguousarray(np.asarray(src, np.float32).flatten(order="F"))  # [ns][nt][nx][nz]
+    if sv.size != a.nz * a.nx * a.nt * a.ns:
+        raise L.ShapeError(L.PW_ERR_SHAPE, "src must hold nz*nx*nt*ns values")
+    d = _data_flat(dobs)
+    wt = None if weight is None else np.ascontiguousarray(np.asarray(weight, np.float32))
+    g = np.empty(a.nz * a.nx, np.float32)
+    J = ctypes.c_double(0.0)
+    m = L.PW_GRAD_EXACT if mode == "exact" else L.PW_GRAD_REFERENCE
+    L.check(L.lib().pw_pfwi_gradient_passive(a, m, L.ptr(v), L.ptr(sv), L.ptr(d), L.ptr(wt),
+                                             L.ptr(g), ctypes.byref(J), int(ckpt_k), None))
+    return g.reshape(a.nz, a.nx, order="F"), J.value
+
+
 def postprocess(grad, rect=3, waterz=0, scaling=None):
     """gradient_av's tail: triangle smoothing and the (first-call) scale."""
     g = np.ascontiguousarray(np.asarray(grad, np.float32).flatten(order="F"))

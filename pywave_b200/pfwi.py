@@ -1,10 +1,10 @@
 """``pfwi`` and ``fillpar`` with the reference's signatures (pywave/pfwi.py:5, :262).
 
-Modes 1 (modelling), 2 (FWI) and 4 without velocity update (passive
-modelling and least-squares time-reversal source inversion, lstric) run on
-the GPU engine; mode 3 (RTM) does nothing, as in the reference
-(pfwi.py:114-119); mode 4 with velocity update (pfwic) raises
-``NotImplementedError``.  As in the reference only ``par`` is read:
+Modes 1 (modelling), 2 (FWI) and 4 (passive modelling and least-squares
+time-reversal source inversion through lstric; passive FWI with known
+sources through pfwic) run on the GPU engine; mode 3 (RTM) does nothing,
+as in the reference (pfwi.py:114-119).  As in the reference only ``par`` is
+read:
 the keyword arguments after ``mode`` are accepted and ignored
 (pfwi.py:29-61).
 """
@@ -54,14 +54,24 @@ def pfwi(vel, q, wav, src, data=None, mode=1, media=1, inv=0, verb=1, nb=60, coe
 
 def _mode4(vel, q, wav, src, data, par):
     """pfwi.py:121-251: passive modelling (inv False) or source inversion
-    (inv True, onlysrc True) through lstric; passive FWI (onlysrc False)
-    is pfwic."""
+    (inv True, onlysrc True) through lstric; passive FWI (inv True, onlysrc
+    False) through pfwic."""
     v = np.asarray(vel).flatten(order="F").astype(np.float32)
     qq = np.asarray(q).flatten(order="F").astype(np.float32)
     w = np.asarray(wav).flatten(order="F").astype(np.float32)
+    if par["inv"] and not par["onlysrc"]:
+        # pfwi.py:167-210: pfwic on the data followed by the sources; the
+        # wrapper returns the flattened data in the data slot
+        par["inv"] = 1
+        d = np.asarray(data).flatten(order="F").astype(np.float32)
+        s = np.asarray(src).flatten(order="F").astype(np.float32)
+        vinv = pfwic(v, qq, w, np.concatenate([d, s]), pararray(par))
+        vinv = vinv.reshape(par["nz"], par["nx"], par["niter"], order="F")
+        if par["onlyvel"]:
+            return d, vinv, None, None, None
+        # the reference's wrapper leaves grad and mwt unbound here (pfwi.py:205-210)
+        return d, vinv, None, src, None
     if par["inv"]:
-        if not par["onlysrc"]:
-            raise NotImplementedError("passive-source FWI (pfwi mode=4, pfwi.c:1507) is not built")
         par["inv"] = 1
         d = np.asarray(data).flatten(order="F").astype(np.float32)
         s = lstric(v, qq, w, d, pararray(par))

@@ -8,8 +8,9 @@ The quality factor ``q`` is read and ignored, as the acoustic path ignores it
 (pfwi.c:864 sends every call to the acoustic gradient).  ``lstric``
 (passive mode 4 without velocity update, pfwi.c:1031) takes
 ``(vel, q, wav, datasrc, pararray)`` and returns the data (``inv`` = 0) or
-the inverted source field (``inv`` = 1); ``pfwic`` (passive FWI,
-pfwi.c:1507) is not built on this engine and raises ``NotImplementedError``.
+the inverted source field (``inv`` = 1); ``pfwic`` (passive FWI with the
+sources known, pfwi.c:1507) takes the same tuple with ``datasrc`` the data
+followed by the source fields and returns the model after each iteration.
 """
 from __future__ import annotations
 
@@ -85,5 +86,29 @@ def lstric(vel, q, wav, datasrc, pararray):
     return out
 
 
-def pfwic(*args, **kwargs):
-    raise NotImplementedError("passive-source FWI (pfwi mode=4, pfwi.c:1507) is not built")
+def pfwic(vel, q, wav, datasrc, pararray):
+    """Passive-source FWI with known sources (pfwi.c:1507-2036 -> pfwi,
+    wave_fwi.c:212-322, gradient_pas_av): ``datasrc`` is the data
+    (nt*nx*ns, time fastest) followed by the source fields (nz*nx*nt*ns, z
+    fastest), the result the model after each of ``pararray[19]`` (niter)
+    L-BFGS iterations (nz*nx*niter, zero after an early stop).  ``q`` and
+    ``wav`` are read and ignored.  With ``pararray[9]`` (inv) = 0 the
+    reference returns an unset array; here that raises ``ValueError``."""
+    par = L.f32(pararray).reshape(-1)
+    a = _args(par)
+    if int(par[9]) == 0:
+        raise L.ShapeError(L.PW_ERR_VALUE, "pfwic needs inv = 1 (pfwi.c:1997-2018)")
+    vel = L.f32(vel).reshape(-1)
+    ds = L.f32(datasrc).reshape(-1)
+    nd, nm = a.nt * a.nx * a.ns, a.nz * a.nx * a.nt * a.ns
+    if vel.size != a.nz * a.nx or ds.size != nd + nm:
+        raise L.ShapeError(L.PW_ERR_SHAPE, "vel must hold nz*nx and datasrc nt*nx*ns + "
+                                           "nz*nx*nt*ns values")
+    data = np.ascontiguousarray(ds[:nd])
+    src = np.ascontiguousarray(ds[nd:])
+    vinv = np.zeros(a.nz * a.nx * max(a.niter, 0), np.float32)
+    import ctypes
+    done = ctypes.c_int(0)
+    L.check(L.lib().pw_pfwi_passive(a, L.ptr(vel), L.ptr(src), L.ptr(data), L.ptr(vinv),
+                                    ctypes.byref(done), None))
+    return vinv

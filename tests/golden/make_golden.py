@@ -24,8 +24,8 @@ import sys
 
 import numpy as np
 
-from models import (BIG3D, BIG3D_BAND, BIG3D_TRI_JSNAP, LSTRI, MID, big3d_velocity, digest,
-                    lstri_case, mid_models, mid_wavelet, pfwi_scale_case)
+from models import (BIG3D, BIG3D_BAND, BIG3D_TRI_JSNAP, LSTRI, MID, PAS, big3d_velocity, digest,
+                    lstri_case, mid_models, mid_wavelet, pas_case, pfwi_scale_case)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
@@ -61,6 +61,7 @@ def refdrv():
     f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
     L.refdrv_ricker.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, f32p]
     L.refdrv_gradient.argtypes = [f32p, f32p, f32p, f32p, f32p, C.c_int, f32p, f32p]
+    L.refdrv_gradient_pas.argtypes = [f32p, f32p, f32p, f32p, f32p, f32p, C.c_int, f32p, f32p]
     return L
 
 
@@ -189,6 +190,55 @@ def make_lstri():
                         data=data, srcinv=srcinv)
 
 
+def _pas_child(out_path):
+    """Runs in a fresh process: the passive data of the true model by the
+    reference's lstric (pfwi mode 4, inv 0) and the reference's pfwic (mode
+    4, inv 1, onlysrc False, onlyvel True) from the start model."""
+    pf = load("pfwi")
+    vt, vs, src = pas_case()
+    q = np.full(vt.shape, 1e4, np.float32)
+    wav = np.zeros(PAS["nt"], np.float32)
+    data = quiet(pf.pfwi, vt, q, wav, src, mode=4, par=dict(PAS, inv=False))[0]
+    out = quiet(pf.pfwi, vs, q, wav, src, data=data, mode=4,
+                par=dict(PAS, inv=True, onlysrc=False, onlyvel=True))
+    np.savez(out_path, data=data, vinv=out[1], ret0=out[0])
+
+
+def make_pfwi_pas(R):
+    """pfwi mode 4 with velocity update (pfwic, pfwi.c:1507): the reference's
+    raw gradient_pas_av at the start model (rect 1 and 3, first-call
+    scaling included) and 4 iterations of pfwic, 30 x 40, 2 shots, nt 400,
+    data from the reference's lstric on the true model."""
+    import subprocess
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "pas.npz")
+        code = ("import sys; sys.path.insert(0, %r); import make_golden as M; "
+                "M._pas_child(%r)" % (HERE, path))
+        subprocess.run([sys.executable, "-c", code], check=True, env=dict(os.environ))
+        with np.load(path) as z:
+            data, vinv, ret0 = z["data"], z["vinv"], z["ret0"]
+    vt, vs, src = pas_case()
+    nz, nx, nt, ns = src.shape
+    parr = _fwi_parr(PAS)
+    q = np.full(nz * nx, 1e4, np.float32)
+    wav = np.zeros(nt, np.float32)
+    dflat = np.ascontiguousarray(data.flatten(order="F"))  # [ns][nr][nt]
+    sflat = np.ascontiguousarray(src.flatten(order="F"))   # [ns][nt][nx][nz]
+    g = {}
+    for rect in (1, 3):
+        gr = np.zeros(nz * nx, np.float32)
+        fc = np.zeros(1, np.float32)
+        quiet(R.refdrv_gradient_pas, parr, np.ascontiguousarray(vs.flatten(order="F")), q.copy(),
+              wav.copy(), dflat.copy(), sflat.copy(), rect, gr, fc)
+        g[rect] = (gr.reshape(nz, nx, order="F"), float(fc[0]))
+    np.savez_compressed(os.path.join(HERE, "pfwi_pas.npz"), vtrue=vt, vstart=vs,
+                        src_digest=digest(src), data=data, grad_rect1=g[1][0],
+                        grad_rect3=g[3][0], fcost=g[1][1], vinv=vinv,
+                        ret0_equals_data_flat=np.array_equal(ret0.reshape(-1),
+                                                             data.flatten(order="F")))
+
+
 class _Recorder:
     """Stands in for an extension module: records each call's arguments and
     returns the real module's result."""
@@ -281,7 +331,7 @@ def main(names=()):
     R.refdrv_forward.argtypes = [np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")] * 5
     extra = {"afd3d_big": lambda: make_afd3d_big(a3, R), "pfwi_scale": lambda: make_pfwi_scale(R),
              "pfwi_mid": lambda: make_pfwi_mid(pf, R), "dropin": make_dropin,
-             "lstri": make_lstri}
+             "lstri": make_lstri, "pfwi_pas": lambda: make_pfwi_pas(R)}
     if names:
         for n in names:
             extra[n]()

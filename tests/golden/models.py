@@ -132,3 +132,32 @@ def lstri_case():
             a = (np.pi * 15.0 * (t - t0)) ** 2
             src[iz, ix, :, s] += (1e3 * (1 - 2 * a) * np.exp(-a)).astype(np.float32)
     return vel, src
+
+
+# ---- passive mode 4 with velocity update (pfwic): 30 x 40, 2 shots ---------
+PAS = dict(nz=30, nx=40, dz=0.01, dx=0.01, oz=0.0, ox=0.0, nt=400, dt=0.001, ot=0.0, ns=2,
+           ds=0.1, os=0.05, nb=20, coef=0.005, f0=10.0, acqui_type=1, interval=1, niter=4)
+
+
+def pas_case():
+    """True velocity (2.0 -> 2.6 km/s with depth and a +8% lens), the start
+    model (the linear trend alone), and the source field (nz, nx, nt, ns):
+    per shot three buried point sources carrying seeded, delayed 15 Hz
+    Ricker pulses of amplitude 1e6 (the demos' scale,
+    demos/test_pfwi_vel2d.py)."""
+    p = PAS
+    rng = np.random.default_rng(17)
+    nz, nx, nt, ns = p["nz"], p["nx"], p["nt"], p["ns"]
+    z = np.arange(nz, dtype=np.float32)[:, None]
+    vs = (2.0 + 0.6 * z / nz + np.zeros((nz, nx))).astype(np.float32)
+    iz, ix = np.ogrid[:nz, :nx]
+    lens = ((iz - 14) / 5.0) ** 2 + ((ix - 20) / 8.0) ** 2 <= 1.0
+    vt = np.where(lens, vs * 1.08, vs).astype(np.float32)
+    t = np.arange(nt) * p["dt"]
+    src = np.zeros((nz, nx, nt, ns), np.float32)
+    for s in range(ns):
+        for _ in range(3):
+            jz, jx = int(rng.integers(18, nz - 3)), int(rng.integers(4, nx - 4))
+            a = (np.pi * 15.0 * (t - float(rng.uniform(0.05, 0.12)))) ** 2
+            src[jz, jx, :, s] += (1e6 * (1 - 2 * a) * np.exp(-a)).astype(np.float32)
+    return vt, vs, src

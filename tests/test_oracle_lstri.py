@@ -59,3 +59,28 @@ def test_timerev_is_an_exact_adjoint_pair(oracle):
         a = float(np.sum(Am.astype(np.float64) * d))
         b = float(np.sum(m * Ad.astype(np.float64)))
         assert abs(a - b) <= tol * abs(a)
+
+
+def _pas(golden, oracle):
+    g = golden("pfwi_pas")
+    vt, vs, src = M.pas_case()
+    assert np.array_equal(vt, g["vtrue"]) and np.array_equal(vs, g["vstart"])
+    assert M.digest(src) == str(g["src_digest"])
+    p = M.PAS
+    geo = oracle.pfwi_geometry(p["nz"], p["nx"], p["dz"], p["dx"], 0, 0, p["ns"], p["ds"],
+                               p["os"], p["nb"])
+    kw = dict(nb=p["nb"], coef=p["coef"], dz=p["dz"], dx=p["dx"], dt=p["dt"], geo=geo,
+              ns=p["ns"], nt=p["nt"])
+    return g, vs, src, kw
+
+
+def test_gradient_pas_av_bit_exact(golden, oracle):
+    """pfwic's passive gradient (gradient_pas_av with the source fields, the
+    first-call scaling and the rect 1 / 3 smoothing) identical to the
+    reference's, and its misfit."""
+    g, vs, src, kw = _pas(golden, oracle)
+    raw, fcost = oracle.pfwi_gradient_pas(vs, src, g["data"], **kw)
+    assert np.float32(fcost) == np.float32(g["fcost"])
+    for rect in (1, 3):
+        pp, _ = oracle.pfwi_postprocess(raw, rect=rect)
+        assert np.array_equal(pp, g["grad_rect%d" % rect])

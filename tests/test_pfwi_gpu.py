@@ -187,6 +187,7 @@ def test_pfwi_errors(cuda_lib):
                os=0.1, nb=10, coef=0.005, f0=10, acqui_type=1, interval=1, niter=1)
     with pytest.raises(ValueError):  # 2.0 * 0.01 / 0.01 > 0.555
         pw.pfwi(vel, q, np.zeros(50, np.float32), None, mode=1, par=par)
-    with pytest.raises(NotImplementedError):  # passive FWI (pfwic)
-        pw.pfwi(vel, q, np.zeros(50, np.float32), None, mode=4,
+    with pytest.raises(ValueError):  # passive FWI (pfwic): the same stability check
+        pw.pfwi(vel, q, np.zeros(50, np.float32), np.zeros((20, 30, 50, 1), np.float32),
+                data=np.zeros((50, 30, 1), np.float32), mode=4,
                 par=dict(par, inv=True, onlysrc=False))
