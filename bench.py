@@ -48,12 +48,13 @@ def parse():
     p.add_argument("--no-fwi2d", action="store_true",
                    help="tri3d: skip the secondary 2-D FWI gradients/s field")
     p.add_argument("--workload", default="tri3d",
-                   choices=["tri3d", "fwi2d", "batch2d", "c1", "fwi3d", "lstri"],
+                   choices=["tri3d", "fwi2d", "batch2d", "c1", "fwi3d", "lstri", "pfwic"],
                    help="tri3d: the 3-D TRI image (default); fwi2d: 2-D FWI gradients/s; "
                         "batch2d: uneven 2-D forward shots in one batch; c1: one 2-D shot; "
-                        "fwi3d: 3-D FWI gradients/s; lstri: pfwi mode 4 source inversion")
+                        "fwi3d: 3-D FWI gradients/s; lstri: pfwi mode 4 source inversion; "
+                        "pfwic: pfwi mode 4 passive FWI gradients/s")
     p.add_argument("--lstri-niter", type=int, default=30, help="lstri: CG iterations per shot")
-    p.add_argument("--lstri-nt", type=int, default=3001, help="lstri: time samples")
+    p.add_argument("--lstri-nt", type=int, default=3001, help="lstri / pfwic: time samples")
     p.add_argument("--fwi3d-nt", type=int, default=2500, help="fwi3d: time samples")
     p.add_argument("--fwi3d-shots", type=int, default=16, help="fwi3d: shots per gradient")
     p.add_argument("--shots", type=int, default=32, help="fwi2d: shots per gradient")
@@ -1289,6 +1290,183 @@ def run_lstri(args, world, rank, local):
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks}), flush=True)
 
 
+def _pas_ref_worker(kind, nt_s):
+    """One passive gradient (gradient_pas_av) of one shot at the benchmark
+    grid over nt_s steps by the reference itself (oracle/_ref libpwref;
+    kind "port": the oracle's restatement); returns (point-updates, s)."""
+    sys.path.insert(0, ROOT)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    vel, src = lstri_case(7, ns=1, nt=nt_s)
+    par = lstri_par(1, ns=1, nt=nt_s)
+    pts = 2.0 * (LS_NZ + 2 * LS_NB) * (LS_NX + 2 * LS_NB) * nt_s  # forward + backward
+    dobs = np.zeros((1, LS_NX, nt_s), np.float32)
+    sflat = np.ascontiguousarray(src.reshape(-1))
+    if kind == "reference":
+        import ctypes as C
+        L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libpwref.so"))
+        f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+        L.refdrv_gradient_pas.argtypes = [f32p] * 6 + [C.c_int, C.c_float, C.c_float, f32p, f32p]
+        parr = np.array([par[k] for k in ("nz", "nx", "dz", "dx", "oz", "ox", "nt", "dt", "ot",
+                                          "ns", "ds", "os", "nb", "coef", "f0", "acqui_type",
+                                          "interval")], np.float32)
+        g = np.zeros(LS_NZ * LS_NX, np.float32)
+        fc = np.zeros(1, np.float32)
+        t0 = time.perf_counter()
+        L.refdrv_gradient_pas(parr, np.ascontiguousarray(vel.flatten(order="F")),
+                              np.full(LS_NZ * LS_NX, 1e4, np.float32), np.zeros(nt_s, np.float32),
+                              np.ascontiguousarray(dobs.reshape(-1)), sflat, 1, 0.0,
+                              float(np.float32(0.5) / np.float32(LS_DT)), g, fc)
+    else:
+        from oracle import oracle as O
+        geo = O.pfwi_geometry(LS_NZ, LS_NX, LS_DZ, LS_DX, 0, 0, 1, 0.1, 0.0, LS_NB)
+        t0 = time.perf_counter()
+        O.pfwi_gradient_pas(vel, src.transpose(3, 2, 1, 0), dobs.transpose(2, 1, 0), LS_NB, LS_COEF,
+                            LS_DZ, LS_DX, LS_DT, geo, 1, nt_s)
+    return pts, time.perf_counter() - t0
+
+
+def _pas_cpu(workers, nt_s):
+    for kind in ("reference", "port"):
+        try:
+            res = pool_map(_pas_ref_worker, [(kind, nt_s)] * workers, timeout_s=600)
+            return sum(r[0] for r in res) / max(r[1] for r in res) / 1e9, kind
+        except Exception:  # noqa: BLE001
+            continue
+    raise RuntimeError("neither the reference nor the port ran")
+
+
+def run_pfwic(args, world, rank, local):
+    """Passive FWI (pfwic) at the passive demos' grid: a step is one passive
+    gradient (gradient_pas_av: forward with the source fields, backward with
+    the residual, imaging) of all shots, the unit pfwic's L-BFGS spends its
+    time in."""
+    nt = args.lstri_nt
+    pad = (LS_NZ + 2 * LS_NB) * (LS_NX + 2 * LS_NB)
+    cfg = {"workload": f"pfwi mode 4 passive FWI gradient {LS_NZ}x{LS_NX} dz=8m dx=12m nt={nt} "
+                       f"nb={LS_NB} shots={LS_NS} (gradient_pas_av, reference mode)",
+           "padded_cells": pad}
+    metric = "passive FWI gradients/s (pfwic's gradient_pas_av)"
+    nt_ref = min(nt, 600)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        workers = max(1, min(os.cpu_count() or 1, 16))
+        rates = []
+        for i in range(args.warmup + args.steps):
+            v, kind = _pas_cpu(workers, nt_ref)
+            if i >= args.warmup:
+                rates.append(v)
+        gps = statistics.median(rates) * 1e9 / (2.0 * pad * nt * LS_NS)
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": gps, "unit": "gradients/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": gps, "unit": "gradients/s", "cores": workers, "kind": kind,
+                             "sample": f"one gradient_pas_av of one shot over nt={nt_ref} per "
+                                       f"process, {workers} single-threaded processes, scaled to "
+                                       f"{LS_NS} shots x nt={nt}"},
+            "e2e": {"value": gps, "unit": "gradients/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import ctypes
+    import torch
+    import torch.distributed as dist
+    from pywave_b200 import _lib as L
+    from pywave_b200 import build as B
+    from pywave_b200 import fwi, lstri
+    B.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from scipy.ndimage import gaussian_filter
+    vel, src = lstri_case(7 + rank, nt=nt)
+    vs = gaussian_filter(vel.astype(np.float64), 8.0).astype(np.float32)
+    par = lstri_par(1, nt=nt)
+    st = torch.cuda.current_stream().cuda_stream
+    v_d = torch.from_numpy(np.ascontiguousarray(vel.T)).cuda()
+    s_d = torch.from_numpy(src).cuda()  # [ns][nt][nx][nz]
+    d_d = torch.empty((LS_NS, LS_NX, nt), device="cuda")
+    lstri.lstri_forward_torch(v_d, s_d, d_d, par)  # observed data as the demos make it
+    vs_d = torch.from_numpy(np.ascontiguousarray(vs.T)).cuda()
+    g_d = torch.empty(LS_NZ * LS_NX, device="cuda")
+    a = fwi.fwi_args(par, 0)
+    J = ctypes.c_double(0.0)
+    lib = L.lib()
+
+    def grad():
+        L.check(lib.pw_pfwi_gradient_passive(a, L.PW_GRAD_REFERENCE, vs_d.data_ptr(),
+                                             s_d.data_ptr(), d_d.data_ptr(), None, g_d.data_ptr(),
+                                             ctypes.byref(J), 0, st))
+        return L.last_timing()
+
+    for _ in range(args.warmup):
+        grad()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches, loops = 0, []
+    e0.record()
+    for _ in range(args.steps):
+        ms_, nst, tot = grad()
+        loops.append(ms_)
+        launches += tot
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    # algorithmic bytes per padded point-step-shot: forward 20 B (+4 B of the
+    # source field on the interior), reference backward 20 B + imaging reads
+    loop_ms = statistics.median(loops)
+    nzx = LS_NZ * LS_NX
+    # algorithmic bytes per step and shot: forward 16 B per padded point (A,
+    # B, V read; B write) + 8 B per interior cell (source sample, snapshot);
+    # reference backward 16 B per padded point + 24 B per imaged interior
+    # cell (three snapshots, -2/v^3, gradient read and write)
+    alg = (32.0 * pad + 32.0 * nzx) * nt * LS_NS
+    peak, peak_kind = peaks()
+    e2e = None
+    if not args.no_e2e:
+        # the same gradient through the public API with host arrays (the
+        # source fields, data and model copied in, the gradient copied out)
+        dh = np.ascontiguousarray(d_d.cpu().numpy().transpose(2, 1, 0))  # (nt, nr, ns)
+        sh = np.ascontiguousarray(src.transpose(3, 2, 1, 0))             # (nz, nx, nt, ns)
+        fwi.gradient_passive(vs, sh, dh, par)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            fwi.gradient_passive(vs, sh, dh, par)
+        wall = time.perf_counter() - t0
+        e2e = {"value": args.steps / wall, "unit": "gradients/s",
+               "h2d_bytes_per_step": int(dh.nbytes + sh.nbytes + vs.nbytes),
+               "d2h_bytes_per_step": 4 * nzx}
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0:
+        workers = max(1, min(os.cpu_count() or 1, 16))
+        v, kind = _pas_cpu(workers, nt_ref)
+        cpu = {"value": v * 1e9 / (2.0 * pad * nt * LS_NS), "unit": "gradients/s",
+               "cores": workers, "kind": kind,
+               "sample": f"one gradient_pas_av of one shot over nt={nt_ref} per process, "
+                         f"{workers} single-threaded processes, scaled to {LS_NS} shots x nt={nt}"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": job_rate(1, args.steps, world, ms), "unit": "gradients/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 misfit)",
+            "data": "synthetic (seeded layered model, 3 buried Ricker sources per shot; data by "
+                    "lstric on the true model, start = smoothed)",
+            "config": cfg, "gpu_launches": launches,
+            "point_updates_per_s": 2.0 * pad * nt * LS_NS / (ms / args.steps / 1e3),
+            "roofline": {"bound": "hbm", "achieved": alg / (loop_ms / 1e3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": alg / (loop_ms / 1e3) / 1e9 / peak,
+                         "traffic": None, "kernel": "pf_step_kernel FWD(passive) + ADJ_REF",
+                         "loop_ms": loop_ms, "peak_source": peak_kind},
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks}), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1304,6 +1482,8 @@ def main():
         return run_fwi3d(args, world, rank, local)
     if args.workload == "lstri":
         return run_lstri(args, world, rank, local)
+    if args.workload == "pfwic":
+        return run_pfwic(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, rank)
 

@@ -149,6 +149,11 @@ typedef struct pw_fwi_args {
   int flags;       /* PW_HOST_PTRS | PW_NO_CFL_CHECK | PW_PER_SHOT */
   long long hbm_budget; /* bytes of device memory the exact gradient's checkpoints, segment
                            buffer and wavefields may hold; 0 = a quarter of the device */
+  float flo, fhi;       /* multiscale residual filter of the REFERENCE-mode gradients (Hz):
+                           a 3-pole zero-phase Butterworth high-pass at flo when flo*dt >
+                           0.0001 and low-pass at fhi when 0 < fhi*dt < 0.4999
+                           (gradient_pas_init / gradient_pas_av, wave_fwigradient.c:657-658,
+                           767-780); 0, 0 = off, as pfwic and fwic run it */
 } pw_fwi_args;
 
 /* Fills a pw_fwi_args from pfwi's float parameter array (pfwi.c:691-713
@@ -285,6 +290,24 @@ int pw_lstri_forward(const pw_fwi_args *a, const float *vel, const float *src, f
  * dot products run in FP64 in a fixed block order. */
 int pw_lstri_invert(const pw_fwi_args *a, const float *vel, const float *data, float *src,
                     void *stream);
+
+/* ---------------------------------------------- residual utilities --- */
+
+/* np_butter_init + np_butter_apply (wave_butter.c:18-102): every one of the
+ * ntr traces x [ntr][n] filtered in place, causally, by a Butterworth
+ * low-pass (low = 1) or high-pass (low = 0) of npoles (1..16) poles at
+ * cutoff cycles per sample.  flags: PW_HOST_PTRS. */
+int pw_butter_apply(int n, int ntr, int low, float cutoff, int npoles, float *x, int flags,
+                    void *stream);
+
+/* residual_weighting (wave_fwiutil.c:225-296), host only: w [nr][nt] is 1 on
+ * the window [woffn1, woffn2] x [wtn1, wtn2] with 10-sample sine tapers
+ * inside its edges (oreo = 0, as fwic and pfwic use it), or 0 on the window
+ * and 1 outside with the tapers outside its edges (oreo = 1).  Taper samples
+ * beyond the array (a window closer than 10 samples to an edge, where the
+ * reference writes out of bounds) are skipped. */
+int pw_residual_weights(int nt, int nr, int wtn1, int wtn2, int woffn1, int woffn2, int oreo,
+                        float *w);
 
 /* ------------------------------------------------------------ utility --- */
 

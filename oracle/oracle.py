@@ -64,6 +64,10 @@ def lib():
         L.or_smooth2d.restype = None
         L.or_residual_weights.argtypes = [C.c_int] * 6 + [_f32p]
         L.or_residual_weights.restype = None
+        L.or_residual_weights_oreo.argtypes = [C.c_int] * 6 + [_f32p]
+        L.or_residual_weights_oreo.restype = None
+        L.or_butter_coefs.argtypes = [C.c_int, C.c_float, C.c_int, _f32p, _f32p]
+        L.or_butter_coefs.restype = None
         for sfx, rp in (("f32", _f32p), ("f64", _f64p)):
             f = getattr(L, "or_afd_" + sfx)
             f.argtypes = ([C.c_int] * 5 + [C.c_float] * 5 + [C.c_int, C.c_int, _i32p, _i32p, _i32p,
@@ -81,8 +85,11 @@ def lib():
             f = getattr(L, "or_pfwi_gradient_pas_" + sfx)
             f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 2 + [C.c_int]
                           + [C.c_int, C.c_int, _i32p, _i32p, _i32p, C.c_int, C.c_int]
-                          + [rp, rp, rp, rp, rp])
+                          + [rp, rp, rp, rp, rp, C.c_float, C.c_float])
             f.restype = real
+            f = getattr(L, "or_butter_apply_" + sfx)
+            f.argtypes = [C.c_int, C.c_float, C.c_int, C.c_int, rp]
+            f.restype = None
             f = getattr(L, "or_pfwi_gradient_exact_" + sfx)
             f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 2 + geo
                           + [rp, rp, rp, C.c_void_p, rp])
@@ -264,12 +271,35 @@ def pfwi_forward(vel, wav, nb, coef, dz, dx, dt, geo, ns, precision="f32"):
     return out.reshape(nt, geo["nr"], ns, order="F")
 
 
-def residual_weights(nt, nr, wtn1=None, wtn2=None, woffn1=None, woffn2=None):
-    """residual_weighting (oreo=false) as fwic configures it; (nr,nt) C-order."""
+def residual_weights(nt, nr, wtn1=None, wtn2=None, woffn1=None, woffn2=None, oreo=False):
+    """residual_weighting (oreo=false as fwic configures it, or the oreo
+    branch); (nr,nt) C-order."""
     w = np.zeros(nr * nt, np.float32)
-    lib().or_residual_weights(nt, nr, 0 if wtn1 is None else wtn1, nt - 1 if wtn2 is None else wtn2,
-                              0 if woffn1 is None else woffn1, nr - 1 if woffn2 is None else woffn2, w)
+    fn = lib().or_residual_weights_oreo if oreo else lib().or_residual_weights
+    fn(nt, nr, 0 if wtn1 is None else wtn1, nt - 1 if wtn2 is None else wtn2,
+       0 if woffn1 is None else woffn1, nr - 1 if woffn2 is None else woffn2, w)
     return w.reshape(nr, nt)
+
+
+def butter_apply(x, low, cutoff, npoles=3, precision="f32"):
+    """np_butter_apply over each row of x (a copy), cutoff in cycles per
+    sample (wave_butter.c)."""
+    R = np.float32 if precision == "f32" else np.float64
+    y = np.ascontiguousarray(np.array(x, dtype=R, ndmin=2))
+    for row in y:
+        r = np.ascontiguousarray(row)
+        getattr(lib(), "or_butter_apply_" + precision)(int(low), float(cutoff), int(npoles),
+                                                       r.size, r)
+        row[:] = r
+    return y.reshape(np.shape(x))
+
+
+def butter_coefs(low, cutoff, npoles=3):
+    """(den [nsections][2], mid) of np_butter_init."""
+    den = np.zeros(2 * (npoles // 2 + npoles % 2), np.float32)
+    mid = np.zeros(1, np.float32)
+    lib().or_butter_coefs(int(low), float(cutoff), int(npoles), den, mid)
+    return den.reshape(-1, 2), float(mid[0])
 
 
 def _dobs_flat(dobs, R):
@@ -295,7 +325,7 @@ def pfwi_gradient_ref(vel, wav, dobs, nb, coef, dz, dx, dt, geo, ns, interval=1,
 
 
 def pfwi_gradient_pas(vel, src, dobs, nb, coef, dz, dx, dt, geo, ns, nt, interval=1,
-                      weight=None, precision="f32"):
+                      weight=None, precision="f32", flo=0.0, fhi=None):
     """gradient_pas_av (pfwic's passive gradient) before scaling/smoothing;
     src (nz, nx, nt, ns) source fields, dobs (nt, nr, ns).  Returns
     (grad (nz, nx), fcost)."""
@@ -309,7 +339,8 @@ def pfwi_gradient_pas(vel, src, dobs, nb, coef, dz, dx, dt, geo, ns, nt, interva
     f = getattr(lib(), "or_pfwi_gradient_pas_" + precision)(
         nz, nx, nb, dz, dx, nt, dt, coef, interval, ns, geo["nr"], geo["r0v"], geo["r02"],
         geo["nr2"], geo["drv"], geo["rz"], v, sv, _dobs_flat(dobs, R),
-        np.ascontiguousarray(np.asarray(weight, np.float32).astype(R)), g)
+        np.ascontiguousarray(np.asarray(weight, np.float32).astype(R)), g, float(flo),
+        float(np.float32(0.5) / np.float32(dt)) if fhi is None else float(fhi))
     return g.reshape(nz, nx, order="F"), float(f)
 
 

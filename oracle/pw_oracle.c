@@ -15,7 +15,8 @@
  *                            wave_fwiutil.c:19-223
  *   gradient_av              pywave/src/wave_fwigradient.c:93-262
  *   triangle smoothing       pywave/src/wave_triangle.c:177-238 (np_smooth2)
- *   residual weighting       pywave/src/wave_fwiutil.c:225-296
+ *   residual weighting       pywave/src/wave_fwiutil.c:225-296 (both branches)
+ *   Butterworth filter       pywave/src/wave_butter.c:18-116
  * plus the exact discrete adjoint of the pfwi forward step (FP64), derived
  * for this project and checked against finite differences in tests/, and
  * the 3-D extension of the pfwi scheme with its exact adjoint
@@ -163,6 +164,84 @@ void or_residual_weights(int nt, int nr, int wtn1, int wtn2, int woffn1, int wof
             w[ir * nt + wtn1 + it] *= s[it];
             w[ir * nt + wtn2 - it] *= s[it];
         }
+}
+
+/* residual_weighting with oreo = true (wave_fwiutil.c:236-265): 1 outside
+ * [woffn1,woffn2]x[wtn1,wtn2], 0 inside, 10-sample sine tapers on the
+ * outer sides.  w: [nr][nt]. */
+void or_residual_weights_oreo(int nt, int nr, int wtn1, int wtn2, int woffn1, int woffn2,
+                              float *w)
+{
+    float s[10];
+    for (int i = 0; i < 10; i++) s[i] = sinf(0.5 * M_PI * (i + 1) / 11.);
+    for (int i = 0; i < nr * nt; i++) w[i] = 1.f;
+    for (int ir = woffn1; ir <= woffn2; ir++)
+        for (int it = wtn1; it <= wtn2; it++) w[ir * nt + it] = 0.f;
+    for (int ir = 0; ir < 10; ir++)
+        for (int it = wtn1; it <= wtn2; it++) {
+            if (woffn1 - ir > 0) w[(woffn1 - ir) * nt + it] *= s[ir];
+            if (woffn2 + ir < nr) w[(woffn2 + ir) * nt + it] *= s[ir];
+        }
+    for (int it = 0; it < 10; it++) {
+        for (int ir = 0; ir < woffn1; ir++) {
+            w[ir * nt + wtn1 + it] *= s[it];
+            w[ir * nt + wtn2 - it] *= s[it];
+        }
+        for (int ir = woffn2 + 1; ir < nr; ir++) {
+            w[ir * nt + wtn1 + it] *= s[it];
+            w[ir * nt + wtn2 - it] *= s[it];
+        }
+    }
+}
+
+/* np_butter_init (wave_butter.c:18-62): a Butterworth filter of nn poles as
+ * one first-order section (odd nn) and nn/2 second-order sections, cutoff in
+ * cycles per sample, every coefficient rounded to float as the reference
+ * stores it (its double/float mix kept). */
+typedef struct {
+    int nn, low;
+    float den[16][2];
+    float mid;
+} or_butter_t;
+
+static void or_butter_init(or_butter_t *bw, int low, float cutoff, int nn)
+{
+    const double pi = 3.14159265358979323846264338328;
+    float arg = 2. * pi * cutoff;
+    float sinw = sinf(arg), cosw = cosf(arg), fact, ss;
+    bw->nn = nn;
+    bw->low = low;
+    if (nn % 2) {
+        if (low) {
+            fact = (1. + cosw) / sinw;
+            bw->den[nn / 2][0] = 1. / (1. + fact);
+            bw->den[nn / 2][1] = 1. - fact;
+        } else {
+            fact = sinw / (1. + cosw);
+            bw->den[nn / 2][0] = 1. / (fact + 1.);
+            bw->den[nn / 2][1] = fact - 1.;
+        }
+    }
+    fact = low ? sinf(0.5 * arg) : cosf(0.5 * arg);
+    fact *= fact;
+    for (int j = 0; j < nn / 2; j++) {
+        ss = sinf(pi * (2 * j + 1) / (2 * nn)) * sinw;
+        bw->den[j][0] = fact / (1. + ss);
+        bw->den[j][1] = (1. - ss) / fact;
+    }
+    bw->mid = -2. * cosw / fact;
+}
+
+/* the coefficients, for the GPU tests: den [nn/2 + nn%2][2], mid */
+void or_butter_coefs(int low, float cutoff, int nn, float *den, float *mid)
+{
+    or_butter_t bw;
+    or_butter_init(&bw, low, cutoff, nn);
+    for (int j = 0; j < nn / 2 + nn % 2; j++) {
+        den[2 * j] = bw.den[j][0];
+        den[2 * j + 1] = bw.den[j][1];
+    }
+    *mid = bw.mid;
 }
 
 #define REAL float

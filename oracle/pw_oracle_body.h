@@ -212,6 +212,54 @@ static void SFX(pf_laplace)(const REAL *p, REAL *term, int pnx, int pnz, REAL dx
         }
 }
 
+/* np_butter_apply (wave_butter.c:64-102): in place over one trace, the
+ * first-order section first (odd nn), then each second-order section */
+static void SFX(pf_butter_apply)(const or_butter_t *bw, int nx, REAL *x)
+{
+    const REAL d1 = bw->mid;
+    const int nn = bw->nn;
+    REAL d0, d2, x0 = 0, x1 = 0, x2, y0, y1 = 0, y2 = 0;
+    if (nn % 2) {
+        d0 = bw->den[nn / 2][0];
+        d2 = bw->den[nn / 2][1];
+        x0 = y1 = 0;
+        for (int ix = 0; ix < nx; ix++) {
+            x1 = x0; x0 = x[ix];
+            y0 = bw->low ? (x0 + x1 - d2 * y1) * d0 : (x0 - x1 - d2 * y1) * d0;
+            x[ix] = y1 = y0;
+        }
+    }
+    for (int j = 0; j < nn / 2; j++) {
+        d0 = bw->den[j][0];
+        d2 = bw->den[j][1];
+        x1 = x0 = y1 = y2 = 0;
+        for (int ix = 0; ix < nx; ix++) {
+            x2 = x1; x1 = x0; x0 = x[ix];
+            y0 = bw->low ? (x0 + 2 * x1 + x2 - d1 * y1 - d2 * y2) * d0
+                         : (x0 - 2 * x1 + x2 - d1 * y1 - d2 * y2) * d0;
+            y2 = y1; x[ix] = y1 = y0;
+        }
+    }
+}
+
+/* apply, reverse, apply, reverse (wave_fwigradient.c:769-780): zero phase */
+static void SFX(pf_butter_zero_phase)(const or_butter_t *bw, int nt, REAL *x)
+{
+    for (int pass = 0; pass < 2; pass++) {
+        SFX(pf_butter_apply)(bw, nt, x);
+        for (int i = 0; i < nt / 2; i++) {
+            REAL t = x[i]; x[i] = x[nt - 1 - i]; x[nt - 1 - i] = t;
+        }
+    }
+}
+
+void SFX(or_butter_apply)(int low, float cutoff, int nn, int nx, REAL *x)
+{
+    or_butter_t bw;
+    or_butter_init(&bw, low, cutoff, nn);
+    SFX(pf_butter_apply)(&bw, nx, x);
+}
+
 /* apply_sponge (wave_fwiutil.c:201-223): top, bottom per column, then left,
  * right per row */
 static void SFX(pf_apply_sponge)(REAL *p, const REAL *bc, int pnx, int pnz, int nb)
@@ -314,7 +362,8 @@ static REAL SFX(pf_gradient_core)(int nz, int nx, int nb, float dz, float dx, in
                                   int ns, const int *sx, int sz, int nr, const int *r0v,
                                   const int *r02, const int *nr2, int drv, int rz,
                                   const REAL *vel, const REAL *wav, const REAL *dsrc,
-                                  const REAL *dobs, const REAL *weight, REAL *grad)
+                                  const REAL *dobs, const REAL *weight, REAL *grad,
+                                  const or_butter_t *blo, const or_butter_t *bhi)
 {
     const int pnz = nz + 2 * nb, pnx = nx + 2 * nb;
     const size_t np = (size_t)pnz * pnx, nzx = (size_t)nz * nx;
@@ -372,6 +421,10 @@ static REAL SFX(pf_gradient_core)(int nz, int nx, int nb, float dz, float dx, in
                 pp[k] = dd[k] - pp[k];
                 fcost += 0.5 * pp[k] * pp[k];
             }
+        for (int ir = 0; ir < nr; ir++) {  /* multiscale (wave_fwigradient.c:767-780) */
+            if (blo) SFX(pf_butter_zero_phase)(blo, nt, pp + (size_t)ir * nt);
+            if (bhi) SFX(pf_butter_zero_phase)(bhi, nt, pp + (size_t)ir * nt);
+        }
         for (size_t k = 0; k < (size_t)nr * nt; k++) pp[k] *= weight[k];
         memset(p0, 0, np * sizeof(REAL)); memset(p1, 0, np * sizeof(REAL)); memset(p2, 0, np * sizeof(REAL));
         memset(term, 0, np * sizeof(REAL));
@@ -425,7 +478,8 @@ REAL SFX(or_pfwi_gradient_ref)(int nz, int nx, int nb, float dz, float dx, int n
                                const REAL *weight, REAL *grad)
 {
     return SFX(pf_gradient_core)(nz, nx, nb, dz, dx, nt, dt, coef, interval, ns, sx, sz, nr, r0v,
-                                 r02, nr2, drv, rz, vel, wav, NULL, dobs, weight, grad);
+                                 r02, nr2, drv, rz, vel, wav, NULL, dobs, weight, grad, NULL,
+                                 NULL);
 }
 
 /* gradient_pas_av (wave_fwigradient.c:667-852) as pfwic sets it up
@@ -433,15 +487,25 @@ REAL SFX(or_pfwi_gradient_ref)(int nz, int nx, int nb, float dz, float dx, int n
  * multiscale filter): gradient_av with the source field dsrc
  * [ns][nt][nx][nz] added to the interior's term and the update restricted to
  * [4, pad-4).  Raw, before the scaling and gradient_smooth2b (waterz =
- * waterzb = 0, the same smoothing as gradient_smooth2 with waterz 0). */
+ * waterzb = 0, the same smoothing as gradient_smooth2 with waterz 0).
+ * flo, fhi: the multiscale cutoffs in Hz (soupar, scaled by dt in
+ * preparation); the residual is filtered by a 3-pole zero-phase high-pass
+ * when flo*dt > 0.0001 and low-pass when fhi*dt < 0.4999
+ * (gradient_pas_init :657-658).  pfwic passes flo 0, fhi 0.5/dt: no filter. */
 REAL SFX(or_pfwi_gradient_pas)(int nz, int nx, int nb, float dz, float dx, int nt, float dt,
                                float coef, int interval, int ns, int nr, const int *r0v,
                                const int *r02, const int *nr2, int drv, int rz,
                                const REAL *vel, const REAL *dsrc, const REAL *dobs,
-                               const REAL *weight, REAL *grad)
+                               const REAL *weight, REAL *grad, float flo, float fhi)
 {
+    or_butter_t lo, hi;
+    const float flo_dt = flo * dt, fhi_dt = fhi * dt;
+    const int use_lo = flo_dt > 0.0001, use_hi = fhi_dt < 0.5 - 0.0001;
+    if (use_lo) or_butter_init(&lo, 0, flo_dt, 3);
+    if (use_hi) or_butter_init(&hi, 1, fhi_dt, 3);
     return SFX(pf_gradient_core)(nz, nx, nb, dz, dx, nt, dt, coef, interval, ns, NULL, 0, nr, r0v,
-                                 r02, nr2, drv, rz, vel, NULL, dsrc, dobs, weight, grad);
+                                 r02, nr2, drv, rz, vel, NULL, dsrc, dobs, weight, grad,
+                                 use_lo ? &lo : NULL, use_hi ? &hi : NULL);
 }
 
 /* Exact discrete adjoint of the pfwi forward scheme.

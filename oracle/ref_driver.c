@@ -17,6 +17,7 @@
 #include "wave_fwiutil.h"
 #include "wave_fwimodeling.h"
 #include "wave_fwigradient.h"
+#include "wave_butter.h"
 #include "wave_komplex.h" /* pulls in wave_kissfft.h once */
 #include "wave_ricker.h"
 #include "wave_freqfilt.h"
@@ -117,16 +118,19 @@ void refdrv_gradient(const float *par, float *vel, float *q, float *wav,
 /* gradient_pas_init + one gradient_pas_av call (wave_fwigradient.c:528-870)
  * as pfwic sets them up (pfwi.c:1780-1890: velocity only, so the source
  * weight is 1 and no source inversion runs), with the caller's smoothing
- * radius.  src: [ns][nt][nx][nz] source fields.  The output includes the
+ * radius and multiscale cutoffs.  src: [ns][nt][nx][nz] source fields.  The output includes the
  * first-call 0.1/max|g| scaling. */
 void refdrv_gradient_pas(const float *par, float *vel, float *q, float *wav, float *dobs,
-                         float *src, int rect, float *grad, float *fcost)
+                         float *src, int rect, float flo, float fhi, float *grad, float *fcost)
 {
     np_sou soupar = (np_sou)np_alloc(1, sizeof(*soupar));
     np_acqui acpar = (np_acqui)np_alloc(1, sizeof(*acpar));
     np_vec array = (np_vec)np_alloc(1, sizeof(*array));
     np_fwi fwipar = (np_fwi)np_alloc(1, sizeof(*fwipar));
     fill_acpar(acpar, soupar, par);
+    /* multiscale cutoffs in Hz (pfwic: flo 0, fhi 0.5/dt, i.e. no filter) */
+    soupar->flo = flo;
+    soupar->fhi = fhi;
     np_pas paspar = passive_init(acpar);
     paspar->inv = true;
     paspar->onlysrc = false;
@@ -152,4 +156,23 @@ void refdrv_gradient_pas(const float *par, float *vel, float *q, float *wav, flo
     fwipar->rectz = rect;
     gradient_pas_init(d, w, NULL, soupar, acpar, array, fwipar, paspar, false);
     gradient_pas_av(array->vv, fcost, grad);
+}
+
+/* np_butter_init + np_butter_apply over n samples (wave_butter.c) */
+void refdrv_butter(int low, float cutoff, int nn, int n, float *x)
+{
+    np_butter bw = np_butter_init(low != 0, cutoff, nn);
+    np_butter_apply(bw, n, x);
+    np_butter_close(bw);
+}
+
+/* residual_weighting (wave_fwiutil.c:225-296); w: [nr][nt] */
+void refdrv_residual_weights(int nt, int nr, int wtn1, int wtn2, int woffn1, int woffn2,
+                             int oreo, float *w)
+{
+    float **ww = np_floatalloc2(nt, nr);
+    residual_weighting(ww, nt, nr, wtn1, wtn2, woffn1, woffn2, oreo != 0);
+    memcpy(w, ww[0], sizeof(float) * nt * nr);
+    free(ww[0]);
+    free(ww);
 }

@@ -63,7 +63,7 @@ class FwiArgs(C.Structure):
                 ("nb", C.c_int), ("coef", C.c_float), ("f0", C.c_float),
                 ("acqui_type", C.c_int), ("interval", C.c_int), ("niter", C.c_int),
                 ("sz", C.c_int), ("rz", C.c_int), ("flags", C.c_int),
-                ("hbm_budget", C.c_longlong)]
+                ("hbm_budget", C.c_longlong), ("flo", C.c_float), ("fhi", C.c_float)]
 
 
 class Fwi3dArgs(C.Structure):
@@ -100,6 +100,9 @@ _SIGS = {
     "pw_pfwi_passive": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp, C.POINTER(C.c_int),
                                   _vp]),
     "pw_timerev": (C.c_int, [C.POINTER(FwiArgs), C.c_int, _vp, _vp, _vp, _vp]),
+    "pw_butter_apply": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _vp, C.c_int,
+                                  _vp]),
+    "pw_residual_weights": (C.c_int, [C.c_int] * 7 + [_vp]),
     "pw_lstri_forward": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp]),
     "pw_lstri_invert": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp]),
     "pw_last_fwi_plan": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int),

@@ -489,6 +489,114 @@ __global__ void misfit_sum_kernel(double *misfit, int nblocks) {
 }
 constexpr int RESID_BLOCKS = 592;
 
+// A Butterworth filter as np_butter_init builds it (wave_butter.c:18-62):
+// for odd nn one first-order section (den[nn/2]), and nn/2 second-order
+// sections sharing the middle coefficient `mid`.
+constexpr int BUTTER_MAXP = 16;
+struct ButterCoef {
+  int nn, low;
+  float den[BUTTER_MAXP / 2 + 1][2];
+  float mid;
+};
+
+// One causal sweep of np_butter_apply (wave_butter.c:64-102) over the n
+// samples x[0], x[st], ..., in index order or (bwd) from the last sample to
+// the first -- reverse, apply, reverse in one pass.  Sections run one after
+// the other over the whole trace, each product and sum in the reference's
+// order.
+__device__ __forceinline__ void butter_sweep(const ButterCoef &b, float *x, long long st, int n,
+                                             bool bwd) {
+  const float d1 = b.mid;
+  if (b.nn % 2) {
+    const float d0 = b.den[b.nn / 2][0], d2 = b.den[b.nn / 2][1];
+    float x0 = 0.f, x1, y1 = 0.f;
+    for (int k = 0; k < n; k++) {
+      const long long i = (long long)(bwd ? n - 1 - k : k) * st;
+      x1 = x0;
+      x0 = x[i];
+      const float u = b.low ? fadd(x0, x1) : fsub(x0, x1);
+      y1 = fmul(fsub(u, fmul(d2, y1)), d0);
+      x[i] = y1;
+    }
+  }
+  for (int j = 0; j < b.nn / 2; j++) {
+    const float d0 = b.den[j][0], d2 = b.den[j][1];
+    float x0 = 0.f, x1 = 0.f, x2, y1 = 0.f, y2 = 0.f;
+    for (int k = 0; k < n; k++) {
+      const long long i = (long long)(bwd ? n - 1 - k : k) * st;
+      x2 = x1;
+      x1 = x0;
+      x0 = x[i];
+      const float t = fmul(2.f, x1);
+      const float u = b.low ? fadd(fadd(x0, t), x2) : fadd(fsub(x0, t), x2);
+      const float y0 = fmul(fsub(fsub(u, fmul(d1, y1)), fmul(d2, y2)), d0);
+      y2 = y1;
+      y1 = y0;
+      x[i] = y0;
+    }
+  }
+}
+
+// pw_butter_apply: one causal sweep per trace, traces x [ntr][n]
+__global__ void butter_traces_kernel(const ButterCoef b, float *x, int n, int ntr) {
+  const int tr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tr < ntr) butter_sweep(b, x + (size_t)tr * n, 1, n, false);
+}
+
+// The multiscale residual filter of gradient_pas_av (wave_fwigradient.c:
+// 767-784) on res [shot][nt][nr]: per trace the zero-phase high-pass (apply,
+// reverse, apply, reverse), then the low-pass, then the residual weight
+// w [nr][nt] (or 1).
+__global__ void butter_residual_kernel(const ButterCoef lo, const ButterCoef hi, int use_lo,
+                                       int use_hi, float *res, int ns, int nt, int nr,
+                                       const float *w) {
+  const int tr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tr >= ns * nr) return;
+  const int s = tr / nr, ir = tr - s * nr;
+  float *x = res + (size_t)s * nt * nr + ir;
+  if (use_lo) {
+    butter_sweep(lo, x, nr, nt, false);
+    butter_sweep(lo, x, nr, nt, true);
+  }
+  if (use_hi) {
+    butter_sweep(hi, x, nr, nt, false);
+    butter_sweep(hi, x, nr, nt, true);
+  }
+  if (w)
+    for (int it = 0; it < nt; it++) x[(size_t)it * nr] = fmul(x[(size_t)it * nr], w[(size_t)ir * nt + it]);
+}
+
+// np_butter_init on the host, its float/double mix kept
+static ButterCoef butter_coef(bool low, float cutoff, int nn) {
+  const double pi = 3.14159265358979323846264338328;
+  ButterCoef b{};
+  b.nn = nn;
+  b.low = low ? 1 : 0;
+  const float arg = 2. * pi * cutoff;
+  const float sinw = ::sinf(arg), cosw = ::cosf(arg);
+  float fact;
+  if (nn % 2) {
+    if (low) {
+      fact = (1. + cosw) / sinw;
+      b.den[nn / 2][0] = 1. / (1. + fact);
+      b.den[nn / 2][1] = 1. - fact;
+    } else {
+      fact = sinw / (1. + cosw);
+      b.den[nn / 2][0] = 1. / (fact + 1.);
+      b.den[nn / 2][1] = fact - 1.;
+    }
+  }
+  fact = low ? ::sinf(0.5 * arg) : ::cosf(0.5 * arg);
+  fact *= fact;
+  for (int j = 0; j < nn / 2; j++) {
+    const float ss = ::sinf(pi * (2 * j + 1) / (2 * nn)) * sinw;
+    b.den[j][0] = fact / (1. + ss);
+    b.den[j][1] = (1. - ss) / fact;
+  }
+  b.mid = -2. * cosw / fact;
+  return b;
+}
+
 // total[i] += slice_0[i] + slice_1[i] + ... in shot order (deterministic)
 __global__ void sum_slices_kernel(const float *slices, int nb, long long n, float *total) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -982,6 +1090,53 @@ namespace pf {
 
 // residual_weighting with oreo=false as fwic sets it up (wave_fwiutil.c:225-296,
 // pfwi.c:849-855): 1 inside, 10-sample sine tapers on both axes.  [nr][nt].
+// residual_weighting (wave_fwiutil.c:225-296), both branches; w [nr][nt].
+// Taper samples that would fall outside the array (a window closer than 10
+// samples to its edge, where the reference writes out of bounds) are skipped.
+static void weights_window(int nt, int nr, int wtn1, int wtn2, int woffn1, int woffn2, bool oreo,
+                           float *w) {
+  float sn[10];
+  for (int i = 0; i < 10; i++) sn[i] = sinf(0.5 * M_PI * (i + 1) / 11.);
+  float sink = 0.f;
+  auto W = [&](int ir, int it) -> float & {
+    return (ir >= 0 && ir < nr && it >= 0 && it < nt) ? w[(size_t)ir * nt + it] : sink;
+  };
+  if (oreo) {
+    for (size_t i = 0; i < (size_t)nr * nt; i++) w[i] = 1.f;
+    for (int ir = woffn1; ir <= woffn2; ir++)
+      for (int it = wtn1; it <= wtn2; it++) W(ir, it) = 0.f;
+    for (int ir = 0; ir < 10; ir++)
+      for (int it = wtn1; it <= wtn2; it++) {
+        if (woffn1 - ir > 0) W(woffn1 - ir, it) *= sn[ir];
+        if (woffn2 + ir < nr) W(woffn2 + ir, it) *= sn[ir];
+      }
+    for (int it = 0; it < 10; it++) {
+      for (int ir = 0; ir < woffn1; ir++) {
+        W(ir, wtn1 + it) *= sn[it];
+        W(ir, wtn2 - it) *= sn[it];
+      }
+      for (int ir = woffn2 + 1; ir < nr; ir++) {
+        W(ir, wtn1 + it) *= sn[it];
+        W(ir, wtn2 - it) *= sn[it];
+      }
+    }
+    return;
+  }
+  for (size_t i = 0; i < (size_t)nr * nt; i++) w[i] = 0.f;
+  for (int ir = woffn1; ir <= woffn2; ir++)
+    for (int it = wtn1; it <= wtn2; it++) W(ir, it) = 1.f;
+  for (int ir = 0; ir < 10; ir++)
+    for (int it = wtn1; it <= wtn2; it++) {
+      W(woffn1 + ir, it) *= sn[ir];
+      W(woffn2 - ir, it) *= sn[ir];
+    }
+  for (int it = 0; it < 10; it++)
+    for (int ir = woffn1; ir <= woffn2; ir++) {
+      W(ir, wtn1 + it) *= sn[it];
+      W(ir, wtn2 - it) *= sn[it];
+    }
+}
+
 static void residual_weights(const pw_fwi_args &a, int nr, std::vector<float> &w) {
   const int nt = a.nt;
   const float t0 = a.ot, dt = a.dt, r0 = a.ox, dr = a.dx;
@@ -989,22 +1144,8 @@ static void residual_weights(const pw_fwi_args &a, int nr, std::vector<float> &w
   const float woff1 = r0, woff2 = r0 + (nr - 1) * dr;
   const int wtn1 = (int)((wt1 - t0) / dt + 0.5), wtn2 = (int)((wt2 - t0) / dt + 0.5);
   const int woffn1 = (int)((woff1 - r0) / dr + 0.5), woffn2 = (int)((woff2 - r0) / dr + 0.5);
-  float s[10];
-  for (int i = 0; i < 10; i++) s[i] = sinf(0.5 * M_PI * (i + 1) / 11.);
   w.assign((size_t)nr * nt, 0.f);
-  auto W = [&](int ir, int it) -> float & { return w[(size_t)ir * nt + it]; };
-  for (int ir = woffn1; ir <= woffn2; ir++)
-    for (int it = wtn1; it <= wtn2; it++) W(ir, it) = 1.f;
-  for (int ir = 0; ir < 10; ir++)
-    for (int it = wtn1; it <= wtn2; it++) {
-      W(woffn1 + ir, it) *= s[ir];
-      W(woffn2 - ir, it) *= s[ir];
-    }
-  for (int it = 0; it < 10; it++)
-    for (int ir = woffn1; ir <= woffn2; ir++) {
-      W(ir, wtn1 + it) *= s[it];
-      W(ir, wtn2 - it) *= s[it];
-    }
+  weights_window(nt, nr, wtn1, wtn2, woffn1, woffn2, false, w.data());
 }
 
 struct Fields {
@@ -1267,6 +1408,14 @@ static int gradient_impl(const pw_fwi_args *a, int mode, const float *vel, const
   const int nck = exact ? (nt + k - 1) / k : 0;
   std::vector<float> wts;
   if (weight == nullptr) residual_weights(*a, nr, wts);
+  // multiscale residual filter (gradient_pas_init, wave_fwigradient.c:657-658:
+  // soupar's cutoffs times dt, compared in double)
+  const float flo_dt = a->flo * a->dt, fhi_dt = a->fhi * a->dt;
+  const bool use_lo = flo_dt > 0.0001, use_hi = a->fhi > 0.f && fhi_dt < 0.5 - 0.0001;
+  PW_CHECK(!(exact && (use_lo || use_hi)), PW_ERR_VALUE,
+           "the multiscale residual filter applies to the reference-mode gradient only");
+  const ButterCoef blo = use_lo ? butter_coef(false, flo_dt, 3) : ButterCoef{};
+  const ButterCoef bhi = use_hi ? butter_coef(true, fhi_dt, 3) : ButterCoef{};
 
   Carve cv;
   size_t o_V, o_A, o_B, o_geo, o_bz, o_bx, o_wav;
@@ -1412,11 +1561,17 @@ static int gradient_impl(const pw_fwi_args *a, int mode, const float *vel, const
     p.snap = nullptr;
     p.tout = nullptr;
     // ---- residual and FP64 misfit
+    const bool filt = use_lo || use_hi;  // weights applied after the filter
     residual_kernel<<<RESID_BLOCKS, 256, 0, st>>>(dd, at<float>(base, o_dobs) + (size_t)s0 * nt * nr,
-                                                  at<float>(base, o_w), res, nb_, nt, nr,
-                                                  exact ? 1 : 0, dmis);
+                                                  filt ? nullptr : at<float>(base, o_w), res, nb_,
+                                                  nt, nr, exact ? 1 : 0, dmis);
     misfit_sum_kernel<<<1, 32, 0, st>>>(dmis, RESID_BLOCKS);
     PW_CUDA(cudaGetLastError());
+    if (filt) {
+      butter_residual_kernel<<<ceil_div((long long)nb_ * nr, 128), 128, 0, st>>>(
+          blo, bhi, use_lo, use_hi, res, nb_, nt, nr, at<float>(base, o_w));
+      PW_CUDA(cudaGetLastError());
+    }
     p.res = res;
     if (!exact) {
       // ---- backward with gradient_av's imaging (wave_fwigradient.c:201-241)
@@ -1507,6 +1662,41 @@ static int gradient_impl(const pw_fwi_args *a, int mode, const float *vel, const
 }
 }  // namespace pf
 }  // namespace pw
+
+extern "C" int pw_butter_apply(int n, int ntr, int low, float cutoff, int npoles, float *x,
+                               int flags, void *stream) {
+  PW_CHECK(x && n >= 0 && ntr >= 0, PW_ERR_VALUE, "bad arguments");
+  PW_CHECK(npoles >= 1 && npoles <= BUTTER_MAXP, PW_ERR_VALUE, "npoles must be 1..%d", BUTTER_MAXP);
+  if (n == 0 || ntr == 0) return PW_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool host = (flags & PW_HOST_PTRS) != 0;
+  const ButterCoef b = butter_coef(low != 0, cutoff, npoles);
+  const size_t bytes = (size_t)n * ntr * 4;
+  Workspace &ws = Workspace::for_current_device();
+  std::lock_guard<std::mutex> lock(ws.mutex());
+  float *d = x;
+  if (host) {
+    PW_TRY(ws.reserve(bytes));
+    d = reinterpret_cast<float *>(ws.base());
+    PW_TRY(to_device(d, x, bytes, true, st));
+  }
+  butter_traces_kernel<<<ceil_div(ntr, 128), 128, 0, st>>>(b, d, n, ntr);
+  PW_CUDA(cudaGetLastError());
+  if (host) PW_TRY(to_host(x, d, bytes, true, st));
+  PW_CUDA(cudaStreamSynchronize(st));
+  return PW_OK;
+}
+
+extern "C" int pw_residual_weights(int nt, int nr, int wtn1, int wtn2, int woffn1, int woffn2,
+                                   int oreo, float *w) {
+  PW_CHECK(w && nt >= 1 && nr >= 1, PW_ERR_VALUE, "bad arguments");
+  PW_CHECK(0 <= wtn1 && wtn1 <= wtn2 && wtn2 < nt && 0 <= woffn1 && woffn1 <= woffn2 &&
+               woffn2 < nr,
+           PW_ERR_SHAPE, "window [%d,%d] x [%d,%d] must lie in %d x %d", woffn1, woffn2, wtn1,
+           wtn2, nr, nt);
+  weights_window(nt, nr, wtn1, wtn2, woffn1, woffn2, oreo != 0, w);
+  return PW_OK;
+}
 
 extern "C" int pw_pfwi_gradient(const pw_fwi_args *a, int mode, const float *vel, const float *wav,
                                 const float *dobs, const float *weight, float *grad,

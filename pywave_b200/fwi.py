@@ -70,12 +70,15 @@ def gradient(vel, wav, dobs, par, mode="exact", ckpt_k=0, per_shot=False, weight
 
 
 def gradient_passive(vel, src, dobs, par, mode="reference", ckpt_k=0, per_shot=False,
-                     weight=None, hbm_budget=0):
+                     weight=None, hbm_budget=0, flo=0.0, fhi=0.0):
     """The same gradient with distributed sources (pfwi's passive mode 4,
     gradient_pas_av, wave_fwigradient.c:667-870): src (nz, nx, nt, ns)
-    source fields in place of the point source and wavelet."""
+    source fields in place of the point source and wavelet.  flo, fhi (Hz):
+    the multiscale residual filter (3-pole zero-phase Butterworth high- /
+    low-pass, wave_fwigradient.c:767-780), reference mode only; 0 = off."""
     flags = L.PW_HOST_PTRS | (L.PW_PER_SHOT if per_shot else 0)
     a = fwi_args(par, flags, hbm_budget)
+    a.flo, a.fhi = float(flo), float(fhi)
     v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F"))
     sv = np.ascontiguousarray(np.asarray(src, np.float32).flatten(order="F"))  # [ns][nt][nx][nz]
     if sv.size != a.nz * a.nx * a.nt * a.ns:
@@ -134,3 +137,25 @@ if torch is not None:
         """Differentiable misfit (see FwiMisfit); the checkpoints of the exact
         adjoint fit hbm_budget bytes (0: a quarter of the device)."""
         return FwiMisfit.apply(vel, wav, dobs, par, ckpt_k, weight, hbm_budget)
+
+
+def residual_weights(nt, nr, wtn1=None, wtn2=None, woffn1=None, woffn2=None, oreo=False):
+    """residual_weighting (wave_fwiutil.c:225-296) as an (nr, nt) array:
+    the window defaults to the whole record (fwic's and pfwic's set-up)."""
+    w = np.empty((nr, nt), np.float32)
+    L.check(L.lib().pw_residual_weights(nt, nr, 0 if wtn1 is None else wtn1,
+                                        nt - 1 if wtn2 is None else wtn2,
+                                        0 if woffn1 is None else woffn1,
+                                        nr - 1 if woffn2 is None else woffn2, int(oreo),
+                                        L.ptr(w)))
+    return w
+
+
+def butter_apply(x, low, cutoff, npoles=3):
+    """np_butter_apply (wave_butter.c) on the GPU: each row of x (traces
+    [ntr][n]) filtered causally by a Butterworth low- or high-pass of npoles
+    poles at cutoff cycles per sample; returns a new array."""
+    y = np.ascontiguousarray(np.array(x, dtype=np.float32, ndmin=2))
+    L.check(L.lib().pw_butter_apply(y.shape[-1], y.size // y.shape[-1], int(low), float(cutoff),
+                                    int(npoles), L.ptr(y), L.PW_HOST_PTRS, None))
+    return y.reshape(np.shape(x))

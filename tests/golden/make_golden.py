@@ -24,8 +24,9 @@ import sys
 
 import numpy as np
 
-from models import (BIG3D, BIG3D_BAND, BIG3D_TRI_JSNAP, LSTRI, MID, PAS, big3d_velocity, digest,
-                    lstri_case, mid_models, mid_wavelet, pas_case, pfwi_scale_case)
+from models import (BIG3D, BIG3D_BAND, BIG3D_TRI_JSNAP, BUTTER_CASES, LSTRI, MID, PAS, PAS_FHI,
+                    PAS_FLO, WEIGHT_CASE, big3d_velocity, digest, lstri_case, mid_models,
+                    mid_wavelet, pas_case, pfwi_scale_case)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
@@ -61,7 +62,10 @@ def refdrv():
     f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
     L.refdrv_ricker.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, f32p]
     L.refdrv_gradient.argtypes = [f32p, f32p, f32p, f32p, f32p, C.c_int, f32p, f32p]
-    L.refdrv_gradient_pas.argtypes = [f32p, f32p, f32p, f32p, f32p, f32p, C.c_int, f32p, f32p]
+    L.refdrv_gradient_pas.argtypes = [f32p, f32p, f32p, f32p, f32p, f32p, C.c_int, C.c_float,
+                                      C.c_float, f32p, f32p]
+    L.refdrv_butter.argtypes = [C.c_int, C.c_float, C.c_int, C.c_int, f32p]
+    L.refdrv_residual_weights.argtypes = [C.c_int] * 7 + [f32p]
     return L
 
 
@@ -226,17 +230,43 @@ def make_pfwi_pas(R):
     dflat = np.ascontiguousarray(data.flatten(order="F"))  # [ns][nr][nt]
     sflat = np.ascontiguousarray(src.flatten(order="F"))   # [ns][nt][nx][nz]
     g = {}
-    for rect in (1, 3):
+    fhi_off = float(np.float32(0.5) / np.float32(PAS["dt"]))  # pfwic's soupar->fhi
+    for key, rect, flo, fhi in ((1, 1, 0.0, fhi_off), (3, 3, 0.0, fhi_off),
+                                ("ms", 1, PAS_FLO, PAS_FHI)):
         gr = np.zeros(nz * nx, np.float32)
         fc = np.zeros(1, np.float32)
         quiet(R.refdrv_gradient_pas, parr, np.ascontiguousarray(vs.flatten(order="F")), q.copy(),
-              wav.copy(), dflat.copy(), sflat.copy(), rect, gr, fc)
-        g[rect] = (gr.reshape(nz, nx, order="F"), float(fc[0]))
+              wav.copy(), dflat.copy(), sflat.copy(), rect, flo, fhi, gr, fc)
+        g[key] = (gr.reshape(nz, nx, order="F"), float(fc[0]))
     np.savez_compressed(os.path.join(HERE, "pfwi_pas.npz"), vtrue=vt, vstart=vs,
                         src_digest=digest(src), data=data, grad_rect1=g[1][0],
                         grad_rect3=g[3][0], fcost=g[1][1], vinv=vinv,
+                        grad_ms_rect1=g["ms"][0], fcost_ms=g["ms"][1],
+                        flo=np.float32(PAS_FLO), fhi=np.float32(PAS_FHI),
                         ret0_equals_data_flat=np.array_equal(ret0.reshape(-1),
                                                              data.flatten(order="F")))
+
+
+def make_butter(R):
+    """np_butter_apply (wave_butter.c) on seeded noise traces for low- and
+    high-pass filters of 3 to 5 poles, and residual_weighting
+    (wave_fwiutil.c:225-296) in both branches with an inner window."""
+    rng = np.random.default_rng(23)
+    x = rng.standard_normal((4, 300)).astype(np.float32)
+    out = {"x": x}
+    for i, (low, cut, nn) in enumerate(BUTTER_CASES):
+        y = x.copy()
+        for row in y:
+            r = np.ascontiguousarray(row)
+            R.refdrv_butter(low, cut, nn, r.size, r)
+            row[:] = r
+        out["y%d" % i] = y
+    nt, nr, wtn1, wtn2, woffn1, woffn2 = WEIGHT_CASE
+    for oreo in (0, 1):
+        w = np.zeros(nr * nt, np.float32)
+        R.refdrv_residual_weights(nt, nr, wtn1, wtn2, woffn1, woffn2, oreo, w)
+        out["w_oreo%d" % oreo] = w.reshape(nr, nt)
+    np.savez_compressed(os.path.join(HERE, "butter.npz"), **out)
 
 
 class _Recorder:
@@ -331,7 +361,8 @@ def main(names=()):
     R.refdrv_forward.argtypes = [np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")] * 5
     extra = {"afd3d_big": lambda: make_afd3d_big(a3, R), "pfwi_scale": lambda: make_pfwi_scale(R),
              "pfwi_mid": lambda: make_pfwi_mid(pf, R), "dropin": make_dropin,
-             "lstri": make_lstri, "pfwi_pas": lambda: make_pfwi_pas(R)}
+             "lstri": make_lstri, "pfwi_pas": lambda: make_pfwi_pas(R),
+             "butter": lambda: make_butter(R)}
     if names:
         for n in names:
             extra[n]()

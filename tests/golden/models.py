@@ -137,6 +137,12 @@ def lstri_case():
 # ---- passive mode 4 with velocity update (pfwic): 30 x 40, 2 shots ---------
 PAS = dict(nz=30, nx=40, dz=0.01, dx=0.01, oz=0.0, ox=0.0, nt=400, dt=0.001, ot=0.0, ns=2,
            ds=0.1, os=0.05, nb=20, coef=0.005, f0=10.0, acqui_type=1, interval=1, niter=4)
+PAS_FLO, PAS_FHI = 4.0, 25.0  # multiscale cutoffs (Hz) of the filtered passive gradient
+
+# Butterworth cases (low-pass?, cutoff in cycles per sample, poles) and a
+# residual-weighting window (nt, nr, wtn1, wtn2, woffn1, woffn2)
+BUTTER_CASES = [(1, 0.02, 3), (0, 0.004, 3), (1, 0.1, 4), (0, 0.05, 5)]
+WEIGHT_CASE = (120, 50, 10, 100, 12, 40)
 
 
 def pas_case():

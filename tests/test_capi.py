@@ -43,3 +43,21 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "nope.so"))
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _lib.lib()
+
+
+def test_residual_weights_host_entry_matches_reference(golden):
+    """pw_residual_weights (host code, no device) against the reference's
+    residual_weighting in both branches, and the default whole-record window
+    fwic uses."""
+    import sys
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import models as M
+    from pywave_b200 import fwi
+    g = golden("butter")
+    nt, nr, wtn1, wtn2, woffn1, woffn2 = M.WEIGHT_CASE
+    for oreo in (0, 1):
+        w = fwi.residual_weights(nt, nr, wtn1, wtn2, woffn1, woffn2, oreo=bool(oreo))
+        assert np.array_equal(w, g["w_oreo%d" % oreo]), oreo
+    from oracle import oracle as O
+    assert np.array_equal(fwi.residual_weights(80, 30), O.residual_weights(80, 30))

@@ -84,3 +84,30 @@ def test_gradient_pas_av_bit_exact(golden, oracle):
     for rect in (1, 3):
         pp, _ = oracle.pfwi_postprocess(raw, rect=rect)
         assert np.array_equal(pp, g["grad_rect%d" % rect])
+
+
+def test_passive_multiscale_gradient_bit_exact(golden, oracle):
+    """gradient_pas_av with the multiscale residual filter switched on
+    (flo 4 Hz, fhi 25 Hz: 3-pole zero-phase high- and low-pass,
+    wave_fwigradient.c:657-658,767-780) identical to the reference's."""
+    g, vs, src, kw = _pas(golden, oracle)
+    raw, fcost = oracle.pfwi_gradient_pas(vs, src, g["data"], flo=float(g["flo"]),
+                                          fhi=float(g["fhi"]), **kw)
+    assert np.float32(fcost) == np.float32(g["fcost_ms"])
+    pp, _ = oracle.pfwi_postprocess(raw, rect=1)
+    assert np.array_equal(pp, g["grad_ms_rect1"])
+    assert not np.array_equal(pp, g["grad_rect1"])
+
+
+def test_butterworth_and_weights_bit_exact(golden, oracle):
+    """np_butter_init / np_butter_apply (wave_butter.c) for low- and high-pass
+    filters of 3 to 5 poles, and residual_weighting in both branches
+    (wave_fwiutil.c:225-296), identical to the reference's."""
+    g = golden("butter")
+    for i, (low, cut, nn) in enumerate(M.BUTTER_CASES):
+        y = oracle.butter_apply(g["x"], low, cut, nn)
+        assert np.array_equal(y, g["y%d" % i]), (low, cut, nn)
+    nt, nr, wtn1, wtn2, woffn1, woffn2 = M.WEIGHT_CASE
+    for oreo in (0, 1):
+        w = oracle.residual_weights(nt, nr, wtn1, wtn2, woffn1, woffn2, oreo=bool(oreo))
+        assert np.array_equal(w, g["w_oreo%d" % oreo]), oreo

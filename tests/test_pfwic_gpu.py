@@ -110,3 +110,28 @@ def test_pfwi_mode4_fwi_returns(golden, cuda_lib):
     assert np.array_equal(out[0], g["data"].flatten(order="F"))
     assert out[1].shape == (M.PAS["nz"], M.PAS["nx"], 1) and out[2:] == (None, None, None)
     assert rel_l2(out[1][:, :, 0], g["vinv"][:, :, 0]) < 1e-3
+
+
+def test_butterworth_bit_exact_vs_reference(golden, cuda_lib):
+    """pw_butter_apply against the reference's np_butter_init / apply on
+    seeded traces: low- and high-pass, 3 to 5 poles, identical bits."""
+    from pywave_b200 import fwi
+    g = golden("butter")
+    for i, (low, cut, nn) in enumerate(M.BUTTER_CASES):
+        assert np.array_equal(fwi.butter_apply(g["x"], low, cut, nn), g["y%d" % i]), i
+
+
+def test_passive_multiscale_gradient_bit_exact(golden, cuda_lib):
+    """The passive gradient with the multiscale residual filter on (flo 4 Hz,
+    fhi 25 Hz), one shot at a time: identical to the reference's
+    gradient_pas_av after scaling; the exact mode refuses the filter."""
+    from pywave_b200 import _lib as L
+    from pywave_b200 import fwi
+    g, _, vs, src = _case(golden)
+    raw, J = fwi.gradient_passive(vs, src, g["data"], M.PAS, mode="reference", per_shot=True,
+                                  flo=float(g["flo"]), fhi=float(g["fhi"]))
+    pp, _ = fwi.postprocess(raw, rect=1)
+    assert np.array_equal(pp, g["grad_ms_rect1"])
+    assert abs(J - float(g["fcost_ms"])) <= 1e-4 * abs(J)
+    with pytest.raises(L.ShapeError):
+        fwi.gradient_passive(vs, src, g["data"], M.PAS, mode="exact", flo=4.0)
