@@ -262,6 +262,19 @@ int pw_fwi(const pw_fwi_args *a, const float *vel0, const float *wav, const floa
 int pw_pfwi_passive(const pw_fwi_args *a, const float *vel0, const float *src, const float *dobs,
                     float *vinv, int *iters_done, void *stream);
 
+/* ------------------------------------------------- pseudo-spectral --- */
+
+/* Forward modelling or time reversal with the pseudo-spectral method: the
+ * reference's apscfun.aps2dc / aps3dc (pywave/src/aps.c:315, :22) and the
+ * time loops of psm2d / psm (wave_psp.c:367-635, 25-352).  Arguments exactly
+ * as pw_afd's (the two modules share their argument tuples and outputs);
+ * the Laplacian is -(2 pi |k|)^2 applied through cuFFT on the reference's
+ * FFT-padded grid with its centring, so results agree with the reference to
+ * float rounding (its KISS FFT rounds differently), not bit for bit.  No
+ * stability check (the reference has none). */
+int pw_aps(const pw_afd_args *a, const float *vel, const float *src, const float *wavelet,
+           float *dat, float *wfd, void *stream);
+
 /* ---------------------------------------------- pfwi mode 4: LS-TRI --- */
 
 /* pfwi's passive mode 4 without velocity update (pfwicfun.lstric,

@@ -493,3 +493,110 @@ def lstri(inv, vel, par, src=None, data=None, precision="f32"):
     if inv:
         return s.transpose(3, 2, 1, 0), iters
     return d.transpose(2, 1, 0), iters
+
+
+# --------------------------------------------------------------------------
+# pseudo-spectral propagator psm2d / psm (wave_psp.c:25-635, aps.c glue),
+# restated in FP64 with numpy's FFT (the reference runs KISS FFT in float)
+# --------------------------------------------------------------------------
+
+def psm(vel, nt, dt, d, nbt=30, ct=0.01, src=None, tri=False, dat=None, jsnap=0, rick=None):
+    """aps2d / aps3d in FP64: vel (nz,nx) or (nz,nx,ny), d (dz,dx[,dy]).
+    The expanded grid (nbt cells on every face, edge-replicated velocity) is
+    padded for the FFT to nz2 = 2*next_fast((nz+1)/2), nx2 = next_fast(nx),
+    ny2 = next_fast(ny).  Per step: wave = sign * IFFT(lapl * FFT(sign *
+    curr)) with sign = (-1)^(ix [+ iy]) (the reference's FFT centering) and
+    lapl = -(2 pi |k|)^2 on the centred grid kx = -0.5/dx + ix/(nx2 dx),
+    kz = iz/(nz2 dz); then curr' = 2 curr - prev + wave vv on the expanded
+    grid, the 3x3(x3) source spread (or, time-reversed, the traces on row
+    nbt), the taper on curr and prev (abc_apply over the padded grid, bottom
+    and right faces counted from the padded size), traces and snapshots.
+    Returns (traces, snapshots) shaped as oracle.afd returns them."""
+    vel = np.asarray(vel, np.float64)
+    dim = vel.ndim
+    if dim == 2:
+        vel = vel[:, :, None]
+        dz, dx = d
+        dy = 1.0
+    else:
+        dz, dx, dy = d
+    nz1, nx1, ny1 = vel.shape
+    nb = nbt
+    nby = nb if dim == 3 else 0
+    nz, nx, ny = nz1 + 2 * nb, nx1 + 2 * nb, ny1 + 2 * nby
+    ez = np.clip(np.arange(nz) - nb, 0, nz1 - 1)
+    ex = np.clip(np.arange(nx) - nb, 0, nx1 - 1)
+    ey = np.clip(np.arange(ny) - nby, 0, ny1 - 1)
+    ve = vel[np.ix_(ez, ex, ey)]
+    vv = ve * ve * dt * dt
+    nz2 = 2 * next_fast((nz + 1) // 2)
+    nx2 = next_fast(nx)
+    ny2 = next_fast(ny) if dim == 3 else 1
+    kz = np.arange(nz2 // 2 + 1) / (nz2 * dz)
+    kx = -0.5 / dx + np.arange(nx2) / (nx2 * dx)
+    ky = (-0.5 / dy + np.arange(ny2) / (ny2 * dy)) if dim == 3 else np.zeros(1)
+    K = np.sqrt(kz[:, None, None] ** 2 + kx[None, :, None] ** 2 + ky[None, None, :] ** 2)
+    lapl = -(2 * np.pi * K) ** 2
+    sign = ((-1.0) ** (np.arange(nx2)[:, None] + np.arange(ny2)[None, :]))[None, :, :]
+    w = np.exp(-(ct ** 2) * (nb - 1 - np.arange(nb)) ** 2) if nb else np.zeros(0)
+
+    def taper(a):
+        for ib in range(nb):
+            a[ib, :, :] *= w[ib]
+            a[nz2 - 1 - ib, :, :] *= w[ib]
+        for ib in range(nb):
+            a[:, ib, :] *= w[ib]
+            a[:, nx2 - 1 - ib, :] *= w[ib]
+        if dim == 3:
+            for ib in range(nb):
+                a[:, :, ib] *= w[ib]
+                a[:, :, ny2 - 1 - ib] *= w[ib]
+
+    axes = (1, 2) if dim == 3 else (1,)
+    curr = np.zeros((nz2, nx2, ny2))
+    prev = np.zeros((nz2, nx2, ny2))
+    ntsnap = _ntsnap(nt, jsnap)
+    snaps = np.zeros((nz1, nx1, ny1, max(ntsnap, 1)))
+    traces = np.zeros((nt, nx1, ny1))
+    if tri:
+        dd = np.asarray(dat, np.float64).reshape(nt, nx1, ny1)
+        steps = range(nt - 1, -1, -1)
+    else:
+        sx = np.asarray(src["sx"]).astype(np.float32).astype(int)
+        sz = np.asarray(src["sz"]).astype(np.float32).astype(int)
+        sy = np.asarray(src.get("sy", np.zeros_like(sx))).astype(np.float32).astype(int)
+        if rick is None:
+            rick = np.stack([ricker(nt, dt, src["f"][i], src["t"][i], src["A"][i])
+                             for i in range(len(sx))])
+        steps = range(nt)
+    for it in steps:
+        spec = np.fft.rfft(curr * sign, axis=0)
+        for ax in axes:
+            spec = np.fft.fft(spec, axis=ax)
+        spec = spec * lapl
+        for ax in axes:
+            spec = np.fft.ifft(spec, axis=ax)
+        wave = np.fft.irfft(spec, n=nz2, axis=0).real * sign
+        c = curr[:nz, :nx, :ny]
+        new = c + (c - prev[:nz, :nx, :ny]) + wave[:nz, :nx, :ny] * vv
+        prev[:nz, :nx, :ny] = c
+        curr[:nz, :nx, :ny] = new
+        if tri:
+            curr[nb, nb:nb + nx1, nby:nby + ny1] += vv[nb, nb:nb + nx1, nby:nby + ny1] * dd[it]
+        else:
+            for i in range(len(sx)):
+                for jy in ((-1, 0, 1) if dim == 3 else (0,)):
+                    for jx in (-1, 0, 1):
+                        for jz in (-1, 0, 1):
+                            z_, x_, y_ = sz[i] + nb + jz, sx[i] + nb + jx, sy[i] + nby + jy
+                            den = abs(jx) + abs(jz) + abs(jy) + 1
+                            curr[z_, x_, y_] += vv[z_, x_, y_] * rick[i][it] / den
+        taper(curr)
+        taper(prev)
+        if not tri:
+            traces[it] = curr[nb, nb:nb + nx1, nby:nby + ny1]
+        if jsnap > 0 and it % jsnap == 0:
+            snaps[..., it // jsnap] = curr[nb:nb + nz1, nb:nb + nx1, nby:nby + ny1]
+    if dim == 2:
+        traces, snaps = traces[:, :, 0], snaps[:, :, 0, :]
+    return (None if tri else traces), (snaps if ntsnap > 0 else None)

@@ -21,6 +21,13 @@ def afd2d(vel, nt=1501, dt=0.001, ax=[0, 20, 81], az=[0, 20, 81], ns=2, sx=[30, 
           ps=True, tri=False, dat=None, verb=True, gz=0, wavelet=None):
     """2-D acoustic finite-difference modelling (tri=False) or time-reversal
     propagation of ``dat`` (tri=True), as pywave.afd2d.  vel: [nz, nx]."""
+    return _model2d(afd2dc, vel, nt, dt, ax, az, ns, sx, sz, f, t, A, nbt, ct, jsnap, abc,
+                    ifsnaps, tri, dat, verb, gz, wavelet)
+
+
+def _model2d(cfun, vel, nt, dt, ax, az, ns, sx, sz, f, t, A, nbt, ct, jsnap, abc, ifsnaps, tri,
+             dat, verb, gz, wavelet):
+    # the body of pywave's afd2d.py / aps2d.py around their C call
     vel = np.asarray(vel).flatten(order="F").astype(np.float32)
     ox, dx, nx = ax
     oz, dz, nz = az
@@ -31,8 +38,8 @@ def afd2d(vel, nt=1501, dt=0.001, ax=[0, 20, 81], az=[0, 20, 81], ns=2, sx=[30, 
     else:
         source = np.concatenate([np.array(sx), np.array(sz), np.array(f), np.array(t),
                                  np.array(A)], axis=0, dtype="float32")
-    dout = afd2dc(vel, source, 1 if tri else 0, nt, nx, nz, ns, verb, jsnap, ifsnaps, abc, nbt,
-                  ct, dt, ox, dx, oz, dz, gz=gz, wavelet=wavelet)
+    dout = cfun(vel, source, 1 if tri else 0, nt, nx, nz, ns, verb, jsnap, ifsnaps, abc, nbt,
+                ct, dt, ox, dx, oz, dz, gz=gz, wavelet=wavelet)
     if jsnap > 0:
         ntsnap = _ntsnap(nt, jsnap)
         wfd = dout[nt * nx:].reshape(nz, nx, ntsnap, order="F")
@@ -47,6 +54,13 @@ def afd3d(vel, nt=1501, dt=0.001, ax=[0, 20, 81], ay=[0, 20, 81], az=[0, 20, 81]
           dat=None, verb=True, gz=0, wavelet=None):
     """3-D acoustic finite-difference modelling / time reversal, as
     pywave.afd3d.  vel: [nz, nx, ny]."""
+    return _model3d(afd3dc, vel, nt, dt, ax, ay, az, ns, sx, sy, sz, f, t, A, nbt, ct, jsnap,
+                    abc, ifsnaps, tri, dat, verb, gz, wavelet)
+
+
+def _model3d(cfun, vel, nt, dt, ax, ay, az, ns, sx, sy, sz, f, t, A, nbt, ct, jsnap, abc, ifsnaps,
+             tri, dat, verb, gz, wavelet):
+    # the body of pywave's afd3d.py / aps3d.py around their C call
     vel = np.asarray(vel).flatten(order="F").astype(np.float32)
     ox, dx, nx = ax
     oy, dy, ny = ay
@@ -58,8 +72,8 @@ def afd3d(vel, nt=1501, dt=0.001, ax=[0, 20, 81], ay=[0, 20, 81], az=[0, 20, 81]
     else:
         source = np.concatenate([np.array(sx), np.array(sy), np.array(sz), np.array(f),
                                  np.array(t), np.array(A)], axis=0, dtype="float32")
-    dout = afd3dc(vel, source, 1 if tri else 0, nt, nx, ny, nz, ns, verb, jsnap, ifsnaps, abc,
-                  nbt, ct, dt, ox, dx, oy, dy, oz, dz, gz=gz, wavelet=wavelet)
+    dout = cfun(vel, source, 1 if tri else 0, nt, nx, ny, nz, ns, verb, jsnap, ifsnaps, abc,
+                nbt, ct, dt, ox, dx, oy, dy, oz, dz, gz=gz, wavelet=wavelet)
     if jsnap > 0:
         ntsnap = _ntsnap(nt, jsnap)
         wfd = dout[nt * nx * ny:].reshape(nz, nx, ny, ntsnap, order="F")

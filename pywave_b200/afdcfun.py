@@ -25,7 +25,7 @@ def _ntsnap(nt, jsnap):
 
 
 def _run(dim, vel, source, tri, nt, nx, ny, nz, ns, jsnap, nbt, ct, dt, dx, dy, dz,
-         gz=0, wavelet=None):
+         gz=0, wavelet=None, entry="pw_afd"):
     vel = L.f32(vel).reshape(-1)
     if vel.size != nz * nx * ny:
         raise L.ShapeError(L.PW_ERR_SHAPE,
@@ -49,7 +49,8 @@ def _run(dim, vel, source, tri, nt, nx, ny, nz, ns, jsnap, nbt, ct, dt, dx, dy, 
         dat = out[:nt * nx * ny]
     wfd = out[nt * nx * ny:] if ntsnap > 0 else None
     wav = None if wavelet is None else L.f32(wavelet).reshape(-1)
-    L.check(L.lib().pw_afd(a, L.ptr(vel), L.ptr(source), L.ptr(wav), L.ptr(dat), L.ptr(wfd), None))
+    fn = getattr(L.lib(), entry)
+    L.check(fn(a, L.ptr(vel), L.ptr(source), L.ptr(wav), L.ptr(dat), L.ptr(wfd), None))
     return out
 
 

@@ -19,6 +19,7 @@ LIB = os.path.join(HERE, "libpywave_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
          "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
+LIBS = ["-lcufft"]  # the pseudo-spectral propagator's FFTs (psm.cu)
 
 
 def sources():
@@ -44,7 +45,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         t = os.path.getmtime(LIB)
         if all(os.path.getmtime(d) <= t for d in deps):
             return LIB
-    cmd = [nvcc()] + ARCH + FLAGS + ["-I" + os.path.join(ROOT, "include"), "-o", LIB + ".tmp"] + srcs
+    cmd = ([nvcc()] + ARCH + FLAGS + ["-I" + os.path.join(ROOT, "include"), "-o", LIB + ".tmp"]
+           + srcs + LIBS)
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)

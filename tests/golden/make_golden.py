@@ -24,6 +24,7 @@ import sys
 
 import numpy as np
 
+from models import (APS2, APS3, aps2_velocity, aps3_velocity)
 from models import (BIG3D, BIG3D_BAND, BIG3D_TRI_JSNAP, BUTTER_CASES, LSTRI, MID, PAS, PAS_FHI,
                     PAS_FLO, WEIGHT_CASE, big3d_velocity, digest, lstri_case, mid_models,
                     mid_wavelet, pas_case, pfwi_scale_case)
@@ -269,6 +270,25 @@ def make_butter(R):
     np.savez_compressed(os.path.join(HERE, "butter.npz"), **out)
 
 
+def make_aps():
+    """The reference's pseudo-spectral propagator (apscfun, aps.c ->
+    psm2d / psm, wave_psp.c:25-635) through its unmodified aps2d.py /
+    aps3d.py: 2-D forward modelling with snapshots, 2-D time reversal of
+    one half of the traces, 3-D forward modelling."""
+    a2 = load("aps2d")
+    a3 = load("aps3d")
+    v2 = aps2_velocity()
+    d2, w2 = quiet(a2.aps2d, v2, ifsnaps=True, verb=False, **APS2)
+    dt_ = np.zeros_like(d2)
+    dt_[:, :30] = d2[:, :30]
+    kw = {k: APS2[k] for k in ("nt", "dt", "ax", "az", "nbt", "ct", "jsnap")}
+    _, wt = quiet(a2.aps2d, v2, tri=True, dat=dt_, ifsnaps=True, verb=False, **kw)
+    v3 = aps3_velocity()
+    d3, w3 = quiet(a3.aps3d, v3, ifsnaps=True, verb=False, **APS3)
+    np.savez_compressed(os.path.join(HERE, "aps.npz"), v2=v2, d2=d2, w2=w2, dtri=dt_, wtri=wt,
+                        v3=v3, d3=d3, w3=w3)
+
+
 class _Recorder:
     """Stands in for an extension module: records each call's arguments and
     returns the real module's result."""
@@ -362,7 +382,7 @@ def main(names=()):
     extra = {"afd3d_big": lambda: make_afd3d_big(a3, R), "pfwi_scale": lambda: make_pfwi_scale(R),
              "pfwi_mid": lambda: make_pfwi_mid(pf, R), "dropin": make_dropin,
              "lstri": make_lstri, "pfwi_pas": lambda: make_pfwi_pas(R),
-             "butter": lambda: make_butter(R)}
+             "butter": lambda: make_butter(R), "aps": make_aps}
     if names:
         for n in names:
             extra[n]()

@@ -167,3 +167,27 @@ def pas_case():
             a = (np.pi * 15.0 * (t - float(rng.uniform(0.05, 0.12)))) ** 2
             src[jz, jx, :, s] += (1e6 * (1 - 2 * a) * np.exp(-a)).astype(np.float32)
     return vt, vs, src
+
+
+# ---- pseudo-spectral aps2d / aps3d (apscfun) ------------------------------
+APS2 = dict(nt=300, dt=0.001, ax=[0, 10, 60], az=[0, 10, 40], ns=2, sx=[20, 40], sz=[10, 15],
+            f=[20, 20], t=[0.05, 0.08], A=[1, 2], nbt=20, ct=0.01, jsnap=10)
+APS3 = dict(nt=120, dt=0.001, ax=[0, 10, 24], ay=[0, 10, 22], az=[0, 10, 20], ns=2, sx=[8, 15],
+            sy=[9, 12], sz=[6, 10], f=[25, 25], t=[0.04, 0.06], A=[1, 2], nbt=8, ct=0.02,
+            jsnap=10)
+
+
+def aps2_velocity():
+    """40 x 60: 2000 m/s over 2500 m/s at depth 20 with a seeded 3% texture."""
+    rng = np.random.default_rng(31)
+    v = np.full((40, 60), 2000.0, np.float32)
+    v[20:] = 2500.0
+    return (v * (1.0 + 0.03 * rng.random(v.shape))).astype(np.float32)
+
+
+def aps3_velocity():
+    """20 x 24 x 22: linear 1800 -> 2400 m/s with depth plus a seeded 3% texture."""
+    rng = np.random.default_rng(32)
+    z = np.arange(20, dtype=np.float32)[:, None, None]
+    v = 1800.0 + 600.0 * z / 20 + np.zeros((20, 24, 22), np.float32)
+    return (v * (1.0 + 0.03 * rng.random(v.shape))).astype(np.float32)
