@@ -48,11 +48,11 @@ def parse():
     p.add_argument("--no-fwi2d", action="store_true",
                    help="tri3d: skip the secondary 2-D FWI gradients/s field")
     p.add_argument("--workload", default="tri3d",
-                   choices=["tri3d", "fwi2d", "batch2d", "c1", "fwi3d", "lstri", "pfwic"],
+                   choices=["tri3d", "fwi2d", "batch2d", "c1", "fwi3d", "lstri", "pfwic", "aps3d"],
                    help="tri3d: the 3-D TRI image (default); fwi2d: 2-D FWI gradients/s; "
                         "batch2d: uneven 2-D forward shots in one batch; c1: one 2-D shot; "
                         "fwi3d: 3-D FWI gradients/s; lstri: pfwi mode 4 source inversion; "
-                        "pfwic: pfwi mode 4 passive FWI gradients/s")
+                        "pfwic: pfwi mode 4 passive FWI gradients/s; aps3d: pseudo-spectral 3-D")
     p.add_argument("--lstri-niter", type=int, default=30, help="lstri: CG iterations per shot")
     p.add_argument("--lstri-nt", type=int, default=3001, help="lstri / pfwic: time samples")
     p.add_argument("--fwi3d-nt", type=int, default=2500, help="fwi3d: time samples")
@@ -1467,6 +1467,173 @@ def run_pfwic(args, world, rank, local):
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks}), flush=True)
 
 
+APS_STEPS = (2, 4)  # reference arm: two step counts per call, their difference excludes set-up
+
+
+def _aps_ref_worker(n, kind):
+    """The reference's aps3dc (oracle/_ref apscfun; kind "port": the FP64
+    restatement) forward-modelling the benchmark model for APS_STEPS[0] and
+    APS_STEPS[1] steps; returns the two walls."""
+    sys.path.insert(0, ROOT)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    vel, pos, f, t = c2_model(n, 1234)
+    t = np.zeros(3) + 0.001  # onsets inside the short runs
+    walls = []
+    for nt_s in APS_STEPS:
+        if kind == "reference":
+            sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+            import apscfun  # the reference's own extension module
+            src = np.concatenate([pos[:, 0], pos[:, 1], pos[:, 2], f, t, np.ones(3)]).astype(
+                np.float32)
+            t0 = time.perf_counter()
+            apscfun.aps3dc(vel.flatten(order="F"), src, 0, nt_s, n, n, n, 3, 0, 0, 0, 1, NBT, CT,
+                           DT, 0.0, H, 0.0, H, 0.0, H)
+        else:
+            from oracle import oracle as O
+            t0 = time.perf_counter()
+            O.psm(vel, nt_s, DT, (H, H, H), NBT, CT,
+                  src=dict(sx=pos[:, 0], sy=pos[:, 1], sz=pos[:, 2], f=f, t=t, A=np.ones(3)))
+        walls.append(time.perf_counter() - t0)
+    return walls[0], walls[1]
+
+
+def _aps_cpu(n, workers):
+    pts = (n + 2 * NBT) ** 3
+    for kind in ("reference", "port"):
+        try:
+            res = pool_map(_aps_ref_worker, [(n, kind)] * workers, timeout_s=900)
+            d = max(r[1] - r[0] for r in res)
+            return pts * (APS_STEPS[1] - APS_STEPS[0]) * workers / d / 1e9, kind, d
+        except Exception:  # noqa: BLE001
+            continue
+    raise RuntimeError("neither the reference nor the port ran")
+
+
+def run_aps3d(args, world, rank, local):
+    """3-D pseudo-spectral forward modelling (aps3d) of the headline's model
+    (201^3 interior at 10 m, nbt 30: 261^3 expanded, 270^3 FFT grid, three
+    seeded Ricker sources, surface traces), nt from --nt."""
+    n, nt = args.n, args.nt
+    pts = (n + 2 * NBT) ** 3
+    nz2 = 2 * int(next_fast_size((n + 2 * NBT + 1) // 2))
+    nx2 = int(next_fast_size(n + 2 * NBT))
+    cfg = {"workload": f"aps3d pseudo-spectral forward {n}^3 h={H:g}m nt={nt} nbt={NBT} "
+                       f"(FFT grid {nz2}x{nx2}x{nx2})", "expanded_points": pts}
+    metric = "Gpt-updates/s (3-D pseudo-spectral, aps3d)"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        workers = max(1, min(os.cpu_count() or 1, 8))
+        rates = []
+        for i in range(args.warmup + args.steps):
+            v, kind, _ = _aps_cpu(n, workers)
+            if i >= args.warmup:
+                rates.append(v)
+        value = statistics.median(rates)
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": value, "unit": "Gpt/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "Gpt/s", "cores": workers, "kind": kind,
+                             "sample": f"aps3dc for {APS_STEPS[0]} and {APS_STEPS[1]} steps per "
+                                       f"process (difference = steps alone), {workers} processes"},
+            "e2e": {"value": value, "unit": "Gpt/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    import torch.distributed as dist
+    from pywave_b200 import _lib as L
+    from pywave_b200 import build as B
+    import pywave_b200 as pw
+    B.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    vel, pos, f, t = c2_model(n, 1234 + rank, nt)
+    src = np.concatenate([pos[:, 0], pos[:, 1], pos[:, 2], f, t, np.ones(3)]).astype(np.float32)
+    a = L.AfdArgs(dim=3, nz=n, nx=n, ny=n, nt=nt, nbt=NBT, ct=CT, dt=DT, dz=H, dx=H, dy=H, ns=3,
+                  tri=0, jsnap=0, gz=0, flags=0)
+    st = torch.cuda.current_stream().cuda_stream
+    vel_d = torch.from_numpy(np.ascontiguousarray(vel.flatten(order="F"))).cuda()
+    src_d = torch.from_numpy(src).cuda()
+    dat = torch.empty(n * n * nt, device="cuda")
+    lib = L.lib()
+
+    def step():
+        L.check(lib.pw_aps(a, vel_d.data_ptr(), src_d.data_ptr(), None, dat.data_ptr(), None, st))
+        return L.last_timing()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches, loops = 0, []
+    e0.record()
+    for _ in range(args.steps):
+        ms_, nst, tot = step()
+        loops.append(ms_)
+        launches += tot
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    loop_ms = statistics.median(loops)
+    # algorithmic bytes per step: R2C reads the real grid and writes the
+    # half spectrum, the multiply reads and writes it, C2R the reverse, the
+    # update reads S, P, F, vv and writes S, P (each transform's own passes
+    # not counted)
+    nre = nz2 * nx2 * nx2
+    ncx = (nz2 // 2 + 1) * nx2 * nx2
+    alg_step = 4.0 * nre + 8.0 * ncx + 16.0 * ncx + 8.0 * ncx + 4.0 * nre + 24.0 * pts
+    peak, peak_kind = peaks()
+    e2e = None
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        d, _ = pw.aps3d(vel, nt=nt, dt=DT, ax=[0, H, n], ay=[0, H, n], az=[0, H, n], ns=3,
+                        sx=list(pos[:, 0]), sy=list(pos[:, 1]), sz=list(pos[:, 2]), f=list(f),
+                        t=list(t), A=[1, 1, 1], nbt=NBT, ct=CT, jsnap=0, verb=False), None
+        wall = time.perf_counter() - t0
+        e2e = {"value": pts * nt / wall / 1e9, "unit": "Gpt/s",
+               "h2d_bytes_per_step": int(vel.nbytes + src.nbytes),
+               "d2h_bytes_per_step": int(4 * n * n * nt)}
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0:
+        v, kind, d = _aps_cpu(n, 1)
+        cpu = {"value": v, "unit": "Gpt/s", "cores": 1, "kind": kind,
+               "sample": f"aps3dc for {APS_STEPS[0]} and {APS_STEPS[1]} steps, one process "
+                         f"(difference = {APS_STEPS[1] - APS_STEPS[0]} steps, {d:.1f} s)"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": job_rate(pts * nt, args.steps, world, ms) / 1e9,
+            "unit": "Gpt/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (cuFFT)",
+            "data": "synthetic (the headline's seeded velocity model and sources)",
+            "config": cfg, "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": alg_step * nt / (loop_ms / 1e3) / 1e9,
+                         "peak": peak, "unit": "GB/s",
+                         "frac": alg_step * nt / (loop_ms / 1e3) / 1e9 / peak, "traffic": None,
+                         "kernel": "cuFFT R2C + lapl multiply + cuFFT C2R + update per step",
+                         "loop_ms": loop_ms, "peak_source": peak_kind},
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks}), flush=True)
+
+
+def next_fast_size(n):
+    while True:
+        m = n
+        for p_ in (2, 3, 5):
+            while m % p_ == 0:
+                m //= p_
+        if m <= 1:
+            return n
+        n += 1
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1484,6 +1651,8 @@ def main():
         return run_lstri(args, world, rank, local)
     if args.workload == "pfwic":
         return run_pfwic(args, world, rank, local)
+    if args.workload == "aps3d":
+        return run_aps3d(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, rank)
 

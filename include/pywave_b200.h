@@ -326,7 +326,8 @@ int pw_residual_weights(int nt, int nr, int wtn1, int wtn2, int woffn1, int woff
 
 const char *pw_last_error(void);
 const char *pw_version(void);
-/* Releases the calling device's cached device memory. */
+/* Releases the calling device's cached device memory: the workspace and
+ * the cached cuFFT plans of pw_aps. */
 int pw_release_cache(void);
 /* Device time of the calling thread's last completed call: the time loop
  * alone (CUDA events recorded on the call's stream around its step kernels),

@@ -210,6 +210,8 @@ extern "C" int pw_last_timing(double *loop_ms, long long *step_launches,
 extern "C" int pw_release_cache(void) {
   auto &ws = pw::Workspace::for_current_device();
   std::lock_guard<std::mutex> g(ws.mutex());
+  cudaDeviceSynchronize();
+  pw::release_fft_plans();
   ws.release();
   return PW_OK;
 }

@@ -121,6 +121,10 @@ class LoopTimer {
   cudaEvent_t a_ = nullptr, b_ = nullptr;
 };
 
+// Destroys the calling device's cached cuFFT plans (psm.cu); the caller
+// holds the device's workspace lock.
+void release_fft_plans();
+
 // Copy helper honouring PW_HOST_PTRS.
 int to_device(void *dst, const void *src, size_t bytes, bool host, cudaStream_t s);
 int to_host(void *dst, const void *src, size_t bytes, bool host, cudaStream_t s);
