@@ -193,6 +193,21 @@ int pw_pfwi_gradient_passive(const pw_fwi_args *a, int mode, const float *vel, c
                              const float *dobs, const float *weight, float *grad, double *misfit,
                              int ckpt_k, void *stream);
 
+/* Visco-acoustic pfwi (media 2), which the reference implements but its
+ * Python glue never reaches (pfwi.c:864 always takes the acoustic path):
+ * the pfwi scheme with a memory variable whose relaxation times come from
+ * the quality factor q [nx][nz] and a->f0 (preparation, wave_fwiutil.c:90-96).
+ * pw_pfwi_forward_visco: forward_modeling (wave_fwimodeling.c:116-220),
+ * data [ns][nr][nt].  pw_pfwi_gradient_visco: gradient_v
+ * (wave_fwigradient.c:264-452) before its post-processing, shots summed in
+ * the reference's order; weight, grad, misfit as pw_pfwi_gradient's
+ * REFERENCE mode.  Source maps must stay clear of the grid's 4-cell rim. */
+int pw_pfwi_forward_visco(const pw_fwi_args *a, const float *vel, const float *q,
+                          const float *wav, float *data, void *stream);
+int pw_pfwi_gradient_visco(const pw_fwi_args *a, const float *vel, const float *q,
+                           const float *wav, const float *dobs, const float *weight, float *grad,
+                           double *misfit, void *stream);
+
 /* Checkpoint plan of the calling thread's last PW_GRAD_EXACT gradient: the
  * interval k, the shots per batch, the device bytes the call held and the
  * recompute factor (forward steps run / nt; 1 = nothing recomputed).  The

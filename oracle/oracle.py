@@ -87,6 +87,14 @@ def lib():
                           + [C.c_int, C.c_int, _i32p, _i32p, _i32p, C.c_int, C.c_int]
                           + [rp, rp, rp, rp, rp, C.c_float, C.c_float])
             f.restype = real
+            f = getattr(L, "or_pfwi_forward_visco_" + sfx)
+            f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 3 + geo
+                          + [rp, rp, rp, rp])
+            f.restype = None
+            f = getattr(L, "or_pfwi_gradient_visco_" + sfx)
+            f.argtypes = ([C.c_int] * 3 + [C.c_float] * 2 + [C.c_int] + [C.c_float] * 3 + [C.c_int]
+                          + geo + [rp, rp, rp, rp, rp, rp])
+            f.restype = real
             f = getattr(L, "or_butter_apply_" + sfx)
             f.argtypes = [C.c_int, C.c_float, C.c_int, C.c_int, rp]
             f.restype = None
@@ -320,6 +328,40 @@ def pfwi_gradient_ref(vel, wav, dobs, nb, coef, dz, dx, dt, geo, ns, interval=1,
     g = np.zeros(nz * nx, R)
     f = getattr(lib(), "or_pfwi_gradient_ref_" + precision)(
         nz, nx, nb, dz, dx, nt, dt, coef, interval, *_geo_args(geo, ns), v, w,
+        _dobs_flat(dobs, R), np.ascontiguousarray(np.asarray(weight, np.float32).astype(R)), g)
+    return g.reshape(nz, nx, order="F"), float(f)
+
+
+def pfwi_forward_visco(vel, q, wav, nb, coef, dz, dx, dt, f0, geo, ns, precision="f32"):
+    """Visco-acoustic forward_modeling (wave_fwimodeling.c:116); vel, q
+    (nz, nx); returns data (nt, nr, ns)."""
+    R = np.float32 if precision == "f32" else np.float64
+    nz, nx = vel.shape
+    nt = len(wav)
+    v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F").astype(R))
+    qq = np.ascontiguousarray(np.asarray(q, np.float32).flatten(order="F").astype(R))
+    w = np.ascontiguousarray(np.asarray(wav, np.float32).astype(R))
+    out = np.zeros(ns * geo["nr"] * nt, R)
+    getattr(lib(), "or_pfwi_forward_visco_" + precision)(nz, nx, nb, dz, dx, nt, dt, coef, f0,
+                                                         *_geo_args(geo, ns), v, qq, w, out)
+    return out.reshape(nt, geo["nr"], ns, order="F")
+
+
+def pfwi_gradient_visco(vel, q, wav, dobs, nb, coef, dz, dx, dt, f0, geo, ns, interval=1,
+                        weight=None, precision="f32"):
+    """gradient_v (wave_fwigradient.c:264) before scaling / smoothing.
+    Returns (grad (nz, nx), fcost)."""
+    R = np.float32 if precision == "f32" else np.float64
+    nz, nx = vel.shape
+    nt = len(wav)
+    if weight is None:
+        weight = residual_weights(nt, geo["nr"])
+    v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F").astype(R))
+    qq = np.ascontiguousarray(np.asarray(q, np.float32).flatten(order="F").astype(R))
+    w = np.ascontiguousarray(np.asarray(wav, np.float32).astype(R))
+    g = np.zeros(nz * nx, R)
+    f = getattr(lib(), "or_pfwi_gradient_visco_" + precision)(
+        nz, nx, nb, dz, dx, nt, dt, coef, f0, interval, *_geo_args(geo, ns), v, qq, w,
         _dobs_flat(dobs, R), np.ascontiguousarray(np.asarray(weight, np.float32).astype(R)), g)
     return g.reshape(nz, nx, order="F"), float(f)
 

@@ -508,6 +508,221 @@ REAL SFX(or_pfwi_gradient_pas)(int nz, int nx, int nb, float dz, float dx, int n
                                  use_lo ? &lo : NULL, use_hi ? &hi : NULL);
 }
 
+/* preparation's attenuation parameters (wave_fwiutil.c:90-96): tmp =
+ * sqrt(q^2+1), taue = (tmp+1)/(2 pi f0 q), taus = (tmp-1)/(2 pi f0 q),
+ * tau = taue/taus - 1; the float instance keeps the reference's float /
+ * double mix. */
+static void SFX(pf_tau)(const REAL *q, size_t n, float f0, REAL *tau, REAL *taus)
+{
+    const double pi = 3.14159265358979323846264338328;
+    for (size_t i = 0; i < n; i++) {
+#if PW_F32
+        float tmp = sqrtf(q[i] * q[i] + 1);
+        float taue = (tmp + 1) / (2. * pi * f0 * q[i]);
+        taus[i] = (tmp - 1) / (2. * pi * f0 * q[i]);
+        tau[i] = taue / taus[i] - 1;
+#else
+        double tmp = sqrt(q[i] * q[i] + 1);
+        double taue = (tmp + 1) / (2. * pi * f0 * q[i]);
+        taus[i] = (tmp - 1) / (2. * pi * f0 * q[i]);
+        tau[i] = taue / taus[i] - 1;
+#endif
+    }
+}
+
+/* One visco-acoustic step of forward_modeling (wave_fwimodeling.c:187-205;
+ * whole padded grid, term persisting where laplace does not write) or of
+ * gradient_v's forward pass (wave_fwigradient.c:334-345; [4, pad-4) only):
+ * memory variable r2 from term and r1, term corrected, then the pfwi
+ * update; rotate p and r; sponge p0, p1, r1. */
+static void SFX(pf_visco_step)(REAL **p0, REAL **p1, REAL **p2, REAL **r1, REAL **r2,
+                               REAL *term, const REAL *vp, const REAL *tau, const REAL *taus,
+                               const REAL *rr, REAL wv, REAL dt2, REAL idt, const REAL *bc,
+                               int pnx, int pnz, int nb, int inner)
+{
+    const int lo = inner ? 4 : 0;
+    for (int ix = lo; ix < pnx - lo; ix++)
+        for (int iz = lo; iz < pnz - lo; iz++) {
+            size_t j = (size_t)ix * pnz + iz;
+            (*r2)[j] = (tau[j] / taus[j] * term[j] + (idt - 0.5 / taus[j]) * (*r1)[j]) /
+                       (idt + 0.5 / taus[j]);
+            term[j] = term[j] * (1. + tau[j]) - ((*r2)[j] + (*r1)[j]) * 0.5 + rr[j] * wv;
+            (*p2)[j] = 2 * (*p1)[j] - (*p0)[j] + vp[j] * vp[j] * dt2 * term[j];
+        }
+    REAL *t = *p0; *p0 = *p1; *p1 = *p2; *p2 = t;
+    t = *r1; *r1 = *r2; *r2 = t;
+    SFX(pf_apply_sponge)(*p0, bc, pnx, pnz, nb);
+    SFX(pf_apply_sponge)(*p1, bc, pnx, pnz, nb);
+    SFX(pf_apply_sponge)(*r1, bc, pnx, pnz, nb);
+}
+
+/* forward_modeling, visco-acoustic (wave_fwimodeling.c:116-220); q [nx][nz]
+ * quality factor, f0 reference frequency; other arguments as
+ * or_pfwi_forward. */
+void SFX(or_pfwi_forward_visco)(int nz, int nx, int nb, float dz, float dx, int nt, float dt,
+                                float coef, float f0, int ns, const int *sx, int sz, int nr,
+                                const int *r0v, const int *r02, const int *nr2, int drv, int rz,
+                                const REAL *vel, const REAL *q, const REAL *wav, REAL *data)
+{
+    const int pnz = nz + 2 * nb, pnx = nx + 2 * nb;
+    const size_t np = (size_t)pnz * pnx, nzx = (size_t)nz * nx;
+    REAL *vp = (REAL *)calloc(np, sizeof(REAL)), *rr = (REAL *)calloc(np, sizeof(REAL));
+    REAL *tp = (REAL *)calloc(np, sizeof(REAL)), *tsp = (REAL *)calloc(np, sizeof(REAL));
+    REAL *t1 = (REAL *)calloc(nzx, sizeof(REAL)), *ts1 = (REAL *)calloc(nzx, sizeof(REAL));
+    REAL *buf[5], *term = (REAL *)calloc(np, sizeof(REAL));
+    for (int i = 0; i < 5; i++) buf[i] = (REAL *)calloc(np, sizeof(REAL));
+    REAL *bc = (REAL *)calloc(nb > 0 ? nb : 1, sizeof(REAL));
+    const REAL dx2 = (REAL)dx * dx, dz2 = (REAL)dz * dz, dt2 = (REAL)dt * dt;
+#if PW_F32
+    const float idt = 1. / dt;
+#else
+    const double idt = 1. / (double)dt;
+#endif
+    SFX(pf_sponge_table)(nb, coef, bc);
+    SFX(pf_pad)(vel, vp, nz, nx, nb);
+    SFX(pf_tau)(q, nzx, f0, t1, ts1);
+    SFX(pf_pad)(t1, tp, nz, nx, nb);
+    SFX(pf_pad)(ts1, tsp, nz, nx, nb);
+    for (int is = 0; is < ns; is++) {
+        REAL *p0 = buf[0], *p1 = buf[1], *p2 = buf[2], *r1 = buf[3], *r2 = buf[4];
+        for (int i = 0; i < 5; i++) memset(buf[i], 0, np * sizeof(REAL));
+        REAL *dd = data + (size_t)is * nr * nt;
+        memset(dd, 0, (size_t)nr * nt * sizeof(REAL));
+        SFX(pf_source_map)(sx[is], sz, pnx, pnz, rr);
+        for (int it = 0; it < nt; it++) {
+            for (int ir = 0; ir < nr2[is]; ir++) {
+                int rx = r0v[is] + ir * drv;
+                dd[(size_t)(r02[is] + ir) * nt + it] = p1[(size_t)rx * pnz + rz];
+            }
+            SFX(pf_laplace)(p1, term, pnx, pnz, dx2, dz2);
+            SFX(pf_visco_step)(&p0, &p1, &p2, &r1, &r2, term, vp, tp, tsp, rr, wav[it], dt2, idt,
+                               bc, pnx, pnz, nb, 0);
+        }
+    }
+    for (int i = 0; i < 5; i++) free(buf[i]);
+    free(vp); free(rr); free(tp); free(tsp); free(t1); free(ts1); free(term); free(bc);
+}
+
+/* gradient_v (wave_fwigradient.c:264-452), raw: before the first-call
+ * scaling and gradient_smooth2.  Forward: pf_visco_step on [4, pad-4) with
+ * snapshots; residual and misfit as gradient_av; backward: r2 and tmp =
+ * p1 (1 + tau) - 0.5 (r2 + r1) from p1 and r1, term = laplace(tmp) plus the
+ * residual, the pfwi update, gradient_av's imaging; rotate; sponge. */
+REAL SFX(or_pfwi_gradient_visco)(int nz, int nx, int nb, float dz, float dx, int nt, float dt,
+                                 float coef, float f0, int interval, int ns, const int *sx, int sz,
+                                 int nr, const int *r0v, const int *r02, const int *nr2, int drv,
+                                 int rz, const REAL *vel, const REAL *q, const REAL *wav,
+                                 const REAL *dobs, const REAL *weight, REAL *grad)
+{
+    const int pnz = nz + 2 * nb, pnx = nx + 2 * nb;
+    const size_t np = (size_t)pnz * pnx, nzx = (size_t)nz * nx;
+    const int wnt = (nt - 1) / interval + 1;
+    REAL *vp = (REAL *)calloc(np, sizeof(REAL)), *rr = (REAL *)calloc(np, sizeof(REAL));
+    REAL *tp = (REAL *)calloc(np, sizeof(REAL)), *tsp = (REAL *)calloc(np, sizeof(REAL));
+    REAL *t1 = (REAL *)calloc(nzx, sizeof(REAL)), *ts1 = (REAL *)calloc(nzx, sizeof(REAL));
+    REAL *buf[5], *term = (REAL *)calloc(np, sizeof(REAL)), *tmp = (REAL *)calloc(np, sizeof(REAL));
+    for (int i = 0; i < 5; i++) buf[i] = (REAL *)calloc(np, sizeof(REAL));
+    REAL *bc = (REAL *)calloc(nb > 0 ? nb : 1, sizeof(REAL));
+    REAL *wave = (REAL *)calloc(nzx * wnt, sizeof(REAL));
+    REAL *pp = (REAL *)calloc((size_t)nr * nt, sizeof(REAL));
+    const REAL dx2 = (REAL)dx * dx, dz2 = (REAL)dz * dz, dt2 = (REAL)dt * dt;
+#if PW_F32
+    const float idt = 1. / dt;
+    float wdt = dt * interval, wdt2 = wdt * wdt;
+    float fcost = 0.;
+#else
+    const double idt = 1. / (double)dt;
+    double wdt = (double)dt * interval, wdt2 = wdt * wdt;
+    double fcost = 0.;
+#endif
+    SFX(pf_sponge_table)(nb, coef, bc);
+    SFX(pf_pad)(vel, vp, nz, nx, nb);
+    SFX(pf_tau)(q, nzx, f0, t1, ts1);
+    SFX(pf_pad)(t1, tp, nz, nx, nb);
+    SFX(pf_pad)(ts1, tsp, nz, nx, nb);
+    memset(grad, 0, nzx * sizeof(REAL));
+    for (int is = 0; is < ns; is++) {
+        REAL *p0 = buf[0], *p1 = buf[1], *p2 = buf[2], *r1 = buf[3], *r2 = buf[4];
+        for (int i = 0; i < 5; i++) memset(buf[i], 0, np * sizeof(REAL));
+        memset(pp, 0, (size_t)nr * nt * sizeof(REAL));
+        memset(term, 0, np * sizeof(REAL));
+        memset(tmp, 0, np * sizeof(REAL));
+        SFX(pf_source_map)(sx[is], sz, pnx, pnz, rr);
+        int wit = 0;
+        for (int it = 0; it < nt; it++) {
+            for (int ir = 0; ir < nr2[is]; ir++) {
+                int rx = r0v[is] + ir * drv;
+                pp[(size_t)(r02[is] + ir) * nt + it] = p1[(size_t)rx * pnz + rz];
+            }
+            if (it % interval == 0) {
+                for (int ix = 0; ix < nx; ix++)
+                    for (int iz = 0; iz < nz; iz++)
+                        wave[(size_t)wit * nzx + (size_t)ix * nz + iz] = p1[(size_t)(ix + nb) * pnz + iz + nb];
+                wit++;
+            }
+            SFX(pf_laplace)(p1, term, pnx, pnz, dx2, dz2);
+            SFX(pf_visco_step)(&p0, &p1, &p2, &r1, &r2, term, vp, tp, tsp, rr, wav[it], dt2, idt,
+                               bc, pnx, pnz, nb, 1);
+        }
+        wit--;
+        const REAL *dd = dobs + (size_t)is * nr * nt;
+        for (int ir = 0; ir < nr; ir++)
+            for (int it = 0; it < nt; it++) {
+                size_t k = (size_t)ir * nt + it;
+                pp[k] = dd[k] - pp[k];
+                fcost += 0.5 * pp[k] * pp[k];
+                pp[k] *= weight[k];
+            }
+        for (int i = 0; i < 5; i++) memset(buf[i], 0, np * sizeof(REAL));
+        p0 = buf[0]; p1 = buf[1]; p2 = buf[2]; r1 = buf[3]; r2 = buf[4];
+        memset(term, 0, np * sizeof(REAL));
+        memset(tmp, 0, np * sizeof(REAL));
+        for (int it = nt - 1; it >= 0; it--) {
+            for (int ix = 4; ix < pnx - 4; ix++)
+                for (int iz = 4; iz < pnz - 4; iz++) {
+                    size_t j = (size_t)ix * pnz + iz;
+                    r2[j] = (-tp[j] / tsp[j] * p1[j] + (-idt + 0.5 / tsp[j]) * r1[j]) /
+                            (-idt - 0.5 / tsp[j]);
+                    tmp[j] = p1[j] * (1. + tp[j]) - 0.5 * (r2[j] + r1[j]);
+                }
+            SFX(pf_laplace)(tmp, term, pnx, pnz, dx2, dz2);
+            for (int ir = 0; ir < nr2[is]; ir++) {
+                int rx = r0v[is] + ir * drv;
+                term[(size_t)rx * pnz + rz] += pp[(size_t)(r02[is] + ir) * nt + it];
+            }
+            for (int ix = 4; ix < pnx - 4; ix++)
+                for (int iz = 4; iz < pnz - 4; iz++) {
+                    size_t j = (size_t)ix * pnz + iz;
+                    p2[j] = 2 * p1[j] - p0[j] + vp[j] * vp[j] * dt2 * term[j];
+                }
+            if (it % interval == 0) {
+                if (wit != wnt - 1 && wit != 0) {
+                    for (int ix = 0; ix < nx; ix++)
+                        for (int iz = 0; iz < nz; iz++) {
+                            size_t k = (size_t)ix * nz + iz;
+                            REAL temp = vp[(size_t)(ix + nb) * pnz + iz + nb];
+                            temp = temp * temp * temp;
+                            temp = -2. / temp;
+                            grad[k] += (wave[(size_t)(wit + 1) * nzx + k] - 2. * wave[(size_t)wit * nzx + k] +
+                                        wave[(size_t)(wit - 1) * nzx + k]) / wdt2 *
+                                       p1[(size_t)(ix + nb) * pnz + iz + nb] * temp;
+                        }
+                }
+                wit--;
+            }
+            REAL *t = p0; p0 = p1; p1 = p2; p2 = t;
+            t = r1; r1 = r2; r2 = t;
+            SFX(pf_apply_sponge)(p0, bc, pnx, pnz, nb);
+            SFX(pf_apply_sponge)(p1, bc, pnx, pnz, nb);
+            SFX(pf_apply_sponge)(r1, bc, pnx, pnz, nb);
+        }
+    }
+    for (int i = 0; i < 5; i++) free(buf[i]);
+    free(vp); free(rr); free(tp); free(tsp); free(t1); free(ts1); free(term); free(tmp); free(bc);
+    free(wave); free(pp);
+    return fcost;
+}
+
 /* Exact discrete adjoint of the pfwi forward scheme.
  *
  * Forward (n = 0..nt-1), a_0 = b_0 = 0, S the sponge, V = v_pad^2 dt^2:

@@ -176,3 +176,49 @@ void refdrv_residual_weights(int nt, int nr, int wtn1, int wtn2, int woffn1, int
     free(ww[0]);
     free(ww);
 }
+
+/* visco-acoustic forward_modeling (wave_fwimodeling.c:116-220): the
+ * memory-variable scheme with tau, taus from q and f0 (preparation,
+ * wave_fwiutil.c:90-96).  data out: [ns][nr=nx][nt]. */
+void refdrv_forward_visco(const float *par, float *vel, float *q, float *wav, float *data)
+{
+    np_sou soupar = (np_sou)np_alloc(1, sizeof(*soupar));
+    np_acqui acpar = (np_acqui)np_alloc(1, sizeof(*acpar));
+    np_vec array = (np_vec)np_alloc(1, sizeof(*array));
+    fill_acpar(acpar, soupar, par);
+    preparation(vel, q, wav, acpar, soupar, array);
+    float ***d = np_floatalloc3(acpar->nt, acpar->nx, acpar->ns);
+    forward_modeling(d, soupar, acpar, array, false);
+    memcpy(data, d[0][0], sizeof(float) * acpar->nt * acpar->nx * acpar->ns);
+}
+
+/* gradient_init + one gradient_v call (wave_fwigradient.c:20-92, 264-452),
+ * set up as refdrv_gradient; output after the first-call scaling and the
+ * caller's smoothing radius. */
+void refdrv_gradient_visco(const float *par, float *vel, float *q, float *wav, float *dobs,
+                           int rect, float *grad, float *fcost)
+{
+    np_sou soupar = (np_sou)np_alloc(1, sizeof(*soupar));
+    np_acqui acpar = (np_acqui)np_alloc(1, sizeof(*acpar));
+    np_vec array = (np_vec)np_alloc(1, sizeof(*array));
+    np_fwi fwipar = (np_fwi)np_alloc(1, sizeof(*fwipar));
+    fill_acpar(acpar, soupar, par);
+    preparation(vel, q, wav, acpar, soupar, array);
+    float ***d = np_floatalloc3(acpar->nt, acpar->nx, acpar->ns);
+    memcpy(d[0][0], dobs, sizeof(float) * acpar->nt * acpar->nx * acpar->ns);
+    fwipar->onlygrad = false;
+    fwipar->grad_type = 1;
+    fwipar->misfit_type = 1;
+    fwipar->opt_type = 1;
+    fwipar->wt1 = acpar->t0;
+    fwipar->wt2 = acpar->t0 + (acpar->nt - 1) * acpar->dt;
+    fwipar->woff1 = acpar->r0;
+    fwipar->woff2 = acpar->r0 + (acpar->nr - 1) * acpar->dr;
+    fwipar->oreo = false;
+    fwipar->waterz = 0;
+    fwipar->waterzb = 0;
+    fwipar->rectx = rect;
+    fwipar->rectz = rect;
+    gradient_init(d, soupar, acpar, array, fwipar, false);
+    gradient_v(array->vv, fcost, grad);
+}

@@ -100,6 +100,9 @@ _SIGS = {
     "pw_pfwi_passive": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp, C.POINTER(C.c_int),
                                   _vp]),
     "pw_aps": (C.c_int, [C.POINTER(AfdArgs), _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pw_pfwi_forward_visco": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp, _vp]),
+    "pw_pfwi_gradient_visco": (C.c_int, [C.POINTER(FwiArgs), _vp, _vp, _vp, _vp, _vp, _vp,
+                                         C.POINTER(C.c_double), _vp]),
     "pw_timerev": (C.c_int, [C.POINTER(FwiArgs), C.c_int, _vp, _vp, _vp, _vp]),
     "pw_butter_apply": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _vp, C.c_int,
                                   _vp]),

@@ -1712,6 +1712,472 @@ extern "C" int pw_pfwi_gradient_passive(const pw_fwi_args *a, int mode, const fl
   return gradient_impl(a, mode, vel, nullptr, src, dobs, weight, grad, misfit, ckpt_k, stream);
 }
 
+// ------------------------------------------------------- visco-acoustic --
+// forward_modeling (wave_fwimodeling.c:116-220) and gradient_v
+// (wave_fwigradient.c:264-452): the pfwi scheme with a memory variable r,
+//   r2 = (tau/taus*L + (idt - 0.5/taus)*r1) / (idt + 0.5/taus),
+//   term = L*(1 + tau) - (r2 + r1)*0.5 + rr*w,  p2 = 2 p1 - p0 + V term,
+// sponge on p0, p1 and r1; the adjoint pass forms r2 and tmp = p1*(1 + tau)
+// - 0.5*(r2 + r1) from p1, r1 and takes the Laplacian of tmp.  The
+// reference mixes float and double in these expressions; each operation is
+// written with the matching explicitly rounded intrinsic.  Fields use a plain
+// [pnx][pnz] layout; one thread per padded cell, Laplacian loads through L2.
+// Only the cells [4, pad-4) change: the reference's forward_modeling also
+// updates the 4-cell rim, where everything stays zero as long as no source
+// cell lies there (the drivers check that).  As in the acoustic scheme, a
+// field whose sponged value the step reads is stored before its last sponge
+// (B for p0, R for r1), so p and r need no third buffer.
+namespace pw {
+namespace pf {
+
+struct ViscoArgs {
+  int pnz, pnx, nb, nz, nx;
+  float c0, c1, c2, c3, c4, dx2, dz2, idt;
+  const float *V, *tau, *taus, *bz, *bx;
+  const float *A;        // p1 (sponged)
+  float *B;              // in: p0 before its second sponge; out: the new p1
+  float *R;              // in: r1 before its sponge; out: r2
+  const float *rr;       // forward: dense source maps [shot][pnx][pnz]
+  const float *wav;
+  int it, nt;
+  const ShotGeo *geo;
+  int rz, drv, nr;
+  float *rec;            // forward: traces [shot][nt][nr] or null
+  float *snap;           // forward: interior snapshot of this step [nx][nz] or null
+  long long fstride;     // floats per field (per shot)
+  // adjoint
+  const float *T;        // tmp field
+  const float *res;      // residual [nt][nr] of the shot
+  int imaging;
+  const float *wprev, *wcur, *wnext, *m2v3;
+  float wdt2;
+  float *grad;
+};
+
+__device__ __forceinline__ float visco_lap(const ViscoArgs &a, const float *p, long long j) {
+  const long long s = a.pnz;
+  float tx = fmul(a.c0, p[j]);
+  tx = fadd(tx, fmul(a.c1, fadd(p[j + s], p[j - s])));
+  tx = fadd(tx, fmul(a.c2, fadd(p[j + 2 * s], p[j - 2 * s])));
+  tx = fadd(tx, fmul(a.c3, fadd(p[j + 3 * s], p[j - 3 * s])));
+  tx = fadd(tx, fmul(a.c4, fadd(p[j + 4 * s], p[j - 4 * s])));
+  float tz = fmul(a.c0, p[j]);
+  tz = fadd(tz, fmul(a.c1, fadd(p[j + 1], p[j - 1])));
+  tz = fadd(tz, fmul(a.c2, fadd(p[j + 2], p[j - 2])));
+  tz = fadd(tz, fmul(a.c3, fadd(p[j + 3], p[j - 3])));
+  tz = fadd(tz, fmul(a.c4, fadd(p[j + 4], p[j - 4])));
+  return fadd(fdiv(tx, a.dx2), fdiv(tz, a.dz2));
+}
+
+__device__ __forceinline__ float visco_sponge(const ViscoArgs &a, float v, int ix, int iz) {
+  return fmul(a.bx[ix], fmul(a.bz[iz], v));  // z faces, then x faces (apply_sponge)
+}
+
+// one forward step of every shot of the batch (blockIdx.y = shot)
+__global__ void visco_fwd_kernel(const ViscoArgs a) {
+  const int s = blockIdx.y;
+  const long long n = (long long)a.pnz * a.pnx;
+  const float *A = a.A + s * a.fstride;
+  float *B = a.B + s * a.fstride, *R = a.R + s * a.fstride;
+  const float *rr = a.rr + s * n;
+  const ShotGeo &g = a.geo[s];
+  const float wv = a.wav[a.it];
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(j / a.pnz), iz = (int)(j - (long long)ix * a.pnz);
+    const float p1 = A[j];
+    if (a.rec && iz == a.rz) {  // traces read p1 before the step (wave_fwimodeling.c:181-185)
+      const int d = ix - g.r0v;
+      if (d >= 0 && d % a.drv == 0 && d / a.drv < g.nr2)
+        a.rec[((size_t)s * a.nt + a.it) * a.nr + g.r02 + d / a.drv] = p1;
+    }
+    if (a.snap && ix >= a.nb && ix < a.nb + a.nx && iz >= a.nb && iz < a.nb + a.nz)
+      a.snap[s * (long long)a.nx * a.nz + (long long)(ix - a.nb) * a.nz + (iz - a.nb)] = p1;
+    if (ix < 4 || ix >= a.pnx - 4 || iz < 4 || iz >= a.pnz - 4) continue;
+    const float L = visco_lap(a, A, j);
+    const float tau = a.tau[j], taus = a.taus[j];
+    const float r1 = visco_sponge(a, R[j], ix, iz);
+    const double hts = __ddiv_rn(0.5, (double)taus);
+    const double num = __dadd_rn((double)fmul(fdiv(tau, taus), L),
+                                 __dmul_rn(__dsub_rn((double)a.idt, hts), (double)r1));
+    const float r2 = __double2float_rn(__ddiv_rn(num, __dadd_rn((double)a.idt, hts)));
+    const double tt = __dadd_rn(__dsub_rn(__dmul_rn((double)L, __dadd_rn(1.0, (double)tau)),
+                                          __dmul_rn((double)fadd(r2, r1), 0.5)),
+                                (double)fmul(rr[j], wv));
+    const float t = __double2float_rn(tt);
+    const float p0 = visco_sponge(a, B[j], ix, iz);
+    const float p2 = fadd(fsub(fmul(2.f, p1), p0), fmul(a.V[j], t));
+    B[j] = visco_sponge(a, p2, ix, iz);
+    R[j] = r2;
+  }
+}
+
+// adjoint, first half of a step: r2 and tmp from p1 and r1 (wave_fwigradient.c:393-403)
+__global__ void visco_adj_pre_kernel(const ViscoArgs a) {
+  const long long n = (long long)a.pnz * a.pnx;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(j / a.pnz), iz = (int)(j - (long long)ix * a.pnz);
+    if (ix < 4 || ix >= a.pnx - 4 || iz < 4 || iz >= a.pnz - 4) continue;
+    const float p1 = a.A[j], tau = a.tau[j], taus = a.taus[j];
+    const float r1 = visco_sponge(a, a.R[j], ix, iz);
+    const double hts = __ddiv_rn(0.5, (double)taus);
+    const double nidt = -(double)a.idt;
+    const double num = __dadd_rn((double)fmul(fdiv(-tau, taus), p1),
+                                 __dmul_rn(__dadd_rn(nidt, hts), (double)r1));
+    const float r2 = __double2float_rn(__ddiv_rn(num, __dsub_rn(nidt, hts)));
+    const double tm = __dsub_rn(__dmul_rn((double)p1, __dadd_rn(1.0, (double)tau)),
+                                __dmul_rn(0.5, (double)fadd(r2, r1)));
+    const_cast<float *>(a.T)[j] = __double2float_rn(tm);
+    a.R[j] = r2;
+  }
+}
+
+// adjoint, second half: Laplacian of tmp plus the residual, the update, and
+// gradient_av's imaging with p1 (wave_fwigradient.c:405-438)
+__global__ void visco_adj_kernel(const ViscoArgs a) {
+  const long long n = (long long)a.pnz * a.pnx;
+  const ShotGeo &g = a.geo[0];
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(j / a.pnz), iz = (int)(j - (long long)ix * a.pnz);
+    if (ix < 4 || ix >= a.pnx - 4 || iz < 4 || iz >= a.pnz - 4) continue;
+    float L = visco_lap(a, a.T, j);
+    if (iz == a.rz) {
+      const int d = ix - g.r0v;
+      if (d >= 0 && d % a.drv == 0 && d / a.drv < g.nr2)
+        L = fadd(L, a.res[(size_t)a.it * a.nr + g.r02 + d / a.drv]);
+    }
+    const float p1 = a.A[j];
+    const float p0 = visco_sponge(a, a.B[j], ix, iz);
+    const float p2 = fadd(fsub(fmul(2.f, p1), p0), fmul(a.V[j], L));
+    if (a.imaging && ix >= a.nb && ix < a.nb + a.nx && iz >= a.nb && iz < a.nb + a.nz) {
+      const size_t k = (size_t)(ix - a.nb) * a.nz + (iz - a.nb);
+      const double w = __dadd_rn(__dsub_rn((double)a.wnext[k], __dmul_rn(2., (double)a.wcur[k])),
+                                 (double)a.wprev[k]);
+      const double gsum = __dmul_rn(__dmul_rn(__ddiv_rn(w, (double)a.wdt2), (double)p1),
+                                    (double)a.m2v3[k]);
+      a.grad[k] = __double2float_rn(__dadd_rn((double)a.grad[k], gsum));
+    }
+    a.B[j] = visco_sponge(a, p2, ix, iz);
+  }
+}
+
+// preparation's tau, taus (wave_fwiutil.c:90-96) and the pad2d copies
+static void visco_tables(const Setup &S, const float *q_host, std::vector<float> &tp,
+                         std::vector<float> &tsp, std::vector<float> &Vp, const float *vel_host) {
+  const pw_fwi_args &a = S.a;
+  const double pi = 3.14159265358979323846264338328;
+  const size_t nzx = (size_t)a.nz * a.nx, np = (size_t)S.pnz * S.pnx;
+  std::vector<float> t1(nzx), ts1(nzx);
+  for (size_t i = 0; i < nzx; i++) {
+    const float qq = q_host[i];
+    const float tmp = sqrtf(qq * qq + 1);
+    const float taue = (tmp + 1) / (2. * pi * a.f0 * qq);
+    ts1[i] = (tmp - 1) / (2. * pi * a.f0 * qq);
+    t1[i] = taue / ts1[i] - 1;
+  }
+  const float dt2 = a.dt * a.dt;
+  tp.resize(np);
+  tsp.resize(np);
+  Vp.resize(np);
+  for (int ix = 0; ix < S.pnx; ix++)
+    for (int iz = 0; iz < S.pnz; iz++) {
+      const int jx = std::min(std::max(ix - a.nb, 0), a.nx - 1);
+      const int jz = std::min(std::max(iz - a.nb, 0), a.nz - 1);
+      const size_t j = (size_t)ix * S.pnz + iz, k = (size_t)jx * a.nz + jz;
+      tp[j] = t1[k];
+      tsp[j] = ts1[k];
+      const float v = vel_host[k];
+      Vp[j] = (v * v) * dt2;
+    }
+}
+
+// the shots' source maps as dense fields, checked clear of the 4-cell rim
+static int visco_sources(const Setup &S, int ns, std::vector<float> &rr) {
+  const size_t np = (size_t)S.pnz * S.pnx;
+  rr.assign(np * ns, 0.f);
+  for (int is = 0; is < ns; is++) {
+    const ShotGeo &g = S.geo[is];
+    for (int k = 0; k < g.nsrc; k++) {
+      const int x = g.scell[k] >> 16, z = g.scell[k] & 0xffff;
+      PW_CHECK(x >= 4 && x < S.pnx - 4 && z >= 4 && z < S.pnz - 4, PW_ERR_SHAPE,
+               "visco-acoustic path: shot %d's source map reaches the 4-cell rim", is);
+      rr[np * is + (size_t)x * S.pnz + z] = g.sw[k];
+    }
+  }
+  return PW_OK;
+}
+
+static void visco_base(const Setup &S, ViscoArgs &v) {
+  v = ViscoArgs{};
+  v.pnz = S.pnz;
+  v.pnx = S.pnx;
+  v.nb = S.a.nb;
+  v.nz = S.a.nz;
+  v.nx = S.a.nx;
+  const float c0 = -205. / 72, c1 = 8. / 5, c2 = -1. / 5, c3 = 8. / 315, c4 = -1. / 560;
+  v.c0 = c0; v.c1 = c1; v.c2 = c2; v.c3 = c3; v.c4 = c4;
+  v.dx2 = S.a.dx * S.a.dx;
+  v.dz2 = S.a.dz * S.a.dz;
+  v.idt = 1. / S.a.dt;
+  v.nt = S.a.nt;
+  v.rz = S.rz;
+  v.drv = S.drv;
+  v.nr = S.nr;
+  v.fstride = (long long)S.pnz * S.pnx;
+}
+
+// the acoustic path's stability limit on the host copy of the velocity
+static int check_cfl_host(const Setup &S, const std::vector<float> &vh) {
+  if (S.a.flags & PW_NO_CFL_CHECK) return PW_OK;
+  float vmax = 0.f;
+  for (float v : vh) vmax = std::max(vmax, v);
+  const float cfl = vmax * S.a.dt / std::min(S.a.dx, S.a.dz);
+  PW_CHECK(cfl <= 0.555f, PW_ERR_CFL, "unstable: vmax*dt/h = %g exceeds 0.555", cfl);
+  return PW_OK;
+}
+
+// the host copies a visco call needs: velocity and quality factor
+static int visco_host_inputs(const pw_fwi_args *a, const float *vel, const float *q,
+                             std::vector<float> &vh, std::vector<float> &qh, cudaStream_t st) {
+  const size_t nzx = (size_t)a->nz * a->nx;
+  vh.resize(nzx);
+  qh.resize(nzx);
+  const bool host = (a->flags & PW_HOST_PTRS) != 0;
+  if (host) {
+    memcpy(vh.data(), vel, nzx * 4);
+    memcpy(qh.data(), q, nzx * 4);
+  } else {
+    PW_CUDA(cudaMemcpyAsync(vh.data(), vel, nzx * 4, cudaMemcpyDeviceToHost, st));
+    PW_CUDA(cudaMemcpyAsync(qh.data(), q, nzx * 4, cudaMemcpyDeviceToHost, st));
+    PW_CUDA(cudaStreamSynchronize(st));
+  }
+  for (size_t i = 0; i < nzx; i++)
+    PW_CHECK(vh[i] > 0.f && std::isfinite(vh[i]) && qh[i] > 0.f && std::isfinite(qh[i]),
+             PW_ERR_VALUE, "velocity and quality factor must be finite and positive");
+  return PW_OK;
+}
+
+}  // namespace pf
+}  // namespace pw
+
+extern "C" int pw_pfwi_forward_visco(const pw_fwi_args *a, const float *vel, const float *q,
+                                     const float *wav, float *data, void *stream) {
+  PW_CHECK(a && vel && q && wav && data, PW_ERR_VALUE, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  Setup S;
+  PW_TRY(setup(a, S));
+  const bool host = (a->flags & PW_HOST_PTRS) != 0;
+  const int ns = a->ns, nt = a->nt, nr = S.nr;
+  std::vector<float> vh, qh, tp, tsp, Vp, rr;
+  PW_TRY(visco_host_inputs(a, vel, q, vh, qh, st));
+  PW_TRY(check_cfl_host(S, vh));
+  visco_tables(S, qh.data(), tp, tsp, Vp, vh.data());
+  PW_TRY(visco_sources(S, ns, rr));
+  const size_t np = (size_t)S.pnz * S.pnx;
+  Carve cv;
+  const size_t o_V = cv.add(np * 4), o_t = cv.add(np * 4), o_ts = cv.add(np * 4);
+  const size_t o_A = cv.add((size_t)ns * np * 4), o_B = cv.add((size_t)ns * np * 4);
+  const size_t o_R = cv.add((size_t)ns * np * 4), o_rr = cv.add((size_t)ns * np * 4);
+  const size_t o_bz = cv.add(S.bz.size() * 4), o_bx = cv.add(S.bx.size() * 4);
+  const size_t o_w = cv.add((size_t)nt * 4), o_geo = cv.add(sizeof(ShotGeo) * ns);
+  const size_t o_rec = cv.add((size_t)ns * nt * nr * 4), o_out = cv.add((size_t)ns * nt * nr * 4);
+  Workspace &ws = Workspace::for_current_device();
+  std::lock_guard<std::mutex> lock(ws.mutex());
+  struct Drain {
+    cudaStream_t st;
+    ~Drain() { cudaStreamSynchronize(st); }
+  } drain{st};
+  PW_TRY(ws.reserve(cv.total()));
+  char *base = ws.base();
+  PW_CUDA(cudaMemsetAsync(base, 0, cv.total(), st));
+  PW_CUDA(cudaMemcpyAsync(base + o_V, Vp.data(), np * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_t, tp.data(), np * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_ts, tsp.data(), np * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_rr, rr.data(), rr.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_bz, S.bz.data(), S.bz.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_bx, S.bx.data(), S.bx.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_geo, S.geo.data(), sizeof(ShotGeo) * ns,
+                          cudaMemcpyHostToDevice, st));
+  PW_TRY(to_device(base + o_w, wav, (size_t)nt * 4, host, st));
+  ViscoArgs v;
+  visco_base(S, v);
+  v.V = at<float>(base, o_V);
+  v.tau = at<float>(base, o_t);
+  v.taus = at<float>(base, o_ts);
+  v.bz = at<float>(base, o_bz);
+  v.bx = at<float>(base, o_bx);
+  v.rr = at<float>(base, o_rr);
+  v.wav = at<float>(base, o_w);
+  v.geo = at<ShotGeo>(base, o_geo);
+  v.rec = at<float>(base, o_rec);
+  v.R = at<float>(base, o_R);
+  float *A = at<float>(base, o_A), *B = at<float>(base, o_B);
+  const dim3 grid((unsigned)std::min<long long>(ceil_div((long long)np, 256), 1184), (unsigned)ns);
+  LoopTimer timer(st);
+  timer.start();
+  for (int it = 0; it < nt; it++) {
+    v.it = it;
+    v.A = A;
+    v.B = B;
+    visco_fwd_kernel<<<grid, 256, 0, st>>>(v);
+    PW_CUDA(cudaGetLastError());
+    std::swap(A, B);
+  }
+  timer.stop();
+  // traces [shot][nt][nr] -> data [shot][nr][nt]
+  float *out = at<float>(base, o_out);
+  for (int s = 0; s < ns; s++) {
+    dim3 tb(32, 8), tg(ceil_div(nr, 32), ceil_div(nt, 32));
+    transpose_kernel<<<tg, tb, 0, st>>>(v.rec + (size_t)s * nt * nr, out + (size_t)s * nr * nt,
+                                        nt, nr);
+  }
+  PW_CUDA(cudaGetLastError());
+  PW_TRY(to_host(data, out, (size_t)ns * nr * nt * 4, host, st));
+  timer.finish(nt, nt + ns);
+  PW_CUDA(cudaStreamSynchronize(st));
+  return PW_OK;
+}
+
+extern "C" int pw_pfwi_gradient_visco(const pw_fwi_args *a, const float *vel, const float *q,
+                                      const float *wav, const float *dobs, const float *weight,
+                                      float *grad, double *misfit, void *stream) {
+  PW_CHECK(a && vel && q && wav && dobs && grad, PW_ERR_VALUE, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  Setup S;
+  PW_TRY(setup(a, S));
+  const bool host = (a->flags & PW_HOST_PTRS) != 0;
+  const int ns = a->ns, nt = a->nt, nr = S.nr, nz = a->nz, nx = a->nx;
+  const size_t nzx = (size_t)nz * nx, np = (size_t)S.pnz * S.pnx;
+  const int interval = std::max(1, a->interval);
+  const int wnt = (nt - 1) / interval + 1;
+  std::vector<float> vh, qh, tp, tsp, Vp, rr, wts;
+  PW_TRY(visco_host_inputs(a, vel, q, vh, qh, st));
+  PW_TRY(check_cfl_host(S, vh));
+  visco_tables(S, qh.data(), tp, tsp, Vp, vh.data());
+  PW_TRY(visco_sources(S, ns, rr));
+  if (weight == nullptr) residual_weights(*a, nr, wts);
+  Carve cv;
+  const size_t o_V = cv.add(np * 4), o_t = cv.add(np * 4), o_ts = cv.add(np * 4);
+  const size_t o_A = cv.add(np * 4), o_B = cv.add(np * 4), o_R = cv.add(np * 4);
+  const size_t o_T = cv.add(np * 4), o_rr = cv.add((size_t)ns * np * 4);
+  const size_t o_bz = cv.add(S.bz.size() * 4), o_bx = cv.add(S.bx.size() * 4);
+  const size_t o_w = cv.add((size_t)nt * 4), o_geo = cv.add(sizeof(ShotGeo) * ns);
+  const size_t o_wt = cv.add((size_t)nr * nt * 4);
+  const size_t o_dobs = cv.add((size_t)ns * nt * nr * 4), o_din = cv.add((size_t)ns * nt * nr * 4);
+  const size_t o_rec = cv.add((size_t)nt * nr * 4), o_res = cv.add((size_t)nt * nr * 4);
+  const size_t o_snap = cv.add((size_t)wnt * nzx * 4);
+  const size_t o_m2v3 = cv.add(nzx * 4), o_vel = cv.add(nzx * 4), o_grad = cv.add(nzx * 4);
+  const size_t o_mis = cv.add(8 * (1 + RESID_BLOCKS));
+  Workspace &ws = Workspace::for_current_device();
+  std::lock_guard<std::mutex> lock(ws.mutex());
+  struct Drain {
+    cudaStream_t st;
+    ~Drain() { cudaStreamSynchronize(st); }
+  } drain{st};
+  PW_TRY(ws.reserve(cv.total()));
+  char *base = ws.base();
+  PW_CUDA(cudaMemsetAsync(base, 0, cv.total(), st));
+  PW_CUDA(cudaMemcpyAsync(base + o_V, Vp.data(), np * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_t, tp.data(), np * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_ts, tsp.data(), np * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_rr, rr.data(), rr.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_bz, S.bz.data(), S.bz.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_bx, S.bx.data(), S.bx.size() * 4, cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_geo, S.geo.data(), sizeof(ShotGeo) * ns,
+                          cudaMemcpyHostToDevice, st));
+  PW_CUDA(cudaMemcpyAsync(base + o_vel, vh.data(), nzx * 4, cudaMemcpyHostToDevice, st));
+  PW_TRY(to_device(base + o_w, wav, (size_t)nt * 4, host, st));
+  if (weight) PW_TRY(to_device(base + o_wt, weight, (size_t)nr * nt * 4, host, st));
+  else PW_CUDA(cudaMemcpyAsync(base + o_wt, wts.data(), wts.size() * 4, cudaMemcpyHostToDevice, st));
+  {
+    PW_TRY(to_device(base + o_din, dobs, (size_t)ns * nt * nr * 4, host, st));
+    for (int s = 0; s < ns; s++) {  // dobs [shot][nr][nt] -> [shot][nt][nr]
+      dim3 tb(32, 8), tg(ceil_div(nt, 32), ceil_div(nr, 32));
+      transpose_kernel<<<tg, tb, 0, st>>>(at<float>(base, o_din) + (size_t)s * nr * nt,
+                                          at<float>(base, o_dobs) + (size_t)s * nt * nr, nr, nt);
+    }
+    PW_CUDA(cudaGetLastError());
+  }
+  m2v3_kernel<<<592, 256, 0, st>>>(at<float>(base, o_vel), nzx, at<float>(base, o_m2v3));
+  PW_CUDA(cudaGetLastError());
+  ViscoArgs v;
+  visco_base(S, v);
+  v.V = at<float>(base, o_V);
+  v.tau = at<float>(base, o_t);
+  v.taus = at<float>(base, o_ts);
+  v.bz = at<float>(base, o_bz);
+  v.bx = at<float>(base, o_bx);
+  v.wav = at<float>(base, o_w);
+  v.R = at<float>(base, o_R);
+  v.T = at<float>(base, o_T);
+  v.m2v3 = at<float>(base, o_m2v3);
+  v.grad = at<float>(base, o_grad);
+  v.wdt2 = (a->dt * interval) * (a->dt * interval);
+  float *snap = at<float>(base, o_snap);
+  double *dmis = at<double>(base, o_mis);
+  const dim3 g1((unsigned)std::min<long long>(ceil_div((long long)np, 256), 1184), 1);
+  LoopTimer timer(st);
+  timer.start();
+  long long launches = 0;
+  // one shot at a time: the gradient sums the shots in the reference's order
+  for (int is = 0; is < ns; is++) {
+    float *A = at<float>(base, o_A), *B = at<float>(base, o_B);
+    PW_CUDA(cudaMemsetAsync(A, 0, np * 4, st));
+    PW_CUDA(cudaMemsetAsync(B, 0, np * 4, st));
+    PW_CUDA(cudaMemsetAsync(v.R, 0, np * 4, st));
+    v.geo = at<ShotGeo>(base, o_geo) + is;
+    v.rr = at<float>(base, o_rr) + (size_t)is * np;
+    v.rec = at<float>(base, o_rec);
+    for (int it = 0; it < nt; it++) {
+      v.it = it;
+      v.A = A;
+      v.B = B;
+      v.snap = it % interval == 0 ? snap + (size_t)(it / interval) * nzx : nullptr;
+      visco_fwd_kernel<<<g1, 256, 0, st>>>(v);
+      PW_CUDA(cudaGetLastError());
+      launches++;
+      std::swap(A, B);
+    }
+    v.snap = nullptr;
+    v.rec = nullptr;
+    residual_kernel<<<RESID_BLOCKS, 256, 0, st>>>(at<float>(base, o_rec),
+                                                  at<float>(base, o_dobs) + (size_t)is * nt * nr,
+                                                  at<float>(base, o_wt), at<float>(base, o_res), 1,
+                                                  nt, nr, 0, dmis);
+    misfit_sum_kernel<<<1, 32, 0, st>>>(dmis, RESID_BLOCKS);
+    PW_CUDA(cudaGetLastError());
+    v.res = at<float>(base, o_res);
+    PW_CUDA(cudaMemsetAsync(A, 0, np * 4, st));
+    PW_CUDA(cudaMemsetAsync(B, 0, np * 4, st));
+    PW_CUDA(cudaMemsetAsync(v.R, 0, np * 4, st));
+    for (int it = nt - 1; it >= 0; it--) {
+      const int wit = it / interval;
+      v.it = it;
+      v.A = A;
+      v.B = B;
+      v.imaging = (it % interval == 0) && wit != wnt - 1 && wit != 0;
+      if (v.imaging) {
+        v.wprev = snap + (size_t)(wit - 1) * nzx;
+        v.wcur = snap + (size_t)wit * nzx;
+        v.wnext = snap + (size_t)(wit + 1) * nzx;
+      }
+      visco_adj_pre_kernel<<<g1, 256, 0, st>>>(v);
+      visco_adj_kernel<<<g1, 256, 0, st>>>(v);
+      PW_CUDA(cudaGetLastError());
+      launches += 2;
+      std::swap(A, B);
+    }
+  }
+  timer.stop();
+  PW_TRY(to_host(grad, at<float>(base, o_grad), nzx * 4, host, st));
+  if (misfit) PW_CUDA(cudaMemcpyAsync(misfit, dmis, 8, cudaMemcpyDeviceToHost, st));
+  timer.finish(launches, launches + 4 * ns + 2);
+  PW_CUDA(cudaStreamSynchronize(st));
+  return PW_OK;
+}
+
 extern "C" int pw_last_fwi_plan(int *ckpt_k, int *shots_per_batch, long long *bytes,
                                 double *recompute) {
   const PlanRecord &r = plan_record();

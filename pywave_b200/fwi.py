@@ -93,6 +93,35 @@ def gradient_passive(vel, src, dobs, par, mode="reference", ckpt_k=0, per_shot=F
     return g.reshape(a.nz, a.nx, order="F"), J.value
 
 
+def forward_visco(vel, q, wav, par):
+    """Visco-acoustic forward modelling (forward_modeling,
+    wave_fwimodeling.c:116-220): vel, q (nz, nx), par a pfwi parameter dict
+    (its f0 sets the relaxation times); returns data (nt, nr, ns)."""
+    a = fwi_args(par, L.PW_HOST_PTRS)
+    v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F"))
+    qq = np.ascontiguousarray(np.asarray(q, np.float32).flatten(order="F"))
+    w = np.ascontiguousarray(np.asarray(wav, np.float32).reshape(-1))
+    out = np.empty(a.ns * a.nx * a.nt, np.float32)
+    L.check(L.lib().pw_pfwi_forward_visco(a, L.ptr(v), L.ptr(qq), L.ptr(w), L.ptr(out), None))
+    return out.reshape(a.nt, a.nx, a.ns, order="F")
+
+
+def gradient_visco(vel, q, wav, dobs, par, weight=None):
+    """Visco-acoustic gradient_v (wave_fwigradient.c:264-452) before its
+    smoothing / scaling, and the FP64 misfit 0.5*sum((dobs-d)^2)."""
+    a = fwi_args(par, L.PW_HOST_PTRS)
+    v = np.ascontiguousarray(np.asarray(vel, np.float32).flatten(order="F"))
+    qq = np.ascontiguousarray(np.asarray(q, np.float32).flatten(order="F"))
+    w = np.ascontiguousarray(np.asarray(wav, np.float32).reshape(-1))
+    d = _data_flat(dobs)
+    wt = None if weight is None else np.ascontiguousarray(np.asarray(weight, np.float32))
+    g = np.empty(a.nz * a.nx, np.float32)
+    J = ctypes.c_double(0.0)
+    L.check(L.lib().pw_pfwi_gradient_visco(a, L.ptr(v), L.ptr(qq), L.ptr(w), L.ptr(d), L.ptr(wt),
+                                           L.ptr(g), ctypes.byref(J), None))
+    return g.reshape(a.nz, a.nx, order="F"), J.value
+
+
 def postprocess(grad, rect=3, waterz=0, scaling=None):
     """gradient_av's tail: triangle smoothing and the (first-call) scale."""
     g = np.ascontiguousarray(np.asarray(grad, np.float32).flatten(order="F"))

@@ -24,7 +24,7 @@ import sys
 
 import numpy as np
 
-from models import (APS2, APS3, aps2_velocity, aps3_velocity)
+from models import (APS2, APS3, VISCO, aps2_velocity, aps3_velocity, visco_case)
 from models import (BIG3D, BIG3D_BAND, BIG3D_TRI_JSNAP, BUTTER_CASES, LSTRI, MID, PAS, PAS_FHI,
                     PAS_FLO, WEIGHT_CASE, big3d_velocity, digest, lstri_case, mid_models,
                     mid_wavelet, pas_case, pfwi_scale_case)
@@ -66,6 +66,8 @@ def refdrv():
     L.refdrv_gradient_pas.argtypes = [f32p, f32p, f32p, f32p, f32p, f32p, C.c_int, C.c_float,
                                       C.c_float, f32p, f32p]
     L.refdrv_butter.argtypes = [C.c_int, C.c_float, C.c_int, C.c_int, f32p]
+    L.refdrv_forward_visco.argtypes = [f32p] * 5
+    L.refdrv_gradient_visco.argtypes = [f32p] * 5 + [C.c_int, f32p, f32p]
     L.refdrv_residual_weights.argtypes = [C.c_int] * 7 + [f32p]
     return L
 
@@ -289,6 +291,31 @@ def make_aps():
                         v3=v3, d3=d3, w3=w3)
 
 
+def make_visco(R):
+    """Visco-acoustic pfwi, which the reference's Python glue cannot reach
+    (pfwi.c:864 always takes the acoustic path): forward_modeling
+    (wave_fwimodeling.c:116) of the true model and gradient_v
+    (wave_fwigradient.c:264) at the start model, rect 1 and 3, both called
+    through oracle/ref_driver.c."""
+    vt, vs, q, wav = visco_case()
+    nz, nx, nt, ns = VISCO["nz"], VISCO["nx"], VISCO["nt"], VISCO["ns"]
+    parr = _fwi_parr(VISCO)
+    qf = np.ascontiguousarray(q.flatten(order="F"))
+    data = np.zeros(ns * nx * nt, np.float32)
+    quiet(R.refdrv_forward_visco, parr, np.ascontiguousarray(vt.flatten(order="F")), qf.copy(),
+          wav.copy(), data)
+    g = {}
+    for rect in (1, 3):
+        gr = np.zeros(nz * nx, np.float32)
+        fc = np.zeros(1, np.float32)
+        quiet(R.refdrv_gradient_visco, parr, np.ascontiguousarray(vs.flatten(order="F")),
+              qf.copy(), wav.copy(), data.copy(), rect, gr, fc)
+        g[rect] = (gr.reshape(nz, nx, order="F"), float(fc[0]))
+    np.savez_compressed(os.path.join(HERE, "visco.npz"), q=q,
+                        data=data.reshape(nt, nx, ns, order="F"), grad_rect1=g[1][0],
+                        grad_rect3=g[3][0], fcost=g[1][1])
+
+
 class _Recorder:
     """Stands in for an extension module: records each call's arguments and
     returns the real module's result."""
@@ -382,7 +409,8 @@ def main(names=()):
     extra = {"afd3d_big": lambda: make_afd3d_big(a3, R), "pfwi_scale": lambda: make_pfwi_scale(R),
              "pfwi_mid": lambda: make_pfwi_mid(pf, R), "dropin": make_dropin,
              "lstri": make_lstri, "pfwi_pas": lambda: make_pfwi_pas(R),
-             "butter": lambda: make_butter(R), "aps": make_aps}
+             "butter": lambda: make_butter(R), "aps": make_aps,
+             "visco": lambda: make_visco(R)}
     if names:
         for n in names:
             extra[n]()

@@ -191,3 +191,25 @@ def aps3_velocity():
     z = np.arange(20, dtype=np.float32)[:, None, None]
     v = 1800.0 + 600.0 * z / 20 + np.zeros((20, 24, 22), np.float32)
     return (v * (1.0 + 0.03 * rng.random(v.shape))).astype(np.float32)
+
+
+# ---- visco-acoustic pfwi (forward_modeling / gradient_v) --------------------
+VISCO = dict(nz=30, nx=50, dz=0.01, dx=0.01, oz=0, ox=0, nt=400, dt=0.001, ot=0, ns=3, ds=0.15,
+             os=0.05, nb=20, coef=0.005, f0=10, acqui_type=1, interval=1, niter=2)
+
+
+def visco_case():
+    """True velocity (2.0 / 2.5 / 3.0 km/s layers at 12 and 22), the start
+    model (2.4 constant), a seeded quality factor between 20 and 80, and the
+    10 Hz Ricker wavelet of the pfwi golden."""
+    nz, nx, nt = VISCO["nz"], VISCO["nx"], VISCO["nt"]
+    vt = np.full((nz, nx), 2.0, np.float32)
+    vt[12:] = 2.5
+    vt[22:] = 3.0
+    vs = np.full((nz, nx), 2.4, np.float32)
+    rng = np.random.default_rng(41)
+    q = (20.0 + 60.0 * rng.random((nz, nx))).astype(np.float32)
+    tt = np.arange(nt) * 0.001
+    arg = (np.pi * 10 * (tt - 0.1)) ** 2
+    wav = ((1 - 2 * arg) * np.exp(-arg)).astype(np.float32)
+    return vt, vs, q, wav
