@@ -70,6 +70,10 @@ struct StepArgs {
                             // warps per column chunk
   int WZ, WX;               // warp-tile kernel: warps per CTA along z and x (per group)
   float c0, c1, c2, idx, idy, idz, k0;
+  // 1.0f, as a runtime value: each packed product is multiplied by it
+  // before it is added, so that a product and its add fused into one FMA
+  // (p * one + t) still round as the separate multiply and add
+  float one;
   const float *cur[MAXG];
   float *nxt[MAXG];
   const float *vv;
@@ -733,6 +737,46 @@ __device__ __forceinline__ void tile_lane_setup(const StepArgs &a, TileLane<NC> 
 // 0 no taper and no mask; 1 y taper only (x wy); 2 z / x taper only, no z-x
 // edge (x wz*wx); 3 everything face by face (masks, sources, z-x edges).
 // Returns the path taken.
+// Packed pairs of floats for sm_100's f32x2 pipe: add / sub / mul.rn.f32x2
+// round each lane exactly as the scalar __fadd_rn / __fsub_rn / __fmul_rn.
+// Unlike the scalar .rn forms, a packed multiply whose result feeds a packed
+// add is fused by the assembler into one FMA (one rounding instead of two,
+// with or without -fmad=false), so every product that is added is first
+// multiplied by a runtime 1.0 (StepArgs::one): the fused form p * 1 + t then
+// rounds exactly as the separate add.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 pk2(float a, float b) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void up2(f2 r, float &a, float &b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+  f2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+  f2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+  f2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 lo2(const float4 &v) { return pk2(v.x, v.y); }
+__device__ __forceinline__ f2 hi2(const float4 &v) { return pk2(v.z, v.w); }
+__device__ __forceinline__ float4 join2(f2 l, f2 h) {
+  float4 r;
+  up2(l, r.x, r.y);
+  up2(h, r.z, r.w);
+  return r;
+}
+
 template <bool TRI, bool SNAP, int NC>
 __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> &L, int y,
                                           float wy, const float4 (&q0)[NC],
@@ -743,6 +787,9 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> 
   constexpr int TZ = TILE_TZ;
   const int erz = L.erz, gi = L.gi;
   const bool lyok = y >= g.ly0 && y < g.ly1;
+  const f2 kc0 = pk2(a.c0, a.c0), kc1 = pk2(a.c1, a.c1), kc2 = pk2(a.c2, a.c2);
+  const f2 kk0 = pk2(a.k0, a.k0), kidx = pk2(a.idx, a.idx), kidy = pk2(a.idy, a.idy);
+  const f2 kidz = pk2(a.idz, a.idz), k1 = pk2(a.one, a.one);
   const int nrec = a.nrx * a.nry;
   bool src_plane = false;
   if (!TRI)
@@ -789,43 +836,51 @@ __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> 
     const float2 Rf = reinterpret_cast<const float2 *>(pc + ci + 1)[0];  // (x, y)
     const float4 pv = pbv[L.lane + 32 * j];
     const float4 vv4 = pbv[32 * NC + L.lane + 32 * j];
-    float4 lp;  // Laplacian sums in the reference's order
+    // Laplacian sums in the reference's order, two cells per f32x2 op: cells
+    // (0, 1) and (2, 3) of the quad; the z +-1 neighbours are the quad
+    // shifted by one cell, so their pairs are repacked
+    const float4 &c4 = q2[j];
+    const f2 cv[2] = {lo2(c4), hi2(c4)};
+    const f2 zpa = pk2(Lf.y, c4.x), zpb = pk2(c4.y, c4.z), zpc = pk2(c4.w, Rf.x);
+    const f2 s_y1[2] = {add2(lo2(q1[j]), lo2(q3[j])), add2(hi2(q1[j]), hi2(q3[j]))};
+    const f2 s_y2[2] = {add2(lo2(q0[j]), lo2(q4[j])), add2(hi2(q0[j]), hi2(q4[j]))};
+    const f2 s_x1[2] = {add2(lo2(xm1), lo2(xp1)), add2(hi2(xm1), hi2(xp1))};
+    const f2 s_x2[2] = {add2(lo2(xm2), lo2(xp2)), add2(hi2(xm2), hi2(xp2))};
+    const f2 s_z1[2] = {add2(zpa, zpb), add2(zpb, zpc)};
+    const f2 s_z2[2] = {add2(pk2(Lf.x, Lf.y), hi2(c4)), add2(lo2(c4), pk2(Rf.x, Rf.y))};
+    f2 lp2[2];
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const float cv = el(q2[j], e);
-      const float zm1 = e == 0 ? Lf.y : el(q2[j], e - 1);
-      const float zp1 = e == 3 ? Rf.x : el(q2[j], e + 1);
-      const float zm2 = e == 0 ? Lf.x : (e == 1 ? Lf.y : el(q2[j], e - 2));
-      const float zp2 = e == 2 ? Rf.x : (e == 3 ? Rf.y : el(q2[j], e + 2));
-      float tt = fmul(fmul(a.c0, cv), a.k0);
-      tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1[j], e), el(q3[j], e))), a.idy));
-      tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0[j], e), el(q4[j], e))), a.idy));
-      tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
-      tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
-      tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-      tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-      set_el(lp, e, tt);
+    for (int h = 0; h < 2; h++) {
+      f2 tt = mul2(mul2(mul2(kc0, cv[h]), kk0), k1);
+      tt = add2(tt, mul2(mul2(mul2(kc1, s_y1[h]), kidy), k1));
+      tt = add2(tt, mul2(mul2(mul2(kc2, s_y2[h]), kidy), k1));
+      tt = add2(tt, mul2(mul2(mul2(kc1, s_x1[h]), kidx), k1));
+      tt = add2(tt, mul2(mul2(mul2(kc2, s_x2[h]), kidx), k1));
+      tt = add2(tt, mul2(mul2(mul2(kc1, s_z1[h]), kidz), k1));
+      tt = add2(tt, mul2(mul2(mul2(kc2, s_z2[h]), kidz), k1));
+      lp2[h] = tt;
     }
+    const f2 pvp[2] = {lo2(pv), hi2(pv)}, vvp[2] = {lo2(vv4), hi2(vv4)};
     float4 res;
     if (path == 0) {
+      f2 r[2];
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const float cv = el(q2[j], e);
-        float v = fadd(cv, fsub(cv, el(pv, e)));
-        set_el(res, e, fadd(v, fmul(el(lp, e), el(vv4, e))));
-      }
+      for (int h = 0; h < 2; h++)
+        r[h] = add2(add2(cv[h], sub2(cv[h], pvp[h])), mul2(mul2(lp2[h], vvp[h]), k1));
+      res = join2(r[0], r[1]);
     } else if (path == 1 || path == 2) {
-      float4 f;
+      const f2 f[2] = {path == 1 ? pk2(wy, wy) : pk2(L.wzx[j][0], L.wzx[j][1]),
+                       path == 1 ? pk2(wy, wy) : pk2(L.wzx[j][2], L.wzx[j][3])};
+      f2 r[2];
 #pragma unroll
-      for (int e = 0; e < 4; e++) set_el(f, e, path == 1 ? wy : L.wzx[j][e]);
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const float cv = el(q2[j], e);
-        float v = fadd(cv, fsub(cv, fmul(el(pv, e), el(f, e))));
-        v = fadd(v, fmul(el(lp, e), el(vv4, e)));
-        set_el(res, e, fmul(v, el(f, e)));
+      for (int h = 0; h < 2; h++) {
+        f2 v = add2(cv[h], sub2(cv[h], mul2(mul2(pvp[h], f[h]), k1)));
+        v = add2(v, mul2(mul2(lp2[h], vvp[h]), k1));
+        r[h] = mul2(v, f[h]);
       }
+      res = join2(r[0], r[1]);
     } else {
+      const float4 lp = join2(lp2[0], lp2[1]);
 #pragma unroll
       for (int e = 0; e < 4; e++) {
         const float cv = el(q2[j], e);
@@ -2073,6 +2128,7 @@ static int run(const pw_afd_args *a, int G, const int *group, const float *vel, 
       s.idy = idy;
       s.k0 = (idy + idx) + idz;
     }
+    s.one = 1.f;
   }
   s.vv = vv;
   s.wz = d_wz;
@@ -2303,6 +2359,7 @@ static void batch_args(const pw_afd_args *a, const BatchShot &b, char *base, Ste
   s.idy = idx;  // the model's x is the marched axis
   s.idx = 0.f;
   s.k0 = idx + idz;
+  s.one = 1.f;
   s.cur[0] = at<float>(base, b.o_A);
   s.nxt[0] = at<float>(base, b.o_B);
   s.vv = at<float>(base, b.o_vv);
@@ -2762,6 +2819,7 @@ static int run_noalloc(const pw_afd_args *a, const float *vel, const float *src,
       s.idy = idy;
       s.k0 = (idy + idx) + idz;
     }
+    s.one = 1.f;
   }
   s.vv = vv;
   s.wz = d_wz;
