@@ -106,11 +106,11 @@ int pw_afd_batch(int nshot, const pw_afd_args *args, const float *const *vel,
  *   calls of one process from overlapping.  Every call waits on `stream`: it
  *   reads the source positions back to the host and returns only after its
  *   work has finished.  The first call on a device loads the module holding
- *   the array and takes its address, so make it before any stream capture
- *   begins.  The array is reserved when that module loads: on the first call
- *   under lazy module loading (CUDA_MODULE_LOADING=LAZY, the default since
- *   CUDA 12.2), or when each context loads the library under EAGER loading,
- *   whether or not pw_afd_noalloc is ever called. */
+ *   the array and takes its address.  The array is reserved when that module
+ *   loads: on the first call under lazy module loading
+ *   (CUDA_MODULE_LOADING=LAZY, the default since CUDA 12.2), or when each
+ *   context loads the library under EAGER loading, whether or not
+ *   pw_afd_noalloc is ever called. */
 int pw_afd_noalloc(const pw_afd_args *a, const float *vel, const float *src,
                    const float *wavelet, float *dat, float *wfd, void *stream);
 
