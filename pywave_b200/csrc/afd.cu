@@ -737,46 +737,6 @@ __device__ __forceinline__ void tile_lane_setup(const StepArgs &a, TileLane<NC> 
 // 0 no taper and no mask; 1 y taper only (x wy); 2 z / x taper only, no z-x
 // edge (x wz*wx); 3 everything face by face (masks, sources, z-x edges).
 // Returns the path taken.
-// Packed pairs of floats for sm_100's f32x2 pipe: add / sub / mul.rn.f32x2
-// round each lane exactly as the scalar __fadd_rn / __fsub_rn / __fmul_rn.
-// Unlike the scalar .rn forms, a packed multiply whose result feeds a packed
-// add is fused by the assembler into one FMA (one rounding instead of two,
-// with or without -fmad=false), so every product that is added is first
-// multiplied by a runtime 1.0 (StepArgs::one): the fused form p * 1 + t then
-// rounds exactly as the separate add.
-typedef unsigned long long f2;
-__device__ __forceinline__ f2 pk2(float a, float b) {
-  f2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-  return r;
-}
-__device__ __forceinline__ void up2(f2 r, float &a, float &b) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
-}
-__device__ __forceinline__ f2 add2(f2 a, f2 b) {
-  f2 r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
-  f2 r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
-  f2 r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ f2 lo2(const float4 &v) { return pk2(v.x, v.y); }
-__device__ __forceinline__ f2 hi2(const float4 &v) { return pk2(v.z, v.w); }
-__device__ __forceinline__ float4 join2(f2 l, f2 h) {
-  float4 r;
-  up2(l, r.x, r.y);
-  up2(h, r.z, r.w);
-  return r;
-}
-
 template <bool TRI, bool SNAP, int NC>
 __device__ __forceinline__ int tile_plane(const StepArgs &a, const TileLane<NC> &L, int y,
                                           float wy, const float4 (&q0)[NC],

@@ -67,6 +67,7 @@ struct PfArgs {
   int nb, nz, nx;             // sponge width, interior
   float c0, c1, c2, c3, c4;   // 8th-order coefficients (wave_fwiutil.c:17)
   float dx2, dz2;
+  float one;                  // 1.0f at run time: keeps packed products unfused (pk2 helpers)
   DivC divx, divz;            // fast exact division by dx2 / dz2
   int nshots;
   const float *cur[MAXS];
@@ -361,28 +362,48 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
         }
         float4 term4, res4;
         float txs[4], tzs[4], qx[4], qz[4];
+        {
+          // the x and z sums of the 8th-order Laplacian in the reference's
+          // order, cells (0, 1) and (2, 3) of the float4 per f32x2 op; the
+          // z neighbours at odd distances are the float4s shifted by one cell
+          const f2 k1 = pk2(a.one, a.one);
+          const f2 kc[5] = {pk2(a.c0, a.c0), pk2(a.c1, a.c1), pk2(a.c2, a.c2), pk2(a.c3, a.c3),
+                            pk2(a.c4, a.c4)};
+          const f2 cl = lo2(c), ch = hi2(c);
+          const f2 s_wx = pk2(L.w, c.x), s_yz = pk2(c.y, c.z), s_wR = pk2(c.w, R.x);
+          const f2 s_Lyz = pk2(L.y, L.z), s_Ryz = pk2(R.y, R.z);
+          // z partners (+d, -d) of each pair, d = 1 .. 4
+          const f2 zp[2][4] = {{s_yz, ch, s_wR, lo2(R)}, {s_wR, lo2(R), s_Ryz, hi2(R)}};
+          const f2 zm[2][4] = {{s_wx, hi2(L), s_Lyz, lo2(L)}, {s_yz, cl, s_wx, hi2(L)}};
+          f2 tx2[2], tz2[2];
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-          const float cv = el(c, e);
-          float tx = fmul(a.c0, cv);
-          tx = fadd(tx, fmul(a.c1, fadd(el(q[5], e), el(q[3], e))));
-          tx = fadd(tx, fmul(a.c2, fadd(el(q[6], e), el(q[2], e))));
-          tx = fadd(tx, fmul(a.c3, fadd(el(q[7], e), el(q[1], e))));
-          tx = fadd(tx, fmul(a.c4, fadd(el(q[8], e), el(q[0], e))));
-          float tz = fmul(a.c0, cv);
-          tz = fadd(tz, fmul(a.c1, fadd(znb(L, c, R, e, 1), znb(L, c, R, e, -1))));
-          tz = fadd(tz, fmul(a.c2, fadd(znb(L, c, R, e, 2), znb(L, c, R, e, -2))));
-          tz = fadd(tz, fmul(a.c3, fadd(znb(L, c, R, e, 3), znb(L, c, R, e, -3))));
-          tz = fadd(tz, fmul(a.c4, fadd(znb(L, c, R, e, 4), znb(L, c, R, e, -4))));
-          const bool lap = lz_ok[e] && lx_ok;  // skipped cells vote with zeros
-          txs[e] = lap ? tx : 0.f;
-          tzs[e] = lap ? tz : 0.f;
+          for (int h = 0; h < 2; h++) {
+            const f2 cv2 = h ? ch : cl;
+            f2 tx = mul2(mul2(kc[0], cv2), k1);
+#pragma unroll
+            for (int d = 1; d <= 4; d++) {
+              const f2 xs = h ? add2(hi2(q[4 + d]), hi2(q[4 - d])) : add2(lo2(q[4 + d]), lo2(q[4 - d]));
+              tx = add2(tx, mul2(mul2(kc[d], xs), k1));
+            }
+            f2 tz = mul2(mul2(kc[0], cv2), k1);
+#pragma unroll
+            for (int d = 1; d <= 4; d++)
+              tz = add2(tz, mul2(mul2(kc[d], add2(zp[h][d - 1], zm[h][d - 1])), k1));
+            tx2[h] = tx;
+            tz2[h] = tz;
+          }
+          const float4 tx4 = join2(tx2[0], tx2[1]), tz4 = join2(tz2[0], tz2[1]);
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const bool lap = lz_ok[e] && lx_ok;  // skipped cells vote with zeros
+            txs[e] = lap ? el(tx4, e) : 0.f;
+            tzs[e] = lap ? el(tz4, e) : 0.f;
+          }
         }
         div4x2(txs, tzs, a.divx, a.divz, __activemask(), qx, qz);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
           const int iz = iz0 + e;
-          const float cv = el(c, e);
           float t = (lz_ok[e] && lx_ok) ? fadd(qx[e], qz[e]) : 0.f;
           if (MODE == FWD && PAS) {
             // gradient_pas_av (wave_fwigradient.c:732-737): the interior's source
@@ -399,11 +420,26 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
             t = fadd(t, a.res[((size_t)s * a.nt + a.it) * a.nr + rir]);
           }
           set_el(term4, e, t);
-          // b = S(a_{k-1} as stored): z faces then x faces (apply_sponge)
-          const float p = fmul(bxf, fmul(bzf[e], el(pv, e)));
-          float v = fadd(fsub(fmul(2.f, cv), p), fmul(el(V4, e), t));
-          v = fmul(bxf, fmul(bzf[e], v));
-          set_el(res4, e, zin[e] ? v : 0.f);
+        }
+        {
+          // b = S(a_{k-1} as stored): z faces then x faces (apply_sponge);
+          // 2 c as c + c (the same bits, and no product to fuse into the
+          // subtraction)
+          const f2 k1 = pk2(a.one, a.one), bx2 = pk2(bxf, bxf);
+          f2 r2[2];
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const f2 bz2 = pk2(bzf[2 * h], bzf[2 * h + 1]);
+            const f2 cv2 = h ? hi2(c) : lo2(c);
+            const f2 p = mul2(mul2(bx2, mul2(bz2, h ? hi2(pv) : lo2(pv))), k1);
+            const f2 vt = mul2(mul2(h ? hi2(V4) : lo2(V4), h ? hi2(term4) : lo2(term4)), k1);
+            const f2 v = add2(sub2(add2(cv2, cv2), p), vt);
+            r2[h] = mul2(bx2, mul2(bz2, v));
+          }
+          res4 = join2(r2[0], r2[1]);
+#pragma unroll
+          for (int e = 0; e < 4; e++)
+            if (!zin[e]) set_el(res4, e, 0.f);
         }
         *reinterpret_cast<float4 *>(nxt + o) = res4;
         if (MODE == FWD && a.tout)
@@ -411,11 +447,10 @@ __global__ void __launch_bounds__(ZW) pf_step_kernel(const PfArgs a, int xch) {
         if (MODE == ADJ_EXACT && a.imaging) {
           // dJ/dV accumulates phi_n * term_n (divided by V at the end)
           const float4 tf = s_t[(i % NP) * ZW + tid];
-          float4 gacc = s_g[(i % NP) * ZW + tid];  // read P planes ahead (cp.async)
-          gacc.x = fadd(gacc.x, fmul(c.x, tf.x));
-          gacc.y = fadd(gacc.y, fmul(c.y, tf.y));
-          gacc.z = fadd(gacc.z, fmul(c.z, tf.z));
-          gacc.w = fadd(gacc.w, fmul(c.w, tf.w));
+          const float4 g4 = s_g[(i % NP) * ZW + tid];  // read P planes ahead (cp.async)
+          const f2 k1 = pk2(a.one, a.one);
+          const float4 gacc = join2(add2(lo2(g4), mul2(mul2(lo2(c), lo2(tf)), k1)),
+                                    add2(hi2(g4), mul2(mul2(hi2(c), hi2(tf)), k1)));
           *reinterpret_cast<float4 *>(gs + o) = gacc;
         }
         if (MODE == ADJ_REF && img) {
@@ -1058,6 +1093,7 @@ static void base_args(const Setup &S, PfArgs &p) {
   p.c0 = c0; p.c1 = c1; p.c2 = c2; p.c3 = c3; p.c4 = c4;
   p.dx2 = S.a.dx * S.a.dx;
   p.dz2 = S.a.dz * S.a.dz;
+  p.one = 1.f;
   p.divx = S.divx;
   p.divz = S.divz;
   p.nt = S.a.nt;
@@ -2259,6 +2295,7 @@ struct Args {
   long long sx, sy, fstride;
   int nz4, ZT, nzc, ych;
   float c0, c1, c2, c3, c4, rdx2, rdz2, rdy2;
+  float one;  // 1.0f at run time: keeps packed products unfused (pk2 helpers)
   int nshots;
   const float *cur[MAXS3];
   float *nxt[MAXS3];
@@ -2395,28 +2432,49 @@ __global__ void __launch_bounds__(512) pf3_step_kernel(const __grid_constant__ A
       if (MODE == FWD && trace >= 0 && a.rec)
         a.rec[((size_t)s * a.nt + a.it) * a.nr + trace] = pf::el(c, a.rz - iz0);
       const bool src_here = src_zx && y >= sh.sy0 && y <= sh.sy1;
-      float4 term4, res4;
+      float4 term4, res4, lap4;
+      const f2 k1 = pk2(a.one, a.one);
+      {
+        // the 8th-order sums along x, z and y in the reference's order, and
+        // (tx / dx^2 + tz / dz^2) + ty / dy^2, for cells (0, 1) and (2, 3)
+        // of the float4 per f32x2 op; the z neighbours at odd distances are
+        // the float4s shifted by one cell
+        const f2 kc[5] = {pk2(a.c0, a.c0), pk2(a.c1, a.c1), pk2(a.c2, a.c2), pk2(a.c3, a.c3),
+                          pk2(a.c4, a.c4)};
+        const f2 rx2 = pk2(a.rdx2, a.rdx2), rz2 = pk2(a.rdz2, a.rdz2), ry2 = pk2(a.rdy2, a.rdy2);
+        const f2 cl = lo2(c), ch = hi2(c);
+        const f2 s_wx = pk2(L.w, c.x), s_yz = pk2(c.y, c.z), s_wR = pk2(c.w, R.x);
+        const f2 s_Lyz = pk2(L.y, L.z), s_Ryz = pk2(R.y, R.z);
+        const f2 zp[2][4] = {{s_yz, ch, s_wR, lo2(R)}, {s_wR, lo2(R), s_Ryz, hi2(R)}};
+        const f2 zm[2][4] = {{s_wx, hi2(L), s_Lyz, lo2(L)}, {s_yz, cl, s_wx, hi2(L)}};
+        const float4 *xp[4] = {&xp1, &xp2, &xp3, &xp4}, *xm[4] = {&xm1, &xm2, &xm3, &xm4};
+        f2 t2[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const f2 cv2 = h ? ch : cl;
+          f2 tx = mul2(mul2(kc[0], cv2), k1), tz = tx, ty = tx;
+#pragma unroll
+          for (int d = 1; d <= 4; d++) {
+            const f2 xs = h ? add2(hi2(*xp[d - 1]), hi2(*xm[d - 1]))
+                            : add2(lo2(*xp[d - 1]), lo2(*xm[d - 1]));
+            tx = add2(tx, mul2(mul2(kc[d], xs), k1));
+          }
+#pragma unroll
+          for (int d = 1; d <= 4; d++)
+            tz = add2(tz, mul2(mul2(kc[d], add2(zp[h][d - 1], zm[h][d - 1])), k1));
+#pragma unroll
+          for (int d = 1; d <= 4; d++) {
+            const f2 ys = h ? add2(hi2(q[4 + d]), hi2(q[4 - d])) : add2(lo2(q[4 + d]), lo2(q[4 - d]));
+            ty = add2(ty, mul2(mul2(kc[d], ys), k1));
+          }
+          const f2 sxz = add2(mul2(mul2(tx, rx2), k1), mul2(mul2(tz, rz2), k1));
+          t2[h] = add2(sxz, mul2(mul2(ty, ry2), k1));
+        }
+        lap4 = join2(t2[0], t2[1]);
+      }
 #pragma unroll
       for (int e = 0; e < 4; e++) {
-        const float cv = pf::el(c, e);
-        float tx = fmul(a.c0, cv);
-        tx = fadd(tx, fmul(a.c1, fadd(pf::el(xp1, e), pf::el(xm1, e))));
-        tx = fadd(tx, fmul(a.c2, fadd(pf::el(xp2, e), pf::el(xm2, e))));
-        tx = fadd(tx, fmul(a.c3, fadd(pf::el(xp3, e), pf::el(xm3, e))));
-        tx = fadd(tx, fmul(a.c4, fadd(pf::el(xp4, e), pf::el(xm4, e))));
-        float tz = fmul(a.c0, cv);
-        tz = fadd(tz, fmul(a.c1, fadd(pf::znb(L, c, R, e, 1), pf::znb(L, c, R, e, -1))));
-        tz = fadd(tz, fmul(a.c2, fadd(pf::znb(L, c, R, e, 2), pf::znb(L, c, R, e, -2))));
-        tz = fadd(tz, fmul(a.c3, fadd(pf::znb(L, c, R, e, 3), pf::znb(L, c, R, e, -3))));
-        tz = fadd(tz, fmul(a.c4, fadd(pf::znb(L, c, R, e, 4), pf::znb(L, c, R, e, -4))));
-        float ty = fmul(a.c0, cv);
-        ty = fadd(ty, fmul(a.c1, fadd(pf::el(q[5], e), pf::el(q[3], e))));
-        ty = fadd(ty, fmul(a.c2, fadd(pf::el(q[6], e), pf::el(q[2], e))));
-        ty = fadd(ty, fmul(a.c3, fadd(pf::el(q[7], e), pf::el(q[1], e))));
-        ty = fadd(ty, fmul(a.c4, fadd(pf::el(q[8], e), pf::el(q[0], e))));
-        float t = (lz_ok[e] && lx_ok && ly_ok)
-                      ? fadd(fadd(fmul(tx, a.rdx2), fmul(tz, a.rdz2)), fmul(ty, a.rdy2))
-                      : 0.f;
+        float t = (lz_ok[e] && lx_ok && ly_ok) ? pf::el(lap4, e) : 0.f;
         const int iz = iz0 + e;
         if (MODE == FWD) {
           if (src_here) {
@@ -2428,21 +2486,34 @@ __global__ void __launch_bounds__(512) pf3_step_kernel(const __grid_constant__ A
           t = fadd(t, a.res[((size_t)s * a.nt + a.it) * a.nr + trace]);
         }
         pf::set_el(term4, e, t);
-        const float p = fmul(byf, fmul(bxf, fmul(bzf[e], pf::el(pv, e))));
-        float v = fadd(fsub(fmul(2.f, cv), p), fmul(pf::el(V4, e), t));
-        v = fmul(byf, fmul(bxf, fmul(bzf[e], v)));
-        pf::set_el(res4, e, zin[e] ? v : 0.f);
+      }
+      {
+        // taper of the stored u_{k-1} (z, then x, then y faces), the update
+        // with 2 c as c + c (the same bits, no product to fuse), the taper
+        const f2 bx2 = pk2(bxf, bxf), by2 = pk2(byf, byf);
+        f2 r2[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const f2 bz2 = pk2(bzf[2 * h], bzf[2 * h + 1]);
+          const f2 cv2 = h ? hi2(c) : lo2(c);
+          const f2 p = mul2(mul2(by2, mul2(bx2, mul2(bz2, h ? hi2(pv) : lo2(pv)))), k1);
+          const f2 vt = mul2(mul2(h ? hi2(V4) : lo2(V4), h ? hi2(term4) : lo2(term4)), k1);
+          const f2 v = add2(sub2(add2(cv2, cv2), p), vt);
+          r2[h] = mul2(by2, mul2(bx2, mul2(bz2, v)));
+        }
+        res4 = join2(r2[0], r2[1]);
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+          if (!zin[e]) pf::set_el(res4, e, 0.f);
       }
       *reinterpret_cast<float4 *>(nxt + o) = res4;
       if (MODE == FWD && a.tout)
         *reinterpret_cast<float4 *>(a.tout + s * a.tout_stride + o) = term4;
       if (MODE == ADJ_EXACT) {
         const float4 tf = own[2 * nthr];
-        float4 g = own[3 * nthr];
-        g.x = fadd(g.x, fmul(c.x, tf.x));
-        g.y = fadd(g.y, fmul(c.y, tf.y));
-        g.z = fadd(g.z, fmul(c.z, tf.z));
-        g.w = fadd(g.w, fmul(c.w, tf.w));
+        const float4 g0 = own[3 * nthr];
+        const float4 g = join2(add2(lo2(g0), mul2(mul2(lo2(c), lo2(tf)), k1)),
+                               add2(hi2(g0), mul2(mul2(hi2(c), hi2(tf)), k1)));
         *reinterpret_cast<float4 *>(gs + o) = g;
       }
     }
@@ -2560,6 +2631,7 @@ static int setup3(const pw_fwi3d_args *a, Setup3 &S) {
   g.rdz2 = 1.f / (a->dz * a->dz);
   g.rdx2 = 1.f / (a->dx * a->dx);
   g.rdy2 = 1.f / (a->dy * a->dy);
+  g.one = 1.f;
   g.nt = a->nt;
   std::vector<float> bc(nb);
   for (int i = 0; i < nb; i++) {
