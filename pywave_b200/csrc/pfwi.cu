@@ -156,33 +156,45 @@ __device__ __forceinline__ float div_small(float x, const DivC &c) {
   return q;
 }
 
+// div_bmr on a pair: the same fused product and the sign of x per lane
+__device__ __forceinline__ f2 div_bmr2(f2 x, f2 zh, f2 zl) {
+  const f2 q = fma2(x, zh, mul2(x, zl));
+  return (q & 0x7fffffff7fffffffull) | (x & 0x8000000080000000ull);
+}
+
 // tx[e]/cx.d and tz[e]/cz.d for the 4 cells of a float4, correctly rounded.
 // The lanes of `mask` vote once: every numerator zero or in [xmin, xmax]
-// runs div_bmr; every one below xmax runs div_small or div_bmr per value;
-// otherwise __fdiv_rn (a per-value choice of all three would be if-converted
-// into every sequence).  Any grouping of lanes is correct, as every lane's
-// own vote is in its group.
+// runs div_bmr (two values per op); every one below xmax runs div_small or
+// div_bmr per value; otherwise __fdiv_rn (a per-value choice of all three
+// would be if-converted into every sequence).  Any grouping of lanes is
+// correct, as every lane's own vote is in its group.
 __device__ __forceinline__ void div4x2(const float (&tx)[4], const float (&tz)[4],
                                        const DivC &cx, const DivC &cz, unsigned mask,
                                        float (&qx)[4], float (&qz)[4]) {
-  // |x| in [xmin, xmax] is one unsigned compare on the bits of |x| (positive
-  // floats order as their bit patterns); bits 0 (x = +-0) are in range too
-  const bool ok = cx.ok && cz.ok;
-  bool in = ok, below = ok;
+  // |x| in [xmin, xmax] or 0 for all four: the largest |x| bits at most
+  // umax, and the smallest of |x| bits - 1 (a zero wraps to the top and
+  // drops out) at least umin - 1; positive floats order as their bits
+  unsigned mxx = 0u, mxz = 0u, mnx = ~0u, mnz = ~0u;
 #pragma unroll
   for (int e = 0; e < 4; e++) {
-    const unsigned int ux = __float_as_uint(tx[e]) & 0x7fffffffu;
-    const unsigned int uz = __float_as_uint(tz[e]) & 0x7fffffffu;
-    in = in && (ux - cx.umin <= cx.uspan || ux == 0u) && (uz - cz.umin <= cz.uspan || uz == 0u);
-    below = below && ux <= cx.umax && uz <= cz.umax;
+    const unsigned ux = __float_as_uint(tx[e]) & 0x7fffffffu;
+    const unsigned uz = __float_as_uint(tz[e]) & 0x7fffffffu;
+    mxx = max(mxx, ux);
+    mxz = max(mxz, uz);
+    mnx = min(mnx, ux - 1u);
+    mnz = min(mnz, uz - 1u);
   }
+  const bool ok = cx.ok && cz.ok;
+  const bool in = ok && mxx <= cx.umax && mxz <= cz.umax && mnx >= cx.umin - 1u &&
+                  mnz >= cz.umin - 1u;
   if (__all_sync(mask, in)) {
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      qx[e] = div_bmr(tx[e], cx);
-      qz[e] = div_bmr(tz[e], cz);
-    }
-  } else if (__all_sync(mask, below)) {
+    const f2 xh = pk2(cx.zh, cx.zh), xl = pk2(cx.zl, cx.zl);
+    const f2 zh = pk2(cz.zh, cz.zh), zl = pk2(cz.zl, cz.zl);
+    up2(div_bmr2(pk2(tx[0], tx[1]), xh, xl), qx[0], qx[1]);
+    up2(div_bmr2(pk2(tx[2], tx[3]), xh, xl), qx[2], qx[3]);
+    up2(div_bmr2(pk2(tz[0], tz[1]), zh, zl), qz[0], qz[1]);
+    up2(div_bmr2(pk2(tz[2], tz[3]), zh, zl), qz[2], qz[3]);
+  } else if (__all_sync(mask, ok && mxx <= cx.umax && mxz <= cz.umax)) {
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       const bool sx = (__float_as_uint(tx[e]) & 0x7fffffffu) < cx.umin;

@@ -171,6 +171,12 @@ __device__ __forceinline__ f2 mul2(f2 a, f2 b) {
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
   return r;
 }
+// fused a * b + c per lane, one rounding (fma.rn.f32x2)
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+  f2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
 __device__ __forceinline__ f2 lo2(const float4 &v) { return pk2(v.x, v.y); }
 __device__ __forceinline__ f2 hi2(const float4 &v) { return pk2(v.z, v.w); }
 __device__ __forceinline__ float4 join2(f2 l, f2 h) {
