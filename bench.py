@@ -204,6 +204,9 @@ def reference_sample(n, path, workers):
     Returns (Gpt/s over all workers, kind, per-step seconds, set-up seconds)."""
     res = pool_map(_ref_worker, [(n, path)] * workers)
     d = max(r[1] - r[0] for r in res)  # slowest worker's extra-steps time
+    if d <= 0:
+        raise RuntimeError(f"reference timing: {REF_STEPS[1]} steps took no longer than "
+                           f"{REF_STEPS[0]} ({res})")
     kind = res[0][2]
     extra = REF_STEPS[1] - REF_STEPS[0]
     pts = (n + 2 * NBT) ** 3 * extra * workers
@@ -234,6 +237,7 @@ def _ref_worker(n, path):
     except ImportError:
         from oracle import oracle as O
         kind = "port"
+        O.lib()  # load (and if needed compile) the port before the timed calls
         for nt_s in REF_STEPS:
             t0 = time.perf_counter()
             O.afd(vel, nt_s, DT, (H, H, H), nbt=NBT, ct=CT, tri=True, dat=dat[-nt_s:], jsnap=4)
