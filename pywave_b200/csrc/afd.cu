@@ -117,6 +117,74 @@ template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Two cells per f32x2 op for the march and resident kernels (pk2 helpers;
+// k1 is the runtime 1.0 of StepArgs::one).  lap_quad: the 4th-order
+// Laplacian of the float4 c in the reference's order (y, then x when XT,
+// then z terms), with (Lz, Lw) the two cells below c and (Rx, Ry) the two
+// above; y1 / y2 are the float4s at y +- 1 / y +- 2.
+template <bool XT>
+__device__ __forceinline__ float4 lap_quad(const StepArgs &a, f2 k1, const float4 &c,
+                                           const float4 &ym1, const float4 &yp1,
+                                           const float4 &ym2, const float4 &yp2,
+                                           const float4 &xm1, const float4 &xp1,
+                                           const float4 &xm2, const float4 &xp2, float Lz,
+                                           float Lw, float Rx, float Ry) {
+  const f2 kc0 = pk2(a.c0, a.c0), kc1 = pk2(a.c1, a.c1), kc2 = pk2(a.c2, a.c2);
+  const f2 kk0 = pk2(a.k0, a.k0), kx = pk2(a.idx, a.idx), ky = pk2(a.idy, a.idy);
+  const f2 kz = pk2(a.idz, a.idz);
+  const f2 zb = pk2(c.y, c.z);
+  const f2 z1[2] = {add2(pk2(Lw, c.x), zb), add2(zb, pk2(c.w, Rx))};
+  const f2 z2[2] = {add2(pk2(Lz, Lw), hi2(c)), add2(lo2(c), pk2(Rx, Ry))};
+  f2 t[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    auto P = [h](const float4 &v) { return h ? hi2(v) : lo2(v); };
+    f2 tt = mul2(mul2(mul2(kc0, P(c)), kk0), k1);
+    tt = add2(tt, mul2(mul2(mul2(kc1, add2(P(ym1), P(yp1))), ky), k1));
+    tt = add2(tt, mul2(mul2(mul2(kc2, add2(P(ym2), P(yp2))), ky), k1));
+    if (XT) {
+      tt = add2(tt, mul2(mul2(mul2(kc1, add2(P(xm1), P(xp1))), kx), k1));
+      tt = add2(tt, mul2(mul2(mul2(kc2, add2(P(xm2), P(xp2))), kx), k1));
+    }
+    tt = add2(tt, mul2(mul2(mul2(kc1, z1[h]), kz), k1));
+    tt = add2(tt, mul2(mul2(mul2(kc2, z2[h]), kz), k1));
+    t[h] = tt;
+  }
+  return join2(t[0], t[1]);
+}
+// The leapfrog update before any injection, c + (c - b) + lap vv, with b the
+// stored u_{k-1} tapered face by face (wz per cell, then wx when XT, then wy).
+template <bool XT>
+__device__ __forceinline__ float4 update_quad(f2 k1, const float4 &c, const float4 &pv,
+                                              const float4 &lap, const float4 &vv,
+                                              const float (&wz)[4], float wx, float wy) {
+  const f2 wx2 = pk2(wx, wx), wy2 = pk2(wy, wy);
+  f2 r[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    auto P = [h](const float4 &v) { return h ? hi2(v) : lo2(v); };
+    f2 b = mul2(P(pv), pk2(wz[2 * h], wz[2 * h + 1]));
+    if (XT) b = mul2(b, wx2);
+    b = mul2(mul2(b, wy2), k1);
+    r[h] = add2(add2(P(c), sub2(P(c), b)), mul2(mul2(P(lap), P(vv)), k1));
+  }
+  return join2(r[0], r[1]);
+}
+// The taper of the updated cells, face by face (wz, then wx when XT, then wy).
+template <bool XT>
+__device__ __forceinline__ float4 taper_quad(const float4 &v, const float (&wz)[4], float wx,
+                                             float wy) {
+  const f2 wx2 = pk2(wx, wx), wy2 = pk2(wy, wy);
+  f2 r[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    f2 t = mul2(h ? hi2(v) : lo2(v), pk2(wz[2 * h], wz[2 * h + 1]));
+    if (XT) t = mul2(t, wx2);
+    r[h] = mul2(t, wy2);
+  }
+  return join2(r[0], r[1]);
+}
+
 // March kernel: register-marched, one float4 of z cells per thread.
 //
 // Lanes map onto (z float4 slot, group) with the G receiver groups of a TRI
@@ -260,31 +328,17 @@ __device__ __forceinline__ void march_body(const StepArgs &a, int bx, int by, fl
     bool src_plane = false;
     if (!TRI)
       for (int s = 0; s < a.ns; s++) src_plane |= (y >= a.sy[s] - 1 && y <= a.sy[s] + 1);
-    float4 res;
+    // prev = taper(u_{k-1} as stored); x1.0 outside the faces is exact
+    const f2 k1 = pk2(a.one, a.one);
+    float4 lap = lap_quad<!TWO_D>(a, k1, q2, q1, q3, q0, q4, xm1, xp1, xm2, xp2, Lz, Lw, Rx, Ry);
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (!(lzm[e] && lxm && lyok)) set_el(lap, e, 0.f);
+    float4 res = update_quad<!TWO_D>(k1, q2, pv, lap, vv4, wz, wx, wy);
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      const float cv = el(q2, e);
-      const float zm1 = e == 0 ? Lw : el(q2, e - 1);
-      const float zp1 = e == 3 ? Rx : el(q2, e + 1);
-      const float zm2 = e == 0 ? Lz : (e == 1 ? Lw : el(q2, e - 2));
-      const float zp2 = e == 2 ? Rx : (e == 3 ? Ry : el(q2, e + 2));
-      float tt = fmul(fmul(a.c0, cv), a.k0);
-      tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
-      tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
-      if (!TWO_D) {
-        tt = fadd(tt, fmul(fmul(a.c1, fadd(el(xm1, e), el(xp1, e))), a.idx));
-        tt = fadd(tt, fmul(fmul(a.c2, fadd(el(xm2, e), el(xp2, e))), a.idx));
-      }
-      tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-      tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-      const float lap = (lzm[e] && lxm && lyok) ? tt : 0.f;
-      // prev = taper(u_{k-1} as stored); x1.0 outside the faces is exact
-      float p = fmul(el(pv, e), wz[e]);
-      if (!TWO_D) p = fmul(p, wx);
-      p = fmul(p, wy);
       const float vve = el(vv4, e);
-      float v = fadd(cv, fsub(cv, p));
-      v = fadd(v, fmul(lap, vve));
+      float v = el(res, e);
       if (TRI) {
         if (inj && e == erz) v = fadd(v, fmul(vve, dval));
       } else if (src_plane) {
@@ -297,11 +351,12 @@ __device__ __forceinline__ void march_body(const StepArgs &a, int bx, int by, fl
           }
         }
       }
-      v = fmul(v, wz[e]);
-      if (!TWO_D) v = fmul(v, wx);
-      v = fmul(v, wy);
-      set_el(res, e, keep[e] ? v : 0.f);
+      set_el(res, e, v);
     }
+    res = taper_quad<!TWO_D>(res, wz, wx, wy);
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (!keep[e]) set_el(res, e, 0.f);
     if (live) *reinterpret_cast<float4 *>(B + o) = res;
     if (!TRI && rec_here && a.rec && gi == 0) a.rec[(size_t)a.it * nrec + r_idx] = el(res, erz);
     if (SNAP) {
@@ -520,25 +575,16 @@ __global__ void __launch_bounds__(RES_NTH) resident_kernel(const __grid_constant
           inj = a.gid == nullptr ? gi == 0 : a.gid[r_idx] == gi;
           if (inj) dval = a.tri_dat[(size_t)it * nrec + r_idx];
         }
-        float4 res;
+        const f2 k1 = pk2(a.one, a.one);
+        float4 lap = lap_quad<false>(a, k1, q2, q1, q3, q0, q4, q2, q2, q2, q2, Lz, Lw, Rx, Ry);
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+          if (!((f & (2u << e)) && lyok)) set_el(lap, e, 0.f);
+        float4 res = update_quad<false>(k1, q2, pv, lap, vv4, wz, 1.f, wy);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-          const float cv = el(q2, e);
-          const float zm1 = e == 0 ? Lw : el(q2, e - 1);
-          const float zp1 = e == 3 ? Rx : el(q2, e + 1);
-          const float zm2 = e == 0 ? Lz : (e == 1 ? Lw : el(q2, e - 2));
-          const float zp2 = e == 2 ? Rx : (e == 3 ? Ry : el(q2, e + 2));
-          float tt = fmul(fmul(a.c0, cv), a.k0);
-          tt = fadd(tt, fmul(fmul(a.c1, fadd(el(q1, e), el(q3, e))), a.idy));
-          tt = fadd(tt, fmul(fmul(a.c2, fadd(el(q0, e), el(q4, e))), a.idy));
-          tt = fadd(tt, fmul(fmul(a.c1, fadd(zm1, zp1)), a.idz));
-          tt = fadd(tt, fmul(fmul(a.c2, fadd(zm2, zp2)), a.idz));
-          const float lap = ((f & (2u << e)) && lyok) ? tt : 0.f;
-          float pp = fmul(el(pv, e), wz[e]);
-          pp = fmul(pp, wy);
           const float vve = el(vv4, e);
-          float v = fadd(cv, fsub(cv, pp));
-          v = fadd(v, fmul(lap, vve));
+          float v = el(res, e);
           if (TRI) {
             if (inj && e == erz) v = fadd(v, fmul(vve, dval));
           } else if (src_plane) {
@@ -551,10 +597,12 @@ __global__ void __launch_bounds__(RES_NTH) resident_kernel(const __grid_constant
               }
             }
           }
-          v = fmul(v, wz[e]);
-          v = fmul(v, wy);
-          set_el(res, e, (f & (32u << e)) ? v : 0.f);
+          set_el(res, e, v);
         }
+        res = taper_quad<false>(res, wz, 1.f, wy);
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+          if (!(f & (32u << e))) set_el(res, e, 0.f);
         nxt[o4] = res;
         // the neighbours' halo copies of the two edge columns
         if (f & (1u << 13)) *dsmem_map(nxt + o4 + w * LZ4, rank - 1) = res;
