@@ -56,6 +56,7 @@ struct Args {
   int nz, nx, nt, nb, depth;
   float sx, sz;      // 1/dx^2, 1/dz^2 as the reference rounds them
   float c0, c1, c2, c3, c4;
+  float one;         // 1.0f at run time: keeps packed products unfused (pk2 helpers)
   const float4 *vv;  // [nxp][nq] quads of vvpad = (v v) dt^2, zero beyond nzp
   const float4 *wz;  // [nq] z sponge factors (1 inside, and beyond nzp)
   const float *wx;   // [nxp] x sponge factors
@@ -104,55 +105,83 @@ __device__ __forceinline__ unsigned quad_flags(const Args &a, int ix, int k) {
   return f;
 }
 
-// The 8th-order sums of Lap (ADJ = false: plain samples, times the centre's
-// vv at the end) or LapT (ADJ = true: every sample times its own vv) for
-// element e of the quad.  ux[4] / vx[4] is the quad's own column, ux[4 +- d]
-// the columns +-d; uzl / uzh (vzl / vzh) the quads below / above.
-template <bool ADJ>
-__device__ __forceinline__ float lap_e(const Args &a, const float4 (&ux)[9], const float4 &uzl,
-                                       const float4 &uzh, const float4 (&vx)[9], const float4 &vzl,
-                                       const float4 &vzh, int e) {
-#define TX(i) (ADJ ? fmul(qel(ux[i], e), qel(vx[i], e)) : qel(ux[i], e))
-#define TZ(j) (ADJ ? fmul(zwin(uzl, ux[4], uzh, e + (j)), zwin(vzl, vx[4], vzh, e + (j))) \
-                   : zwin(uzl, ux[4], uzh, e + (j)))
-  float xs = fmul(a.c4, fadd(TX(8), TX(0)));
-  xs = fadd(xs, fmul(a.c3, fadd(TX(7), TX(1))));
-  xs = fadd(xs, fmul(a.c2, fadd(TX(6), TX(2))));
-  xs = fadd(xs, fmul(a.c1, fadd(TX(5), TX(3))));
-  xs = fadd(xs, fmul(a.c0, TX(4)));
-  float zs = fmul(a.c4, fadd(TZ(4), TZ(-4)));
-  zs = fadd(zs, fmul(a.c3, fadd(TZ(3), TZ(-3))));
-  zs = fadd(zs, fmul(a.c2, fadd(TZ(2), TZ(-2))));
-  zs = fadd(zs, fmul(a.c1, fadd(TZ(1), TZ(-1))));
-  zs = fadd(zs, fmul(a.c0, TZ(0)));
-#undef TX
-#undef TZ
-  const float r = fadd(fmul(xs, a.sx), fmul(zs, a.sz));
-  return ADJ ? r : fmul(r, qel(vx[4], e));
-}
-
-// A' of the quad.  inj: modelling, the source samples of the interior cells
-// (mod[it]); adjoint, element 0 the data sample of the data row.
+// A' of the quad, two cells per f32x2 op (pk2 helpers).  The 8th-order sums
+// of Lap (ADJ = false: plain samples, the sum times the centre's vv) or LapT
+// (ADJ = true: every sample times its own vv) in the reference's order;
+// ux[4] / vx[4] is the quad's own column, ux[4 +- d] the columns +-d, uzl /
+// uzh (vzl / vzh) the quads below / above.  Every product that is added is
+// multiplied by the runtime 1.0 first, and 2 u is formed as u + u.  Cells
+// outside the stencil stay zero.  inj: modelling, the source samples of the
+// interior cells (mod[it]); adjoint, element 0 the data sample of the data
+// row.
 template <bool ADJ>
 __device__ __forceinline__ float4 quad_step(const Args &a, unsigned f, const float4 (&ux)[9],
                                             const float4 &uzl, const float4 &uzh,
                                             const float4 (&vx)[9], const float4 &vzl,
                                             const float4 &vzh, const float4 &B, const float4 &wz4,
                                             float wxv, const float4 &inj, int k) {
-  float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+  const f2 k1 = pk2(a.one, a.one);
+  const f2 kc[5] = {pk2(a.c0, a.c0), pk2(a.c1, a.c1), pk2(a.c2, a.c2), pk2(a.c3, a.c3),
+                    pk2(a.c4, a.c4)};
+  // z partners (+d, -d), d = 1..4, of each pair of cells: the quads shifted
+  const float4 &c = ux[4], &L = uzl, &R = uzh;
+  const f2 u_yz = pk2(c.y, c.z), u_wx = pk2(L.w, c.x), u_wR = pk2(c.w, R.x);
+  const f2 zpu[2][4] = {{u_yz, hi2(c), u_wR, lo2(R)}, {u_wR, lo2(R), pk2(R.y, R.z), hi2(R)}};
+  const f2 zmu[2][4] = {{u_wx, hi2(L), pk2(L.y, L.z), lo2(L)}, {u_yz, lo2(c), u_wx, hi2(L)}};
+  f2 zpv[2][4], zmv[2][4];
+  if (ADJ) {
+    const float4 &cv = vx[4], &Lv = vzl, &Rv = vzh;
+    const f2 v_yz = pk2(cv.y, cv.z), v_wx = pk2(Lv.w, cv.x), v_wR = pk2(cv.w, Rv.x);
+    const f2 p0[4] = {v_yz, hi2(cv), v_wR, lo2(Rv)}, p1[4] = {v_wR, lo2(Rv), pk2(Rv.y, Rv.z), hi2(Rv)};
+    const f2 m0[4] = {v_wx, hi2(Lv), pk2(Lv.y, Lv.z), lo2(Lv)}, m1[4] = {v_yz, lo2(cv), v_wx, hi2(Lv)};
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      zpv[0][d] = p0[d];
+      zpv[1][d] = p1[d];
+      zmv[0][d] = m0[d];
+      zmv[1][d] = m1[d];
+    }
+  }
+  const f2 sx = pk2(a.sx, a.sx), sz = pk2(a.sz, a.sz), wx2 = pk2(wxv, wxv);
+  f2 n2[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    auto P = [h](const float4 &v) { return h ? hi2(v) : lo2(v); };
+    // sample i of the x window and the z sample pair at +-d (times vv for LapT)
+    auto tx = [&](int i) { return ADJ ? mul2(mul2(P(ux[i]), P(vx[i])), k1) : P(ux[i]); };
+    auto tzp = [&](int d) { return ADJ ? mul2(mul2(zpu[h][d - 1], zpv[h][d - 1]), k1) : zpu[h][d - 1]; };
+    auto tzm = [&](int d) { return ADJ ? mul2(mul2(zmu[h][d - 1], zmv[h][d - 1]), k1) : zmu[h][d - 1]; };
+    const f2 t0 = ADJ ? mul2(mul2(P(ux[4]), P(vx[4])), k1) : P(ux[4]);
+    f2 xs = mul2(mul2(kc[4], add2(tx(8), tx(0))), k1);
+    xs = add2(xs, mul2(mul2(kc[3], add2(tx(7), tx(1))), k1));
+    xs = add2(xs, mul2(mul2(kc[2], add2(tx(6), tx(2))), k1));
+    xs = add2(xs, mul2(mul2(kc[1], add2(tx(5), tx(3))), k1));
+    xs = add2(xs, mul2(mul2(kc[0], t0), k1));
+    f2 zs = mul2(mul2(kc[4], add2(tzp(4), tzm(4))), k1);
+    zs = add2(zs, mul2(mul2(kc[3], add2(tzp(3), tzm(3))), k1));
+    zs = add2(zs, mul2(mul2(kc[2], add2(tzp(2), tzm(2))), k1));
+    zs = add2(zs, mul2(mul2(kc[1], add2(tzp(1), tzm(1))), k1));
+    zs = add2(zs, mul2(mul2(kc[0], t0), k1));
+    f2 lap = add2(mul2(mul2(xs, sx), k1), mul2(mul2(zs, sz), k1));
+    if (!ADJ) lap = mul2(mul2(lap, P(vx[4])), k1);
+    const f2 u0 = mul2(mul2(mul2(P(B), P(wz4)), wx2), k1);
+    n2[h] = sub2(add2(lap, add2(P(ux[4]), P(ux[4]))), u0);
+  }
+  float4 n = join2(n2[0], n2[1]);
 #pragma unroll
   for (int e = 0; e < 4; e++) {
-    if (!(f & (2u << e))) continue;
-    const float lap = lap_e<ADJ>(a, ux, uzl, uzh, vx, vzl, vzh, e);
-    const float u0 = fmul(fmul(qel(B, e), qel(wz4, e)), wxv);
-    float n = fsub(fadd(lap, fmul(2.f, qel(ux[4], e))), u0);
+    float v = qel(n, e);
     if (!ADJ) {
-      if (f & (32u << e)) n = fadd(n, fmul(qel(inj, e), qel(vx[4], e)));
+      if (f & (32u << e)) v = fadd(v, fmul(qel(inj, e), qel(vx[4], e)));
     } else {
-      if ((f & (1u << 9)) && e == a.depth - 4 * k) n = fadd(n, inj.x);
+      if ((f & (1u << 9)) && e == a.depth - 4 * k) v = fadd(v, inj.x);
     }
-    qset(r, e, fmul(fmul(n, qel(wz4, e)), wxv));
+    qset(n, e, v);
   }
+  float4 r = join2(mul2(mul2(lo2(n), lo2(wz4)), wx2), mul2(mul2(hi2(n), hi2(wz4)), wx2));
+#pragma unroll
+  for (int e = 0; e < 4; e++)
+    if (!(f & (2u << e))) qset(r, e, 0.f);
   return r;
 }
 
@@ -557,6 +586,7 @@ static void base_args(const pw_fwi_args *a, const Plan &p, Args &g, std::vector<
   g.c2 = n1 / 5.0f;
   g.c3 = p8 / 315.0f;
   g.c4 = n1 / 560.0f;
+  g.one = 1.f;
   std::vector<float> decay(a->nb);
   for (int ib = 0; ib < a->nb; ib++) {
     const float c = a->coef;
