@@ -164,7 +164,7 @@ def test_config2_grid_tri_image_vs_oracle(oracle, cuda_lib, monkeypatch, capfd):
     assert np.count_nonzero(ref32) > 0.01 * ref32.size
     ref64 = _oracle_group_runs(oracle, vel, d, groups, ng, nt, "f64")
     e64, o64 = rel_l2(img, ref64), rel_l2(ref32, ref64)
-    print(f"config-2 grid TRI image (nt {nt}): rel-L2 vs FP32 oracle {e32:.2e}; "
+    print(f"201^3 benchmark grid TRI image (nt {nt}): rel-L2 vs FP32 oracle {e32:.2e}; "
           f"vs FP64 oracle: GPU {e64:.2e}, FP32 oracle {o64:.2e}")
     assert e32 <= 1e-5
     assert e64 <= 1e-4
