@@ -1071,9 +1071,13 @@ static int launch_one(const Setup &S, const PfArgs &p, cudaStream_t st) {
     attr = true;
   }
   // x planes per CTA: long enough to amortise the 8-plane prologue, short
-  // enough that shots x chunks x z tiles fill every SM a few times
+  // enough that shots x chunks x z tiles fill every SM a few times.  Small
+  // batches go down to one plane per CTA: a step is then a few dependent
+  // plane updates instead of a long chain (the passive demos' grid, 3 shots:
+  // 175 ms per gradient at 16 planes, 46 ms at 1), the re-read halo planes
+  // staying in L2
   int xch = 128;
-  while (xch > 16 && (long long)p.nshots * S.ztiles * ceil_div(S.pnx, xch) < 6LL * S.nsm) xch /= 2;
+  while (xch > 1 && (long long)p.nshots * S.ztiles * ceil_div(S.pnx, xch) < 6LL * S.nsm) xch /= 2;
   const dim3 grid(p.nshots, ceil_div(S.pnx, xch), S.ztiles);
   pf_step_kernel<ZW, PFP, MODE, PAS><<<grid, ZW, smem, st>>>(p, xch);
   PW_CUDA(cudaGetLastError());
