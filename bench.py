@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--fwi3d-shots", type=int, default=16, help="fwi3d: shots per gradient")
     p.add_argument("--shots", type=int, default=32, help="fwi2d: shots per gradient")
     p.add_argument("--fwi-nt", type=int, default=2000, help="fwi2d: time samples")
+    p.add_argument("--b2-nt", type=int, default=0,
+                   help="batch2d: cut every shot's time samples to this many (0: as drawn)")
     return p.parse_args()
 
 
@@ -664,6 +666,9 @@ def _b2_cpu_sample(workers, nt_s=100):
 
 def run_batch2d(args, world, rank, local):
     shots = batch2d_shots(5 + rank)
+    if args.b2_nt > 0:
+        for sh in shots:
+            sh["nt"] = min(sh["nt"], args.b2_nt)
     cells = sum(_b2_cells(sh) for sh in shots)
     if args.impl == "reference":
         if rank != 0:
@@ -681,7 +686,8 @@ def run_batch2d(args, world, rank, local):
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{len(shots)} 2-D shots, grids 256-1024 x 256-2048, "
-                                   f"nt 1000-4000, h=10m, nbt={B2_NBT}"},
+                                   f"nt {'1000-4000' if args.b2_nt <= 0 else f'cut to {args.b2_nt}'}, "
+                                   f"h=10m, nbt={B2_NBT}"},
             "cpu_baseline": {"value": value, "unit": "Gpt/s", "cores": workers, "kind": kind,
                              "sample": f"afd2dc on a {B2_CROP}^2 crop of the largest shot, 100 "
                                        f"steps, {workers} independent single-threaded processes"},
@@ -787,7 +793,8 @@ def run_batch2d(args, world, rank, local):
             "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded layered models, Ricker sources)",
-            "config": {"workload": f"{n} 2-D shots, grids 256-1024 x 256-2048, nt 1000-4000, "
+            "config": {"workload": f"{n} 2-D shots, grids 256-1024 x 256-2048, "
+                                   f"nt {'1000-4000' if args.b2_nt <= 0 else f'cut to {args.b2_nt}'}, "
                                    f"h=10m dt=1ms nbt={B2_NBT}, one lockstep batch",
                        "cell_updates_per_step": cells,
                        "l2": "inputs larger than L2 (fields of all shots)"},
