@@ -1071,13 +1071,14 @@ static int launch_one(const Setup &S, const PfArgs &p, cudaStream_t st) {
     attr = true;
   }
   // x planes per CTA: long enough to amortise the 8-plane prologue, short
-  // enough that shots x chunks x z tiles fill every SM a few times.  Small
-  // batches go down to one plane per CTA: a step is then a few dependent
-  // plane updates instead of a long chain (the passive demos' grid, 3 shots:
-  // 175 ms per gradient at 16 planes, 46 ms at 1), the re-read halo planes
-  // staying in L2
+  // enough that shots x chunks x z tiles give every SM 12 CTAs (about three
+  // waves of the 4 that fit).  Small batches go down to one plane per CTA:
+  // a step is then a few dependent plane updates instead of a long chain
+  // (the passive demos' grid, 3 shots: 175 ms per gradient at 16 planes,
+  // 46 ms at 1), the re-read halo planes staying in L2; 32 shots of 420 x
+  // 720 run 8 planes (2.94 gradients/s, 2.69 at 16)
   int xch = 128;
-  while (xch > 1 && (long long)p.nshots * S.ztiles * ceil_div(S.pnx, xch) < 6LL * S.nsm) xch /= 2;
+  while (xch > 1 && (long long)p.nshots * S.ztiles * ceil_div(S.pnx, xch) < 12LL * S.nsm) xch /= 2;
   const dim3 grid(p.nshots, ceil_div(S.pnx, xch), S.ztiles);
   pf_step_kernel<ZW, PFP, MODE, PAS><<<grid, ZW, smem, st>>>(p, xch);
   PW_CUDA(cudaGetLastError());
