@@ -48,11 +48,13 @@ def parse():
     p.add_argument("--no-fwi2d", action="store_true",
                    help="tri3d: skip the secondary 2-D FWI gradients/s field")
     p.add_argument("--workload", default="tri3d",
-                   choices=["tri3d", "fwi2d", "batch2d", "c1", "fwi3d", "lstri", "pfwic", "aps3d"],
+                   choices=["tri3d", "fwi2d", "batch2d", "c1", "fwi3d", "lstri", "pfwic", "aps3d",
+                            "afd3d"],
                    help="tri3d: the 3-D TRI image (default); fwi2d: 2-D FWI gradients/s; "
                         "batch2d: uneven 2-D forward shots in one batch; c1: one 2-D shot; "
                         "fwi3d: 3-D FWI gradients/s; lstri: pfwi mode 4 source inversion; "
-                        "pfwic: pfwi mode 4 passive FWI gradients/s; aps3d: pseudo-spectral 3-D")
+                        "pfwic: pfwi mode 4 passive FWI gradients/s; aps3d: pseudo-spectral 3-D; "
+                        "afd3d: 3-D forward modelling of the tri3d model")
     p.add_argument("--lstri-niter", type=int, default=30, help="lstri: CG iterations per shot")
     p.add_argument("--lstri-nt", type=int, default=3001, help="lstri / pfwic: time samples")
     p.add_argument("--fwi3d-nt", type=int, default=2500, help="fwi3d: time samples")
@@ -979,6 +981,191 @@ def run_c1(args, world, rank, local):
 
 
 # --------------------------------------------------------------------------
+# afd3d: 3-D forward modelling of the headline's model (traces of 3 sources)
+# --------------------------------------------------------------------------
+def a3_sources(pos, f, t):
+    """The afd3d source array (sx, sy, sz, f, t, A rows) of c2_model's shots."""
+    return np.concatenate([pos[:, 0], pos[:, 1], pos[:, 2], f, t, np.ones(3)]).astype(np.float32)
+
+
+def _a3_ref_worker(n, nt_s, kind):
+    """Forward modelling of the 3 sources by the reference's afd3dc
+    (oracle/_ref; kind "port": the oracle's C restatement) for nt_s steps;
+    wall seconds."""
+    sys.path.insert(0, ROOT)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    vel, pos, f, t = c2_model(n, 1234, nt_s)
+    src = a3_sources(pos, f, t)
+    if kind == "reference":
+        sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+        import afdcfun  # the reference's own extension module
+        t0 = time.perf_counter()
+        afdcfun.afd3dc(vel.flatten(order="F"), src, 0, nt_s, n, n, n, 3, 0, 0, 0, 1, NBT, CT, DT,
+                       0.0, H, 0.0, H, 0.0, H)
+    else:
+        from oracle import oracle as O
+        O.lib()
+        t0 = time.perf_counter()
+        O.afd(vel, nt_s, DT, (H, H, H), nbt=NBT, ct=CT,
+              src=dict(sx=pos[:, 0], sy=pos[:, 1], sz=pos[:, 2], f=f, t=t, A=np.ones(3)))
+    return time.perf_counter() - t0
+
+
+def _a3_cpu(n, workers):
+    """Per-step rate of the reference's 3-D forward in `workers` processes:
+    calls of REF_STEPS[0] and REF_STEPS[1] steps, their difference excluding
+    the per-call set-up.  Returns (Gpt/s, kind, seconds per step)."""
+    for kind in ("reference", "port"):
+        try:
+            a = pool_map(_a3_ref_worker, [(n, REF_STEPS[0], kind)] * workers, timeout_s=600)
+            b = pool_map(_a3_ref_worker, [(n, REF_STEPS[1], kind)] * workers, timeout_s=600)
+        except Exception:  # noqa: BLE001
+            continue
+        d = max(b) - max(a)
+        if d <= 0:
+            raise RuntimeError(f"reference timing: {REF_STEPS[1]} steps took no longer than "
+                               f"{REF_STEPS[0]}")
+        extra = REF_STEPS[1] - REF_STEPS[0]
+        return (n + 2 * NBT) ** 3 * extra * workers / d / 1e9, kind, d / extra
+    raise RuntimeError("neither the reference nor the port ran")
+
+
+def run_afd3d(args, world, rank, local):
+    n, nt = args.n, args.nt
+    pts = (n + 2 * NBT) ** 3 * nt
+    metric = "Gpt-updates/s (3-D forward modelling, 3 sources)"
+    workload = (f"3-D forward modelling {n}^3 h=10m nt={nt} nbt={NBT}, the TRI benchmark's "
+                "velocity model, 3 seeded Ricker sources, receivers on the surface")
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        workers = max(1, min(os.cpu_count() or 1, 16))
+        rates, per = [], []
+        for i in range(args.warmup + args.steps):
+            v, kind, ps = _a3_cpu(n, workers)
+            if i >= args.warmup:
+                rates.append(v)
+                per.append(ps)
+        value = statistics.median(rates)
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": value, "unit": "Gpt/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": workload},
+            "cpu_baseline": {"value": value, "unit": "Gpt/s", "cores": workers, "kind": kind,
+                             "sample": f"afd3dc forward, {workers} independent single-threaded "
+                                       f"processes, calls of {REF_STEPS[0]} and {REF_STEPS[1]} "
+                                       f"steps ({statistics.median(per):.3f} s per step from "
+                                       "their difference)"},
+            "e2e": {"value": value, "unit": "Gpt/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+    from pywave_b200 import _lib as L
+    from pywave_b200 import build as B
+    B.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lib = L.lib()
+    vel, pos, f, t = c2_model(n, 1234 + rank, nt)
+    src = a3_sources(pos, f, t)
+    a = L.AfdArgs(dim=3, nz=n, nx=n, ny=n, nt=nt, nbt=NBT, ct=CT, dt=DT, dz=H, dx=H, dy=H, ns=3,
+                  tri=0, jsnap=0, gz=0, flags=0)
+    v_d = torch.from_numpy(np.ascontiguousarray(vel.flatten(order="F"))).cuda()
+    s_d = torch.from_numpy(src).cuda()
+    d_d = torch.empty(n * n * nt, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+
+    def shot():
+        L.check(lib.pw_afd(C.byref(a), v_d.data_ptr(), s_d.data_ptr(), None, d_d.data_ptr(),
+                           None, st))
+        return L.last_timing()
+
+    for _ in range(args.warmup):
+        shot()
+    clk = Clocks(local)
+    clk.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    loops, launches = [], 0
+    e0.record()
+    for _ in range(args.steps):
+        ms, nst, tot = shot()
+        loops.append(ms)
+        launches += tot
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms_b = max_over_ranks(e0.elapsed_time(e1), world)
+    value = job_rate(pts, args.steps, world, ms_b) / 1e9
+    # e2e: the same C-ABI call with host buffers (copies inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        vel_h = torch.from_numpy(np.ascontiguousarray(vel.flatten(order="F"))).pin_memory()
+        dat_h = torch.empty(n * n * nt).pin_memory()
+        ah = L.AfdArgs(dim=3, nz=n, nx=n, ny=n, nt=nt, nbt=NBT, ct=CT, dt=DT, dz=H, dx=H, dy=H,
+                       ns=3, tri=0, jsnap=0, gz=0, flags=L.PW_HOST_PTRS)
+
+        def shot_host():
+            L.check(lib.pw_afd(C.byref(ah), vel_h.data_ptr(), src.ctypes.data, None,
+                               dat_h.data_ptr(), None, st))
+
+        shot_host()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            shot_host()
+        torch.cuda.synchronize()
+        ems = max_over_ranks((time.perf_counter() - t0) * 1e3, world)
+        e2e = {"value": job_rate(pts, args.steps, world, ems) / 1e9, "unit": "Gpt/s",
+               "h2d_bytes_per_step": int(vel.nbytes + src.nbytes),
+               "d2h_bytes_per_step": int(dat_h.numel() * 4)}
+    peak, peak_kind = peaks()
+    loop_ms = statistics.median(loops)
+    kern_ms = loop_ms / nt
+    alg = (n + 2 * NBT) ** 3 * 16  # A, B, vv read and B written per expanded point per step
+    achieved = alg / (kern_ms / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, kind, ps = _a3_cpu(n, 1)
+            cpu = {"value": v, "unit": "Gpt/s", "cores": 1, "kind": kind,
+                   "sample": f"afd3dc forward on the {n + 2 * NBT}^3 expanded grid of the same "
+                             f"model and sources, 1 core; calls of {REF_STEPS[0]} and "
+                             f"{REF_STEPS[1]} steps, {ps:.3f} s per step from their difference"}
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "unit": "Gpt/s", "cores": 1, "kind": "reference",
+                   "sample": f"failed: {ex!r}"[:200]}
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": value, "unit": "Gpt/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_b / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded velocity and sources)",
+            "config": {"workload": workload, "points_per_step": pts,
+                       "l2": "inputs larger than L2 (fields 0.21 GB, vv 0.07 GB)"},
+            "e2e": e2e, "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "tile_kernel<forward> (one launch per step)",
+                         "kernel_ms": kern_ms, "alg_bytes_per_launch": alg,
+                         "peak_source": peak_kind},
+            "cpu_baseline": cpu, "clocks": clocks}), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------
 # fwi3d: 3-D FWI gradients/s, 400 x 400 x 200 at 12.5 m (km units)
 # --------------------------------------------------------------------------
 F3_NZ, F3_NX, F3_NY, F3_H, F3_DT, F3_NB, F3_COEF, F3_F0 = 200, 400, 400, 0.0125, 0.001, 20, 0.015, 12.0
@@ -1664,6 +1851,8 @@ def main():
         return run_pfwic(args, world, rank, local)
     if args.workload == "aps3d":
         return run_aps3d(args, world, rank, local)
+    if args.workload == "afd3d":
+        return run_afd3d(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, rank)
 
