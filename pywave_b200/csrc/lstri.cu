@@ -495,6 +495,12 @@ static int check_args(const pw_fwi_args *a, bool need_shots) {
 // Resident plan: the largest cluster (16, 8, 4, 2 CTAs, one per SM) whose
 // bands of at least 4 columns fit in shared memory and that the device can
 // schedule; otherwise (or with PW_LSTRI_RESIDENT=0) the step-per-launch path.
+// The adjoint (LapT reads 9 more vv quads per quad) takes the step path
+// where its resident form would need a 16-CTA cluster: on the passive
+// demos' grid (250 x 454 padded, nt 3001) one adjoint application runs
+// 12.4 ms step by step against 15.2 ms resident, while the modelling stays
+// resident (11.7 against 12.4 ms).  PW_LSTRI_RESIDENT=1 keeps every
+// operator resident where it fits.
 static void make_plan(const pw_fwi_args *a, bool adj, Plan &p) {
   p.nzp = a->nz + 2 * a->nb;
   p.nxp = a->nx + 2 * a->nb;
@@ -503,6 +509,7 @@ static void make_plan(const pw_fwi_args *a, bool adj, Plan &p) {
   p.resident = false;
   const char *env = getenv("PW_LSTRI_RESIDENT");
   if (env && env[0] == '0') return;
+  const bool force = env && env[0] == '1';
   int dev = 0, maxsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -553,6 +560,7 @@ static void make_plan(const pw_fwi_args *a, bool adj, Plan &p) {
       cudaGetLastError();
     }
     if (!ok) continue;
+    if (adj && C == 16 && !force) return;
     p.resident = true;
     p.C = C;
     p.w = w;
